@@ -1,0 +1,518 @@
+"""Benchmark of the skinny SGEMM/SGEMV path on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload sweep|c1|gemv_n|gemv_t|square]
+
+Default workload ("sweep"): the skinny SGEMM precision sweep, C = A * B
+column-major with M = 65536, K = 4096 and N in {8, 32, 64, 128}, A and B
+uniform[-1, 1] from seed 0 (synthetic, generated on the device by the
+library's SplitMix64 stream).  One step = the four GEMMs, each through
+hml_sgemm_ex with the library's own configuration choice.  A is 1 GiB
+(> the 126 MB L2), so no L2 flush is needed between steps.
+
+The JSON line reports useful TFLOPS (2*M*N*K per GEMM), the roofline of the
+dominant kernel, an end-to-end figure through the host-pointer C ABI
+(hml_host_sgemm, pinned host buffers, copies inside the timed region), the
+reference's CPU loop as a CPU baseline, the SM clocks sampled during the
+timed region and the number of library kernel launches in it.
+
+With torchrun (N > 1) every rank runs the same per-GPU workload on its own
+data (weak scaling: the GEMMs are independent row blocks of a larger
+problem, so there is no data-path collective); the timing is the max over
+ranks.  --impl reference times the reference's own CPU implementation
+(hmlSgemmCpu from oracle/_ref) on a bounded sample on rank 0.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "skinny SGEMM TFLOPS & % roofline: split-BF16 TC vs FP32 SIMT at FP32 accuracy"
+UNIT = "TFLOPS"
+
+SWEEP_M, SWEEP_K, SWEEP_N = 65536, 4096, (8, 32, 64, 128)
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="sweep",
+                    choices=["sweep", "c1", "gemv_n", "gemv_t", "square"])
+    ap.add_argument("--algo", default="auto", choices=["auto", "simt", "bf16x3", "bf16x6"],
+                    help="force one algorithm family (default: the library's choice)")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args()
+
+
+# ------------------------------------------------------------------ peaks
+def peaks():
+    p = {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0,
+         "source": "fallback"}
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            m = json.load(f)
+        for k in ("hbm_gbs", "bf16_tflops", "bf16_tflops_sustained"):
+            if k in m:
+                p[k] = float(m[k])
+        p["source"] = "measured"
+    return p
+
+
+def traffic_table():
+    """Per-launch DRAM bytes of the dominant kernels from committed ncu
+    summaries (profiles/traffic.json), keyed by workload name."""
+    path = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            return json.load(f)
+    return {}
+
+
+# ----------------------------------------------------------------- clocks
+class ClockSampler:
+    """Samples SM clock and throttle reasons through NVML while running."""
+
+    REASONS = {
+        0x0000000000000001: "gpu_idle", 0x0000000000000002: "applications_clocks_setting",
+        0x0000000000000004: "sw_power_cap", 0x0000000000000008: "hw_slowdown",
+        0x0000000000000010: "sync_boost", 0x0000000000000020: "sw_thermal_slowdown",
+        0x0000000000000040: "hw_thermal_slowdown", 0x0000000000000080: "hw_power_brake_slowdown",
+        0x0000000000000100: "display_clock_setting",
+    }
+
+    def __init__(self, index=0, period=0.01):
+        self.samples, self.reasons = [], set()
+        self.max_mhz = None
+        self.period = period
+        self._stop = threading.Event()
+        self.ok = False
+        try:
+            import pynvml
+            pynvml.nvmlInit()
+            self.nv = pynvml
+            self.h = pynvml.nvmlDeviceGetHandleByIndex(index)
+            self.max_mhz = pynvml.nvmlDeviceGetMaxClockInfo(self.h, pynvml.NVML_CLOCK_SM)
+            self.ok = True
+        except Exception:  # noqa: BLE001  (NVML unavailable: report no clocks)
+            self.ok = False
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                self.samples.append(self.nv.nvmlDeviceGetClockInfo(self.h, self.nv.NVML_CLOCK_SM))
+                mask = self.nv.nvmlDeviceGetCurrentClocksEventReasons(self.h)
+                for bit, name in self.REASONS.items():
+                    if mask & bit and name != "gpu_idle":
+                        self.reasons.add(name)
+            except Exception:  # noqa: BLE001
+                pass
+            time.sleep(self.period)
+
+    def __enter__(self):
+        if self.ok:
+            self._t = threading.Thread(target=self._run, daemon=True)
+            self._t.start()
+        return self
+
+    def __exit__(self, *exc):
+        if self.ok:
+            self._stop.set()
+            self._t.join()
+
+    def summary(self):
+        if not self.ok or not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": self.max_mhz, "reasons": sorted(self.reasons),
+                    "samples": len(self.samples)}
+        return {"sm_mhz": statistics.median(self.samples), "sm_max_mhz": self.max_mhz,
+                "reasons": sorted(self.reasons), "samples": len(self.samples)}
+
+
+# ------------------------------------------------------------- workloads
+def workload_problems(name):
+    """List of (kind, M, N, K) problems making one step."""
+    if name == "sweep":
+        return [("sgemm", SWEEP_M, n, SWEEP_K) for n in SWEEP_N]
+    if name == "c1":
+        return [("sgemm", 4096, 16, 4096)]
+    if name == "gemv_n":
+        return [("gemv_n", 32768, 1, 4096)]
+    if name == "gemv_t":
+        return [("gemv_t", 32768, 1, 4096)]
+    if name == "square":
+        return [("sgemm", 8192, 8192, 8192)]
+    raise ValueError(name)
+
+
+def flops_of(kind, M, N, K):
+    return 2.0 * M * N * K if kind == "sgemm" else 2.0 * M * K
+
+
+def bytes_of(kind, M, N, K):
+    """Algorithmic bytes: A and B read once, C written once (beta = 0)."""
+    if kind == "sgemm":
+        return 4.0 * (M * K + K * N + M * N)
+    P = M if kind == "gemv_n" else K
+    Q = K if kind == "gemv_n" else M
+    return 4.0 * (M * K + Q + P)
+
+
+def config_desc(name):
+    if name == "sweep":
+        return {"workload": f"skinny SGEMM C=A*B col-major, M={SWEEP_M}, K={SWEEP_K}, "
+                            f"N in {list(SWEEP_N)} (one step = the 4 GEMMs)",
+                "M": SWEEP_M, "K": SWEEP_K, "N": list(SWEEP_N), "alpha": 1.0, "beta": 0.0,
+                "layout": "column-major NN", "inputs": "uniform[-1,1], seed 0",
+                "l2": "A is 1 GiB per GEMM (> 126 MB L2): inputs larger than L2, no flush"}
+    if name == "c1":
+        return {"workload": "skinny SGEMM col-major M=4096, N=16, K=4096", "M": 4096, "N": 16,
+                "K": 4096, "inputs": "uniform[-1,1], seed 0",
+                "l2": "L2 flushed (256 MiB write) before every step"}
+    if name in ("gemv_n", "gemv_t"):
+        return {"workload": f"SGEMV y={'A' if name == 'gemv_n' else 'A^T'}*x, A 32768x4096 "
+                            "col-major", "inputs": "N(0,1), seed 1",
+                "l2": "A is 512 MiB (> L2): no flush"}
+    return {"workload": "square SGEMM 8192^3 col-major", "inputs": "uniform[-1,1], seed 0",
+            "l2": "compute bound; inputs 256 MiB each"}
+
+
+# -------------------------------------------------------------- reference
+def cpu_reference_sample(problems, seconds=10.0, threads=None):
+    """Times the reference's own hmlSgemmCpu / hmlSgemvCpu (oracle/_ref, or
+    the C restatement when the reference build is absent) on row slices of
+    each problem, on all host cores (one independent row block per thread).
+    Returns (TFLOPS, cores, kind, sample description)."""
+    import ctypes
+    from concurrent.futures import ThreadPoolExecutor
+
+    import numpy as np
+
+    import oracle
+    from hiperml_b200 import datagen as dg
+
+    cores = threads or os.cpu_count() or 1
+    kind = "reference" if oracle.ref_available() else "port"
+    if kind == "reference":
+        R = oracle.ref()
+        f_gemm, f_gemv = R.sgemm_cpu, R.sgemv_cpu
+    else:
+        L = oracle.lib()
+        f_gemm, f_gemv = L.oracle_sgemm_rm_f32, L.oracle_sgemv_rm_f32
+    fp = ctypes.POINTER(ctypes.c_float)
+    # row slices of each problem: rows chosen so that one pass takes ~seconds
+    rows_per_thread = 8
+    jobs = []
+    for (k, M, N, K) in problems:
+        # operands: the logical matrices' row-major copies (exact transposes)
+        A = dg.fill(cores * rows_per_thread * K, 0, 0).reshape(cores * rows_per_thread, K)
+        if k == "sgemm":
+            B = dg.fill(K * N, 0, 1).reshape(K, N)
+            jobs.append((k, A, B, N, K))
+        else:
+            x = dg.fill(K, 1, 1)
+            jobs.append((k, A, x, 1, K))
+
+    def run_block(args):
+        k, A, B, N, K, r0, r1 = args
+        a = A[r0:r1]
+        if k == "sgemm":
+            C = np.zeros((r1 - r0, N), np.float32)
+            f_gemm(C.ctypes.data_as(fp), a.ctypes.data_as(fp), B.ctypes.data_as(fp), r1 - r0, N,
+                   K, 1.0, 0.0)
+        else:
+            y = np.zeros(r1 - r0, np.float32)
+            f_gemv(y.ctypes.data_as(fp), a.ctypes.data_as(fp), B.ctypes.data_as(fp), r1 - r0, K,
+                   1.0, 0.0)
+
+    total_flops, elapsed, passes = 0.0, 0.0, 0
+    with oracle._QuietStderr(), ThreadPoolExecutor(cores) as ex:
+        t_end = time.perf_counter() + seconds
+        while True:
+            for (k, A, B, N, K) in jobs:
+                work = [(k, A, B, N, K, t * rows_per_thread, (t + 1) * rows_per_thread)
+                        for t in range(cores)]
+                t0 = time.perf_counter()
+                list(ex.map(run_block, work))
+                elapsed += time.perf_counter() - t0
+                total_flops += flops_of(k, cores * rows_per_thread, N, K)
+            passes += 1
+            if time.perf_counter() > t_end:
+                break
+    desc = (f"{passes} pass(es) over {cores * rows_per_thread} rows of each problem "
+            f"({', '.join(f'{k} M={M} N={N} K={K}' for (k, M, N, K) in problems)}), "
+            f"one row block per thread, {elapsed:.1f} s")
+    return total_flops / elapsed / 1e12, cores, kind, desc
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    problems = workload_problems(args.workload)
+    per_step = max(1.0, 120.0 / max(1, args.steps + args.warmup))
+    per_step = min(per_step, 10.0)
+    vals = []
+    cores = kind = desc = None
+    for i in range(args.warmup + args.steps):
+        v, cores, kind, desc = cpu_reference_sample(problems, seconds=per_step)
+        if i >= args.warmup:
+            vals.append(v)
+    value = statistics.median(vals)
+    step_flops = sum(flops_of(*p) for p in problems)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT,
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": step_flops / (value * 1e12) * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": config_desc(args.workload),
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": kind,
+                         "sample": desc},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# -------------------------------------------------------------------- ours
+def run_ours(args):
+    import torch
+
+    import hiperml_b200 as hml
+    from hiperml_b200 import datagen as dg
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist_on = world > 1
+    if dist_on:
+        import datetime
+
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    stream = torch.cuda.current_stream()
+
+    problems = workload_problems(args.workload)
+    algo = {"auto": None, "simt": 1, "bf16x3": 2, "bf16x6": 3}[args.algo]
+
+    # ---- device operands (one A shared by the sweep's GEMMs)
+    bufs = []
+    Ashared = None
+    for (k, M, N, K) in problems:
+        if k == "sgemm":
+            if Ashared is None or Ashared.numel() != M * K:
+                Ashared = torch.empty(M * K, dtype=torch.float32, device=dev)
+                hml.fill_random(Ashared, 0 + rank * 1000, 0, dg.UNIFORM)
+            B = torch.empty(K * N, dtype=torch.float32, device=dev)
+            hml.fill_random(B, 0 + rank * 1000, 1, dg.UNIFORM)
+            C = torch.zeros(M * N, dtype=torch.float32, device=dev)
+            cfg = hml.select(0, 0, 0, M, N, K)
+            if algo is not None:
+                from hiperml_b200._lib import lib as L
+                import ctypes
+                best = None
+                for c in hml.configs():
+                    if c.algo == algo and L.hml_sgemm_config_check(0, 0, 0, M, N, K, M, K, M,
+                                                                   ctypes.byref(c)) == 0:
+                        best = c
+                        break
+                cfg = best if best is not None else cfg
+            bufs.append((k, M, N, K, Ashared, B, C, cfg))
+        else:
+            A = torch.empty(M * K, dtype=torch.float32, device=dev)
+            hml.fill_random(A, 1 + rank * 1000, 0, dg.NORMAL)
+            Q = K if k == "gemv_n" else M
+            P = M if k == "gemv_n" else K
+            x = torch.empty(Q, dtype=torch.float32, device=dev)
+            hml.fill_random(x, 1 + rank * 1000, 1, dg.NORMAL)
+            y = torch.zeros(P, dtype=torch.float32, device=dev)
+            bufs.append((k, M, N, K, A, x, y, None))
+    flush = None
+    if args.workload == "c1":
+        flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)  # 256 MiB
+
+    def launch(item):
+        k, M, N, K, A, B, C, cfg = item
+        if k == "sgemm":
+            hml.sgemm_ex(0, 0, 0, M, N, K, 1.0, A, M, B, K, 0.0, C, M, stream=stream,
+                         config=cfg if algo is not None else None)
+        elif k == "gemv_n":
+            hml.sgemv_ex(0, 0, M, K, 1.0, A, M, B, 0.0, C, stream=stream)
+        else:
+            hml.sgemv_ex(0, 1, M, K, 1.0, A, M, B, 0.0, C, stream=stream)
+
+    n_items = len(bufs)
+    ev = [[(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+           for _ in range(n_items)] for _ in range(args.steps)]
+
+    def step(i=None):
+        if flush is not None:
+            flush.fill_(float(i or 0))
+        for j, item in enumerate(bufs):
+            if i is not None:
+                ev[i][j][0].record(stream)
+            launch(item)
+            if i is not None:
+                ev[i][j][1].record(stream)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    if hml.device_error() != 0:
+        raise RuntimeError("device wait expired during warm-up")
+
+    if dist_on:
+        dist.barrier()
+    torch.cuda.synchronize()
+    launches0 = hml.lib.hml_launch_count()
+    t0 = torch.cuda.Event(enable_timing=True)
+    t1 = torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clocks:
+        t0.record(stream)
+        for i in range(args.steps):
+            step(i)
+        t1.record(stream)
+        torch.cuda.synchronize()
+    launches = hml.lib.hml_launch_count() - launches0
+    if dist_on:
+        dist.barrier()
+    elapsed_ms = t0.elapsed_time(t1)
+    per_kernel_ms = [statistics.mean(ev[i][j][0].elapsed_time(ev[i][j][1]) for i in
+                                     range(args.steps)) for j in range(n_items)]
+    if flush is not None:
+        # the flush is outside the measured GEMM events; time only the GEMMs
+        elapsed_ms = sum(sum(ev[i][j][0].elapsed_time(ev[i][j][1]) for j in range(n_items))
+                         for i in range(args.steps))
+    if dist_on:
+        t = torch.tensor([elapsed_ms], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        elapsed_ms = float(t.item())
+    if hml.device_error() != 0:
+        raise RuntimeError("device wait expired in the timed region")
+
+    step_flops = sum(flops_of(k, M, N, K) for (k, M, N, K, *_rest) in bufs)
+    value = step_flops * args.steps * world / (elapsed_ms * 1e-3) / 1e12
+    pk = peaks()
+    # dominant kernel = longest per-launch time
+    dom = max(range(n_items), key=lambda j: per_kernel_ms[j])
+    k, M, N, K, *_ = bufs[dom]
+    alg_bytes = bytes_of(k, M, N, K)
+    alg_flops = flops_of(k, M, N, K)
+    dom_s = per_kernel_ms[dom] * 1e-3
+    dcfg = bufs[dom][7]
+    algo_names = {1: "simt", 2: "bf16x3", 3: "bf16x6"}
+    key = f"{args.workload}:{k}:{M}x{N}x{K}:{algo_names.get(dcfg.algo, 'gemv') if dcfg else 'gemv'}"
+    traffic = traffic_table().get(key)
+    ai = alg_flops / alg_bytes
+    roof = {"bound": "hbm", "achieved": alg_bytes / dom_s / 1e9, "peak": pk["hbm_gbs"],
+            "unit": "GB/s", "frac": alg_bytes / dom_s / 1e9 / pk["hbm_gbs"],
+            "traffic": traffic, "kernel": key, "alg_bytes_per_launch": alg_bytes,
+            "alg_flops_per_launch": alg_flops, "ms_per_launch": per_kernel_ms[dom],
+            "peak_source": pk["source"], "arith_intensity": ai}
+    if dcfg is not None and dcfg.algo in (2, 3):
+        ridge = pk["bf16_tflops_sustained"] * 1e12 / (pk["hbm_gbs"] * 1e9)
+        products = 3 if dcfg.algo == 2 else 6
+        if ai * products > ridge:
+            tc = alg_flops * products / dom_s / 1e12
+            roof.update({"bound": "tensor", "achieved": tc, "peak": pk["bf16_tflops_sustained"],
+                         "unit": "TFLOP/s", "frac": tc / pk["bf16_tflops_sustained"]})
+    if dcfg is not None and dcfg.algo == 1:
+        # SIMT FP32: nominal 148 SMs x 128 FMA lanes x 2 x 1.965 GHz
+        roof["simt_fp32_tflops"] = alg_flops / dom_s / 1e12
+        roof["simt_fp32_peak_nominal"] = 148 * 128 * 2 * 1.965e-3
+
+    per_shape = []
+    for j, (k, M, N, K, A, B, C, cfg) in enumerate(bufs):
+        entry = {"kind": k, "M": M, "N": N, "K": K, "ms": per_kernel_ms[j],
+                 "tflops": flops_of(k, M, N, K) / (per_kernel_ms[j] * 1e-3) / 1e12,
+                 "gbs": bytes_of(k, M, N, K) / (per_kernel_ms[j] * 1e-3) / 1e9,
+                 "config": repr(cfg) if cfg is not None else "gemv"}
+        if k == "sgemm" and rank == 0:
+            err = hml.error_fp64(0, 0, 0, M, N, K, 1.0, A, M, B, K, 0.0, None, C, M)
+            entry["max_rel_err_fp64"] = err[0]
+            entry["rms_rel_err_fp64"] = err[1]
+            entry["compwise_err_fp64"] = err[2]
+        per_shape.append(entry)
+
+    # ---- end to end through the host-pointer C ABI (pinned host buffers)
+    e2e = None
+    if not args.no_e2e and all(b[0] == "sgemm" for b in bufs):
+        e2e_steps = max(1, min(args.steps, 5))
+        hosts = []
+        for (k, M, N, K, A, B, C, cfg) in bufs:
+            hA = A.cpu().pin_memory() if not hosts or hosts[-1][0].numel() != A.numel() else hosts[-1][0]
+            hB = B.cpu().pin_memory()
+            hC = torch.empty(M * N, dtype=torch.float32).pin_memory()
+            hosts.append((hA, hB, hC, M, N, K))
+        # column-major C = A B  ==  row-major C^T = B^T A^T : hmlSgemm(C, B, A, N, M, K)
+        def e2e_step():
+            for (hA, hB, hC, M, N, K) in hosts:
+                from hiperml_b200._lib import check
+                check(hml.lib.hml_host_sgemm(0, hC.data_ptr(), hB.data_ptr(), hA.data_ptr(),
+                                             N, M, K, 1.0, 0.0), "hml_host_sgemm")
+        e2e_step()
+        if dist_on:
+            dist.barrier()
+        ts = time.perf_counter()
+        for _ in range(e2e_steps):
+            e2e_step()
+        te = time.perf_counter() - ts
+        if dist_on:
+            t = torch.tensor([te], device=dev, dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            te = float(t.item())
+        h2d = sum(4 * (M * K + K * N) for (_, _, _, M, N, K) in hosts)
+        d2h = sum(4 * M * N for (_, _, _, M, N, K) in hosts)
+        e2e = {"value": step_flops * e2e_steps * world / te / 1e12, "unit": UNIT,
+               "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+               "api": "hml_host_sgemm (reference-facing hmlSgemm ABI), pinned host buffers",
+               "steps": e2e_steps}
+
+    cpu = None
+    if not args.no_cpu_baseline and rank == 0 and world == 1:
+        v, cores, kind, desc = cpu_reference_sample([(k, M, N, K) for (k, M, N, K, *_r) in bufs],
+                                                    seconds=10.0)
+        cpu = {"value": v, "unit": UNIT, "cores": cores, "kind": kind, "sample": desc}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": elapsed_ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": dict(config_desc(args.workload),
+                           parallelism=f"independent per-GPU problems x{world}"),
+            "roofline": roof, "cpu_baseline": cpu, "e2e": e2e,
+            "clocks": clocks.summary(), "gpu_launches": int(launches),
+            "per_shape": per_shape,
+        }
+        print(json.dumps(line), flush=True)
+    if dist_on:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,15 @@
+"""hiperml_b200 -- HiperML's skinny SGEMM/SGEMV path rebuilt for NVIDIA B200.
+
+The compute lives in ``libhml_b200.so`` (hand-written sm_100a CUDA behind
+the C ABI of ``include/hml_b200.h``); this package is its Python host side.
+Importing it fails when the library has not been built: there is no CPU
+fallback for any entry point.
+"""
+from ._lib import HmlError, SgemmConfig, lib  # noqa: F401  (loads the .so)
+from .api import (  # noqa: F401
+    ALGO_AUTO, ALGO_BF16X3, ALGO_BF16X6, ALGO_SIMT, COL_MAJOR, OP_N, OP_T, ROW_MAJOR,
+    config_check, configs, device_error, error_fp64, fill_random, hmlSgemm, hmlSgemmBasic,
+    hmlSgemmKernelConfig, hmlSgemv, hmlSgemvBasic, hmlSgemvKernelConfig, select, sgemm,
+    sgemm_ex, sgemv_ex)
+
+__version__ = lib.hml_version().decode()

@@ -1,0 +1,216 @@
+"""Python host side of the skinny SGEMM/SGEMV path.
+
+Two layers, both thin over the C ABI (``include/hml_b200.h``):
+
+* the reference's interface, same names and argument meaning as
+  ``include/hml_sgemm.h`` / ``include/hml_sgemv.h`` of the reference:
+  ``hmlSgemm(C, A, B, M, N, K, alpha, beta)`` etc. on host (numpy) arrays,
+  row-major, C updated in place.  Where the reference prints and calls
+  ``exit(1)`` these raise ``HmlError``.
+* the device-pointer interface ``sgemm_ex`` / ``sgemv_ex`` (BLAS argument
+  order, either storage order, transposes, leading dimensions, a stream),
+  taking torch CUDA tensors or raw device addresses.
+"""
+from __future__ import annotations
+
+import ctypes
+from typing import Optional
+
+import numpy as np
+
+from ._lib import SgemmConfig, check, lib
+
+COL_MAJOR, ROW_MAJOR = 0, 1
+OP_N, OP_T = 0, 1
+ALGO_AUTO, ALGO_SIMT, ALGO_BF16X3, ALGO_BF16X6 = 0, 1, 2, 3
+
+
+def _ptr(x) -> Optional[int]:
+    if x is None:
+        return None
+    if isinstance(x, int):
+        return x
+    if hasattr(x, "data_ptr"):
+        return x.data_ptr()
+    if isinstance(x, np.ndarray):
+        return x.ctypes.data
+    raise TypeError(f"cannot take a pointer of {type(x)}")
+
+
+def _stream(stream) -> Optional[int]:
+    if stream is None:
+        try:
+            import torch
+            if torch.cuda.is_available():
+                return torch.cuda.current_stream().cuda_stream
+        except ImportError:
+            pass
+        return None
+    if isinstance(stream, int):
+        return stream
+    return stream.cuda_stream
+
+
+def _host_f32(a, name):
+    if not isinstance(a, np.ndarray) or a.dtype != np.float32 or not a.flags["C_CONTIGUOUS"]:
+        raise TypeError(f"{name} must be a C-contiguous float32 numpy array")
+    return a
+
+
+# ------------------------------------------------------ reference interface
+def hmlSgemmKernelConfig(sgemmKernelConfigFileName: Optional[str]) -> None:
+    """``hmlSgemmKernelConfig`` (reference src/hml_sgemm.cu:213-226)."""
+    path = None if sgemmKernelConfigFileName is None else sgemmKernelConfigFileName.encode()
+    check(lib.hml_config_file(0, path), "hmlSgemmKernelConfig")
+
+
+def hmlSgemvKernelConfig(sgemvKernelConfigFileName: Optional[str]) -> None:
+    """``hmlSgemvKernelConfig`` (reference src/hml_sgemv.cu:215-228)."""
+    path = None if sgemvKernelConfigFileName is None else sgemvKernelConfigFileName.encode()
+    check(lib.hml_config_file(1, path), "hmlSgemvKernelConfig")
+
+
+def _host_sgemm(basic, C, A, B, M, N, K, alpha, beta, where):
+    C = _host_f32(C, "C")
+    A = _host_f32(A, "A")
+    B = _host_f32(B, "B")
+    if C.size < M * N or A.size < M * K or B.size < K * N:
+        raise ValueError(f"{where}: arrays smaller than the M, N, K they are given with")
+    check(lib.hml_host_sgemm(basic, C.ctypes.data, A.ctypes.data, B.ctypes.data, M, N, K,
+                             alpha, beta), where)
+
+
+def hmlSgemm(C, A, B, M, N, K, alpha, beta) -> None:
+    """C = alpha*A*B + beta*C, host arrays, row-major, C updated in place
+    (reference src/hml_sgemm.cu:120-211)."""
+    _host_sgemm(0, C, A, B, M, N, K, alpha, beta, "hmlSgemm")
+
+
+def hmlSgemmBasic(C, A, B, M, N, K, alpha, beta) -> None:
+    """Same with the default configuration (reference src/hml_sgemm.cu:39-113)."""
+    _host_sgemm(1, C, A, B, M, N, K, alpha, beta, "hmlSgemmBasic")
+
+
+def _host_sgemv(basic, y, A, x, M, N, alpha, beta, where):
+    y = _host_f32(y, "y")
+    A = _host_f32(A, "A")
+    x = _host_f32(x, "x")
+    if y.size < M or A.size < M * N or x.size < N:
+        raise ValueError(f"{where}: arrays smaller than the M, N they are given with")
+    check(lib.hml_host_sgemv(basic, y.ctypes.data, A.ctypes.data, x.ctypes.data, M, N,
+                             alpha, beta), where)
+
+
+def hmlSgemv(y, A, x, M, N, alpha, beta) -> None:
+    """y = alpha*A*x + beta*y, host arrays, A row-major M x N
+    (reference src/hml_sgemv.cu:125-213)."""
+    _host_sgemv(0, y, A, x, M, N, alpha, beta, "hmlSgemv")
+
+
+def hmlSgemvBasic(y, A, x, M, N, alpha, beta) -> None:
+    """Same with the default kernel (reference src/hml_sgemv.cu:38-118)."""
+    _host_sgemv(1, y, A, x, M, N, alpha, beta, "hmlSgemvBasic")
+
+
+# ---------------------------------------------------- device-pointer layer
+def sgemm_ex(order, transA, transB, M, N, K, alpha, A, lda, B, ldb, beta, C, ldc,
+             stream=None, config: Optional[SgemmConfig] = None) -> None:
+    """``hml_sgemm_ex`` / ``hml_sgemm_ex_config`` on device memory."""
+    s = _stream(stream)
+    if config is None:
+        st = lib.hml_sgemm_ex(order, transA, transB, M, N, K, alpha, _ptr(A), lda, _ptr(B), ldb,
+                              beta, _ptr(C), ldc, s)
+    else:
+        st = lib.hml_sgemm_ex_config(order, transA, transB, M, N, K, alpha, _ptr(A), lda,
+                                     _ptr(B), ldb, beta, _ptr(C), ldc, ctypes.byref(config), s)
+    check(st, "hml_sgemm_ex")
+
+
+def sgemv_ex(order, trans, M, N, alpha, A, lda, x, beta, y, stream=None, variant=0) -> None:
+    """``hml_sgemv_ex`` on device memory (``variant`` forces a kernel shape)."""
+    s = _stream(stream)
+    if variant:
+        st = lib.hml_sgemv_ex_variant(order, trans, M, N, alpha, _ptr(A), lda, _ptr(x), beta,
+                                      _ptr(y), variant, s)
+    else:
+        st = lib.hml_sgemv_ex(order, trans, M, N, alpha, _ptr(A), lda, _ptr(x), beta, _ptr(y), s)
+    check(st, "hml_sgemv_ex")
+
+
+def _blas_view(t):
+    """(order, ld) of a 2-D torch tensor that is column- or row-major dense
+    along one dimension."""
+    r, c = t.shape
+    s0, s1 = t.stride()
+    if s0 == 1 and (s1 >= max(1, r) or c == 1):
+        return COL_MAJOR, max(1, s1 if c > 1 else r)
+    if s1 == 1 and (s0 >= max(1, c) or r == 1):
+        return ROW_MAJOR, max(1, s0 if r > 1 else c)
+    raise ValueError("tensor must have one unit stride")
+
+
+def sgemm(A, B, C=None, alpha=1.0, beta=0.0, config=None, stream=None):
+    """C = alpha*A@B + beta*C for FP32 CUDA tensors of either storage order.
+    Returns C (allocated column-major when not given)."""
+    import torch
+    M, K = A.shape
+    K2, N = B.shape
+    if K != K2:
+        raise ValueError("inner dimensions differ")
+    if C is None:
+        C = torch.empty((N, M), dtype=torch.float32, device=A.device).t()
+        beta = 0.0
+    oc, ldc = _blas_view(C)
+    # express A and B in C's storage order, transposing as needed
+    def op(t):
+        o, ld = _blas_view(t)
+        return (OP_N if o == oc else OP_T), ld
+    ta, lda = op(A)
+    tb, ldb = op(B)
+    sgemm_ex(oc, ta, tb, M, N, K, alpha, A, lda, B, ldb, beta, C, ldc, stream=stream,
+             config=config)
+    return C
+
+
+def select(order, transA, transB, M, N, K) -> SgemmConfig:
+    c = SgemmConfig()
+    check(lib.hml_sgemm_select(order, transA, transB, M, N, K, ctypes.byref(c)), "hml_sgemm_select")
+    return c
+
+
+def configs():
+    """The autotuner's configuration space."""
+    out = []
+    for i in range(lib.hml_sgemm_num_configs()):
+        c = SgemmConfig()
+        check(lib.hml_sgemm_get_config(i, ctypes.byref(c)), "hml_sgemm_get_config")
+        out.append(c)
+    return out
+
+
+def config_check(order, transA, transB, M, N, K, lda, ldb, ldc, config) -> int:
+    return lib.hml_sgemm_config_check(order, transA, transB, M, N, K, lda, ldb, ldc,
+                                      ctypes.byref(config))
+
+
+def fill_random(t, seed: int, stream_id: int, dist: int = 0, stream=None) -> None:
+    """Fill a float32 CUDA tensor with the SplitMix64 stream of
+    ``hiperml_b200.datagen`` (storage order)."""
+    check(lib.hml_fill_random(_ptr(t), t.numel(), seed, stream_id, dist, _stream(stream)),
+          "hml_fill_random")
+
+
+def error_fp64(order, transA, transB, M, N, K, alpha, A, lda, B, ldb, beta, C0, C, ldc,
+               stream=None):
+    """FP64 check on the GPU: (normwise, rms, componentwise, max|C64|)."""
+    err = (ctypes.c_double * 4)()
+    check(lib.hml_sgemm_error_fp64(order, transA, transB, M, N, K, alpha, _ptr(A), lda, _ptr(B),
+                                   ldb, beta, _ptr(C0), _ptr(C), ldc, err, _stream(stream)),
+          "hml_sgemm_error_fp64")
+    return tuple(err)
+
+
+def device_error() -> int:
+    code = ctypes.c_int()
+    check(lib.hml_device_error(ctypes.byref(code)), "hml_device_error")
+    return code.value

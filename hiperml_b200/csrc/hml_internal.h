@@ -1,0 +1,108 @@
+// hml_internal.h -- host-side internals shared by the library's translation
+// units: the canonical problem forms, launch helpers, tensor-map encoding
+// and per-device resources.
+#pragma once
+
+#include <cuda.h>  // CUtensorMap and its enums (header only; the driver
+                   // entry point is looked up at run time)
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "../../include/hml_b200.h"
+
+namespace hml {
+
+// Canonical SGEMM: C(m,n) = alpha * sum_k A(m,k) B(k,n) + beta * C(m,n),
+// with A(m,k) = A[m*sam + k*sak], B(k,n) = B[k*sbk + n*sbn],
+// C(m,n) = C[m*scm + n*scn].  After normalisation M >= N (M is the long
+// dimension) and each operand has one unit stride.
+struct GemmProblem {
+  int M, N, K;
+  float alpha, beta;
+  const float *A;
+  int64_t sam, sak;
+  const float *B;
+  int64_t sbk, sbn;
+  float *C;
+  int64_t scm, scn;
+  bool a_kcontig() const { return sak == 1 && !(sam == 1 && K == 1); }
+  bool b_kcontig() const { return sbk == 1; }
+};
+
+// Canonical SGEMV: y[p*incy] = alpha * sum_q A(p,q) x[q*incx] + beta * y,
+// A(p,q) = A[p*sp + q*sq].
+struct GemvProblem {
+  int P, Q;
+  float alpha, beta;
+  const float *A;
+  int64_t sp, sq;
+  const float *x;
+  int64_t incx;
+  float *y;
+  int64_t incy;
+};
+
+hml_status gemm_from_blas(hml_order order, hml_op ta, hml_op tb, int M, int N, int K,
+                          float alpha, const float *A, int lda, const float *B, int ldb,
+                          float beta, float *C, int ldc, GemmProblem *out);
+
+hml_status gemv_from_blas(hml_order order, hml_op trans, int M, int N, float alpha,
+                          const float *A, int lda, const float *x, float beta, float *y,
+                          GemvProblem *out);
+
+// Kernels (one launcher per family).  All are stream ordered.
+hml_status launch_gemv(const GemvProblem &p, int variant, cudaStream_t s);
+hml_status launch_scale(float *C, int M, int N, int64_t scm, int64_t scn, float beta,
+                        cudaStream_t s);
+hml_status launch_simt(const GemmProblem &p, const hml_sgemm_config &c, cudaStream_t s);
+hml_status launch_tc(const GemmProblem &p, const hml_sgemm_config &c, cudaStream_t s);
+hml_status check_simt(const GemmProblem &p, const hml_sgemm_config &c);
+hml_status check_tc(const GemmProblem &p, const hml_sgemm_config &c);
+
+// Per-device resources.
+int *device_error_word();  // nullptr on failure
+hml_status workspace(size_t bytes, cudaStream_t s, void **ptr);
+
+// Tensor maps.
+bool tensor_map_2d(CUtensorMap *map, CUtensorMapDataType dtype, const void *base,
+                   uint64_t dim0, uint64_t dim1, uint64_t stride1_bytes, uint32_t box0,
+                   uint32_t box1, CUtensorMapSwizzle swizzle);
+
+inline hml_status cuda_status(cudaError_t e) {
+  return e == cudaSuccess ? HML_STATUS_SUCCESS : HML_STATUS_CUDA_ERROR;
+}
+
+// Remember the last CUDA error text for diagnostics.
+void note_cuda_error(cudaError_t e, const char *where);
+const char *last_error_text();
+
+int sm_count();
+
+// Number of kernels this library has launched (all devices, all threads).
+void count_launch(int n = 1);
+uint64_t launch_count();
+
+// Launch with an optional thread-block cluster along x.
+template <typename... KArgs, typename... Args>
+cudaError_t launch_k(void (*k)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t s,
+                     int cluster_x, Args... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  cfg.numAttrs = 0;
+  if (cluster_x > 1) {
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = cluster_x;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+  }
+  count_launch();
+  return cudaLaunchKernelEx(&cfg, k, static_cast<KArgs>(args)...);
+}
+
+}  // namespace hml

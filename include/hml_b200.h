@@ -1,0 +1,199 @@
+/*
+ * hml_b200.h -- C ABI of the B200 (sm_100a) skinny SGEMM/SGEMV library.
+ *
+ * Every entry point is extern "C", takes plain pointers and sizes, and
+ * returns an hml_status.  Device-pointer entry points are stream ordered
+ * (the stream is passed as an opaque cudaStream_t, NULL = legacy default
+ * stream) and return as soon as the work is enqueued.  Nothing here calls
+ * exit(): errors come back as status codes.
+ *
+ * The reference's public C++ entry points (hmlSgemm, hmlSgemmBasic,
+ * hmlSgemmKernelConfig, hmlSgemv, hmlSgemvBasic, hmlSgemvKernelConfig) are
+ * exported too, with their original C++ linkage, from hml_sgemm.h and
+ * hml_sgemv.h in this directory; they are thin shims over this ABI.
+ *
+ * Conventions
+ *   - BLAS semantics: C = alpha * op(A) * op(B) + beta * C, op(X) = X or X^T,
+ *     with column-major (HML_COL_MAJOR) or row-major (HML_ROW_MAJOR) storage
+ *     and leading dimensions.  beta == 0 means C is not read (NaN in C does
+ *     not propagate), unlike the reference kernels, which always read C
+ *     (include/hml_sgemm_kernel_template.h:187 in the reference).
+ *   - All arithmetic on the hot path is FP32 in and FP32 out.  The split-BF16
+ *     algorithms use BF16 tensor-core products of FP32 operands split on the
+ *     fly into 2 or 3 BF16 terms, accumulated in FP32.
+ */
+#ifndef HML_B200_H_INCLUDED_
+#define HML_B200_H_INCLUDED_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum hml_status {
+  HML_STATUS_SUCCESS = 0,
+  HML_STATUS_INVALID_VALUE = 1,  /* bad size, stride, pointer or enum     */
+  HML_STATUS_NOT_SUPPORTED = 2,  /* valid request this build cannot serve */
+  HML_STATUS_CUDA_ERROR = 3,     /* a CUDA runtime call failed            */
+  HML_STATUS_ALLOC_FAILED = 4,   /* device or pinned allocation failed    */
+  HML_STATUS_CONFIG_ERROR = 5,   /* malformed or out-of-range tuning data */
+  HML_STATUS_TIMEOUT = 6,        /* a bounded device-side wait expired    */
+  HML_STATUS_IO_ERROR = 7        /* file could not be opened or written   */
+} hml_status;
+
+typedef enum hml_order { HML_COL_MAJOR = 0, HML_ROW_MAJOR = 1 } hml_order;
+typedef enum hml_op { HML_OP_N = 0, HML_OP_T = 1 } hml_op;
+
+/* Algorithm families of the SGEMM path. */
+typedef enum hml_algo {
+  HML_ALGO_AUTO = 0,   /* tuned table, then predictor, then default        */
+  HML_ALGO_SIMT = 1,   /* plain FP32 FMA on CUDA cores                     */
+  HML_ALGO_BF16X3 = 2, /* tcgen05: hi/lo BF16 split, 3 products (hh,hl,lh) */
+  HML_ALGO_BF16X6 = 3  /* tcgen05: hi/mid/lo split, 6 products            */
+} hml_algo;
+
+/* One point of the SGEMM configuration space. */
+typedef struct hml_sgemm_config {
+  int32_t algo;    /* hml_algo                                            */
+  int32_t tile_m;  /* rows of C per CTA (the long dimension)              */
+  int32_t tile_n;  /* columns of C per CTA (the skinny dimension)         */
+  int32_t split_k; /* CTAs of one thread-block cluster sharing a C tile,
+                      each taking a slice of K; partial tiles are summed
+                      in rank order through distributed shared memory     */
+  int32_t stages;  /* shared-memory pipeline depth                        */
+  int32_t variant; /* per-algorithm micro-tile selector                   */
+} hml_sgemm_config;
+
+const char *hml_status_string(hml_status status);
+const char *hml_version(void);
+
+/* ---------------------------------------------------------------- SGEMM */
+
+/* C = alpha * op(A) * op(B) + beta * C on device pointers.  op(A) is M x K,
+ * op(B) is K x N, C is M x N.  The configuration comes from the tuned table
+ * (hml_tune_load / hml_autotune_sgemm), else the learned predictor when one
+ * is loaded, else the built-in heuristic.  Replaces the launch half of
+ * hmlSgemm (src/hml_sgemm.cu:120-211 in the reference), generalised to
+ * both storage orders, transposes and leading dimensions. */
+hml_status hml_sgemm_ex(hml_order order, hml_op transA, hml_op transB, int M,
+                        int N, int K, float alpha, const float *A, int lda,
+                        const float *B, int ldb, float beta, float *C, int ldc,
+                        void *stream);
+
+/* Same, with an explicit configuration (algo must not be HML_ALGO_AUTO).
+ * Replaces launching one chosen kernel of the reference's repository
+ * (hmlSgemmKernelSelect + launch, src/hml_sgemm_kernel.cu:189-237). */
+hml_status hml_sgemm_ex_config(hml_order order, hml_op transA, hml_op transB,
+                               int M, int N, int K, float alpha, const float *A,
+                               int lda, const float *B, int ldb, float beta,
+                               float *C, int ldc,
+                               const hml_sgemm_config *config, void *stream);
+
+/* The configuration hml_sgemm_ex would use for this problem. */
+hml_status hml_sgemm_select(hml_order order, hml_op transA, hml_op transB,
+                            int M, int N, int K, hml_sgemm_config *config);
+
+/* Whether a configuration can run this problem (status only, no launch). */
+hml_status hml_sgemm_config_check(hml_order order, hml_op transA, hml_op transB,
+                                  int M, int N, int K, int lda, int ldb, int ldc,
+                                  const hml_sgemm_config *config);
+
+/* Enumeration of the configuration space the autotuner searches.  Replaces
+ * the reference's kernel repository tables (include/hml_sgemm_kernel.h:62-66). */
+int hml_sgemm_num_configs(void);
+hml_status hml_sgemm_get_config(int index, hml_sgemm_config *config);
+int hml_sgemm_config_index(const hml_sgemm_config *config);
+
+/* ---------------------------------------------------------------- SGEMV */
+
+/* y = alpha * op(A) * x + beta * y on device pointers; A is M x N in storage,
+ * op(A) is A (length(y) = M) or A^T (length(y) = N).  Replaces hmlSgemv
+ * (src/hml_sgemv.cu:125-213), which is the row-major, non-transposed case. */
+hml_status hml_sgemv_ex(hml_order order, hml_op trans, int M, int N,
+                        float alpha, const float *A, int lda, const float *x,
+                        float beta, float *y, void *stream);
+
+/* Same, forcing a kernel variant: for A with contiguous rows the number of
+ * threads that share one row (4, 8, ..., 256); for A with contiguous
+ * columns the thread-block-cluster split of the columns (1..8).  0 = the
+ * heuristic.  Replaces launching one chosen SGEMV kernel of the reference's
+ * repository (hmlSgemvKernelSelect + launch, src/hml_sgemv_kernel.cu:315-355). */
+hml_status hml_sgemv_ex_variant(hml_order order, hml_op trans, int M, int N,
+                                float alpha, const float *A, int lda,
+                                const float *x, float beta, float *y,
+                                int variant, void *stream);
+
+/* ------------------------------------------------- host-pointer path */
+
+/* Row-major C = alpha*A*B + beta*C on HOST pointers (A M x K, B K x N),
+ * synchronous; basic != 0 forces the heuristic configuration.  The status
+ * returning form of hmlSgemm / hmlSgemmBasic (src/hml_sgemm.cu:39-211). */
+hml_status hml_host_sgemm(int basic, float *C, const float *A, const float *B,
+                          int M, int N, int K, float alpha, float beta);
+
+/* Row-major y = alpha*A*x + beta*y on HOST pointers, synchronous.  The
+ * status-returning form of hmlSgemv / hmlSgemvBasic (src/hml_sgemv.cu). */
+hml_status hml_host_sgemv(int basic, float *y, const float *A, const float *x,
+                          int M, int N, float alpha, float beta);
+
+/* ------------------------------------------------------ tuning files */
+
+/* kind 0 = SGEMM, 1 = SGEMV.  Reads a tuning file the way
+ * hmlSgemmKernelConfig / hmlSgemvKernelConfig do (src/hml_sgemm.cu:213-226,
+ * src/hml_sgemv.cu:215-228): this library's measured table, or a reference
+ * v1 file.  NULL keeps the current selection. */
+hml_status hml_config_file(int kind, const char *path);
+
+/* Reads a reference v1 file (src/hml_sgemm_kernel.cu:573-602,
+ * src/hml_sgemv_kernel.cu:650-679), range-checking every rule; *rules gets
+ * the number of rules read.  A bad line rejects the file. */
+hml_status hml_cfg_v1_load(int kind, const char *path, int *rules);
+
+/* The v1 rule the reference would apply (its keying: K' = min(K, 96),
+ * colStops = ceil(min(N, 96) / 16); SGEMV: N <= 1024 ? N : 0).
+ * HML_STATUS_CONFIG_ERROR when no valid rule applies. */
+hml_status hml_cfg_v1_sgemm_rule(int K, int N, int *type, int *row_stops);
+hml_status hml_cfg_v1_sgemv_rule(int N, int *type, int *block_stops,
+                                 int *row_stops);
+void hml_cfg_v1_clear(void);
+
+/* ------------------------------------------------------------ utilities */
+
+/* Text of the last CUDA error seen by this thread inside the library. */
+const char *hml_last_error(void);
+
+/* Fill n floats with the counter-based SplitMix64 generator (dist 0 =
+ * uniform[-1,1), 1 = normal(0,1), 2 = log-uniform magnitude 1e-3..1e3 with
+ * random sign).  Identical stream to hiperml_b200.datagen. */
+hml_status hml_fill_random(float *out, size_t n, uint64_t seed,
+                           uint64_t stream_id, int dist, void *stream);
+
+/* FP64 check of an SGEMM result, on the GPU: recomputes alpha*op(A)*op(B) +
+ * beta*C0 in FP64 (C0 = the C that was passed in, given here as C0) and
+ * compares it with C.  err[0] = max|dC| / max|C64| (normwise),
+ * err[1] = ||dC||_2 / ||C64||_2 (RMS), err[2] = max_ij |dC_ij| /
+ * (|alpha| |op(A)||op(B)| + |beta||C0|)_ij (componentwise), err[3] = max|C64|.
+ * FP64 is used only here and never on the hot path. */
+hml_status hml_sgemm_error_fp64(hml_order order, hml_op transA, hml_op transB,
+                                int M, int N, int K, float alpha,
+                                const float *A, int lda, const float *B,
+                                int ldb, float beta, const float *C0,
+                                const float *C, int ldc, double err[4],
+                                void *stream);
+
+/* Device-side error word of bounded waits: 0 when clear.  Reading clears. */
+hml_status hml_device_error(int *code);
+
+/* Number of kernels the library has launched since it was loaded. */
+uint64_t hml_launch_count(void);
+
+/* Frees the library's cached device workspaces and staging buffers. */
+hml_status hml_release_resources(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* HML_B200_H_INCLUDED_ */
