@@ -320,17 +320,8 @@ def run_ours(args):
             B = torch.empty(K * N, dtype=torch.float32, device=dev)
             hml.fill_random(B, 0 + rank * 1000, 1, dg.UNIFORM)
             C = torch.zeros(M * N, dtype=torch.float32, device=dev)
-            cfg = hml.select(0, 0, 0, M, N, K)
-            if algo is not None:
-                from hiperml_b200._lib import lib as L
-                import ctypes
-                best = None
-                for c in hml.configs():
-                    if c.algo == algo and L.hml_sgemm_config_check(0, 0, 0, M, N, K, M, K, M,
-                                                                   ctypes.byref(c)) == 0:
-                        best = c
-                        break
-                cfg = best if best is not None else cfg
+            cfg = hml.select(0, 0, 0, M, N, K) if algo is None else \
+                hml.select_algo(0, 0, 0, M, N, K, algo)
             bufs.append((k, M, N, K, Ashared, B, C, cfg))
         else:
             A = torch.empty(M * K, dtype=torch.float32, device=dev)

@@ -9,7 +9,7 @@ from ._lib import HmlError, SgemmConfig, lib  # noqa: F401  (loads the .so)
 from .api import (  # noqa: F401
     ALGO_AUTO, ALGO_BF16X3, ALGO_BF16X6, ALGO_SIMT, COL_MAJOR, OP_N, OP_T, ROW_MAJOR,
     config_check, configs, device_error, error_fp64, fill_random, hmlSgemm, hmlSgemmBasic,
-    hmlSgemmKernelConfig, hmlSgemv, hmlSgemvBasic, hmlSgemvKernelConfig, select, sgemm,
+    hmlSgemmKernelConfig, hmlSgemv, hmlSgemvBasic, hmlSgemvKernelConfig, select, select_algo, sgemm,
     sgemm_ex, sgemv_ex)
 
 __version__ = lib.hml_version().decode()

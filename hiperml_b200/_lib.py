@@ -49,6 +49,8 @@ _SIGS = {
                                     ctypes.POINTER(SgemmConfig), c_void_p]),
     "hml_sgemm_select": (c_int, [c_int, c_int, c_int, c_int, c_int, c_int,
                                  ctypes.POINTER(SgemmConfig)]),
+    "hml_sgemm_select_algo": (c_int, [c_int, c_int, c_int, c_int, c_int, c_int, c_int,
+                                      ctypes.POINTER(SgemmConfig)]),
     "hml_sgemm_config_check": (c_int, [c_int, c_int, c_int, c_int, c_int, c_int, c_int, c_int,
                                        c_int, ctypes.POINTER(SgemmConfig)]),
     "hml_sgemm_num_configs": (c_int, []),

@@ -178,6 +178,14 @@ def select(order, transA, transB, M, N, K) -> SgemmConfig:
     return c
 
 
+def select_algo(order, transA, transB, M, N, K, algo) -> SgemmConfig:
+    """The heuristic configuration of one algorithm family."""
+    c = SgemmConfig()
+    check(lib.hml_sgemm_select_algo(order, transA, transB, M, N, K, algo, ctypes.byref(c)),
+          "hml_sgemm_select_algo")
+    return c
+
+
 def configs():
     """The autotuner's configuration space."""
     out = []

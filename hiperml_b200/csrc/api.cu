@@ -115,7 +115,7 @@ std::vector<hml_sgemm_config> build_space() {
       int bm, bn;
       tc_shape(var, &bm, &bn);
       for (int split : {1, 2, 4, 8, 16})
-        for (int stages : {2, 3, 4}) {
+        for (int stages : {2, 3, 4, 6}) {
           if (!tc_config_fits(bn, algo == HML_ALGO_BF16X3 ? 2 : 3, stages)) continue;
           hml_sgemm_config c = {algo, bm, bn, split, stages, var};
           v.push_back(c);
@@ -248,11 +248,30 @@ hml_status hml_sgemm_select(hml_order order, hml_op transA, hml_op transB, int M
   return select_config(p, config);
 }
 
+hml_status hml_sgemm_select_algo(hml_order order, hml_op transA, hml_op transB, int M, int N,
+                                 int K, int algo, hml_sgemm_config *config) {
+  if (!config) return HML_STATUS_INVALID_VALUE;
+  if (algo == HML_ALGO_AUTO) return hml_sgemm_select(order, transA, transB, M, N, K, config);
+  if (algo != HML_ALGO_SIMT && algo != HML_ALGO_BF16X3 && algo != HML_ALGO_BF16X6)
+    return HML_STATUS_INVALID_VALUE;
+  GemmProblem p;
+  const bool cm = order == HML_COL_MAJOR;
+  const int lda = std::max(1, cm ? (transA == HML_OP_N ? M : K) : (transA == HML_OP_N ? K : M));
+  const int ldb = std::max(1, cm ? (transB == HML_OP_N ? K : N) : (transB == HML_OP_N ? N : K));
+  const int ldc = std::max(1, cm ? M : N);
+  alignas(16) static float dummy[4];
+  hml_status st = gemm_from_blas(order, transA, transB, M, N, K, 1.0f, dummy, lda, dummy, ldb,
+                                 0.0f, dummy, ldc, &p);
+  if (st != HML_STATUS_SUCCESS) return st;
+  *config = heuristic_config(p, algo);
+  return check_config(p, *config);
+}
+
 hml_status hml_sgemm_config_check(hml_order order, hml_op transA, hml_op transB, int M, int N,
                                   int K, int lda, int ldb, int ldc,
                                   const hml_sgemm_config *config) {
   if (!config) return HML_STATUS_INVALID_VALUE;
-  static float dummy[4];
+  alignas(16) static float dummy[4];
   GemmProblem p;
   hml_status st = gemm_from_blas(order, transA, transB, M, N, K, 1.0f, dummy, lda, dummy, ldb,
                                  0.0f, dummy, ldc, &p);

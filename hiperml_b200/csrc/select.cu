@@ -18,6 +18,7 @@ int simt_num_shapes();
 void simt_shape(int v, int *bm, int *bn, int *wk);
 int tc_num_shapes();
 void tc_shape(int v, int *bm, int *bn);
+bool tc_config_fits(int bn, int ns, int stages);
 
 namespace {
 
@@ -54,7 +55,10 @@ hml_sgemm_config heuristic_config(const GemmProblem &p, int algo) {
       int bm, bn;
       tc_shape(best, &bm, &bn);
       const int64_t tiles = ((p.M + bm - 1) / bm) * static_cast<int64_t>((p.N + bn - 1) / bn);
-      c = {algo, bm, bn, choose_split(tiles, p.K, 1, 256), 4, best};
+      int stages = 2;
+      for (int st : {3, 4, 6})
+        if (tc_config_fits(bn, algo == HML_ALGO_BF16X3 ? 2 : 3, st)) stages = st;
+      c = {algo, bm, bn, choose_split(tiles, p.K, 1, 256), stages, best};
       return c;
     }
   }

@@ -1,28 +1,35 @@
 // sgemm_tc.cu -- split-BF16 SGEMM on the B200 tensor cores (tcgen05 + TMEM).
 //
 // FP32 operands are split into BF16 terms, a = a0 + a1 (+ a2), each term the
-// BF16 rounding of what the previous terms left, and the products that carry
-// FP32-level information are accumulated in FP32 in tensor memory:
-//   BF16X3: a0*b0 + a0*b1 + a1*b0                       (2 planes, 3 MMAs)
-//   BF16X6: a0*b0 + a0*b1 + a1*b0 + a0*b2 + a1*b1 + a2*b0 (3 planes, 6 MMAs)
+// BF16 rounding of what the previous terms left (every residual is exact in
+// FP32), and the products that carry FP32-level information are accumulated
+// in FP32:
+//   BF16X3: a0*b0 + a0*b1 + a1*b0                          (2 planes, 3 MMAs)
+//   BF16X6: a0*b0 + a0*b1 + a1*b0 + a0*b2 + a1*b1 + a2*b0  (3 planes, 6 MMAs)
 // The result is C = alpha * A * B + beta * C in FP32, the reference's
-// hmlSgemm contract (src/hml_sgemm.cu:120-211) with a different machine.
+// hmlSgemm contract (src/hml_sgemm.cu:120-211) on a different machine.
 //
-// Data flow per CTA (one 128-row tile of C, all BN columns, a K range):
+// Data flow of one CTA (a 128-row tile of C, BN columns, a K range):
 //   * B is small (K x N): a pre-pass splits it once into BF16 planes stored
-//     K-contiguous in a workspace ([plane][N_pad][K_pad]); the main kernel
-//     loads plane tiles with TMA straight into the UMMA canonical K-major
-//     128-byte-swizzled layout.
-//   * A is streamed from HBM exactly once: a TMA warp loads 128 x 64 FP32
-//     tiles into a ring; four converter warps split each tile into BF16
-//     planes written in the canonical K-major swizzled layout (a transpose
-//     when A is M-contiguous), then signal the MMA warp.
-//   * one thread of the MMA warp issues tcgen05.mma (M=128, N=BN, K=16,
-//     operands from shared memory, accumulator in TMEM) and releases ring
-//     slots with tcgen05.commit.
-//   * the converter warps then read the accumulator with tcgen05.ld and
-//     apply alpha/beta; with split_k > 1 the CTAs of a cluster sum their
-//     tiles in rank order through distributed shared memory.
+//     K-contiguous in a workspace ([plane][N_pad][K_pad]); the kernel loads
+//     plane tiles with TMA straight into the UMMA canonical K-major layout
+//     (64-byte swizzle, 32 BF16 per row).
+//   * A streams from HBM exactly once: a TMA warp loads 128 x 32 FP32 tiles
+//     into a ring of `stages` slots.
+//   * eight converter warps split each FP32 tile into BF16 planes written in
+//     the same canonical layout (a transpose when A is M-contiguous) into one
+//     of two converted buffers, then signal the MMA warp.
+//   * one thread of the MMA warp issues tcgen05.mma (M=128, N=BN, K=16, both
+//     operands from shared memory, FP32 accumulator in TMEM) and releases
+//     ring slots and buffers with tcgen05.commit.
+//   * the tensor core's FP32 accumulation truncates, so a long accumulation
+//     chain in TMEM loses accuracy as K grows.  Each 64-deep chunk of K is
+//     accumulated into one of two TMEM accumulators; the converter warps then
+//     read it (tcgen05.ld) and add it into FP32 running sums held in
+//     registers (round to nearest) while the tensor core fills the other.
+//   * the converter warps apply alpha/beta from the running sums; with
+//     split_k > 1 the CTAs of one thread-block cluster sum their tiles in
+//     rank order through distributed shared memory.
 // Every wait is bounded (2 s of %globaltimer); on expiry the device error
 // word is set, the CTA skips ahead, frees its TMEM and returns.
 #include <cuda_bf16.h>
@@ -36,15 +43,18 @@
 namespace hml {
 namespace {
 
-constexpr int kBM = 128;  // rows of C per CTA = UMMA M
-constexpr int kBK = 64;   // K per ring stage (one 128-byte BF16 swizzle row)
-constexpr int kConvThreads = 128;
-constexpr int kThreads = 192;  // warps 0-3 convert + epilogue, 4 TMA, 5 MMA
+constexpr int kBM = 128;        // rows of C per CTA = UMMA M
+constexpr int kBK = 32;         // K per ring stage (one 64-byte BF16 swizzle row)
+constexpr int kConvWarps = 8;   // converters + accumulator drain + epilogue
+constexpr int kConvThreads = kConvWarps * 32;
+constexpr int kTmaWarp = kConvWarps, kMmaWarp = kConvWarps + 1;
+constexpr int kThreads = (kConvWarps + 2) * 32;
+constexpr int kChunkK = 64;     // K accumulated in TMEM before an FP32 drain
 
 struct TcShape {
   int bn;
 };
-constexpr TcShape kTcShapes[] = {{16}, {32}, {64}, {128}, {256}};
+constexpr TcShape kTcShapes[] = {{16}, {32}, {64}, {128}};
 constexpr int kNumTcShapes = sizeof(kTcShapes) / sizeof(kTcShapes[0]);
 
 // ------------------------------------------------------------ tcgen05
@@ -85,8 +95,20 @@ __device__ __forceinline__ void mma_commit(uint64_t *bar) {
       : "memory");
 }
 
-// 32 lanes x 16 consecutive 32-bit columns of TMEM into 16 registers.
-__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
+// 32 lanes x 8 / 16 consecutive 32-bit columns of TMEM into registers.
+__device__ __forceinline__ void tmem_ld8(uint32_t taddr, float *v) {
+  uint32_t r[8];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+        "=r"(r[7])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+  for (int i = 0; i < 8; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float *v) {
   uint32_t r[16];
   asm volatile(
       "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, "
@@ -100,12 +122,18 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
   for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
 }
 
-// Shared-memory matrix descriptor: K-major, 128-byte swizzle, rows of 128 B,
-// 8-row atoms 1024 B apart (SBO), descriptor version 1.
-__device__ __forceinline__ uint64_t sw128_desc(uint32_t saddr) {
+// Shared-memory matrix descriptor: K-major, 64-byte swizzle (rows of 64 B),
+// 8-row atoms 512 B apart (stride byte offset), descriptor version 1.
+__device__ __forceinline__ uint64_t sw64_desc(uint32_t saddr) {
   return static_cast<uint64_t>((saddr >> 4) & 0x3FFFu) | (static_cast<uint64_t>(1) << 16) |
-         (static_cast<uint64_t>(1024 >> 4) << 32) | (static_cast<uint64_t>(1) << 46) |
-         (static_cast<uint64_t>(2) << 61);
+         (static_cast<uint64_t>(512 >> 4) << 32) | (static_cast<uint64_t>(1) << 46) |
+         (static_cast<uint64_t>(4) << 61);
+}
+
+// Byte offset of the 16-byte chunk `c` (0..3) of row `r` in a 64-byte-row
+// tile with the 64-byte swizzle (chunk bits 4-5 XOR address bits 7-8).
+__device__ __forceinline__ uint32_t sw64_off(int r, int c) {
+  return static_cast<uint32_t>(r * 64 + ((c ^ ((r >> 1) & 3)) << 4));
 }
 
 // Instruction descriptor: BF16 x BF16 -> F32, both K-major, M = 128, N = bn.
@@ -115,7 +143,6 @@ __host__ __device__ constexpr uint32_t idesc_bf16(int bn) {
 }
 
 // Split x into NS BF16 terms: t0 = bf16(x), t1 = bf16(x - t0), ...
-// (each residual is exact in FP32).
 template <int NS>
 __device__ __forceinline__ void split_bf16(float x, unsigned short (&t)[NS]) {
   float r = x;
@@ -127,13 +154,31 @@ __device__ __forceinline__ void split_bf16(float x, unsigned short (&t)[NS]) {
   }
 }
 
+template <int NS>
+__device__ __forceinline__ void pack8(const float (&x)[8], uint4 (&out)[NS]) {
+  unsigned short t[NS][8];
+#pragma unroll
+  for (int j = 0; j < 8; ++j) {
+    unsigned short sp[NS];
+    split_bf16<NS>(x[j], sp);
+#pragma unroll
+    for (int i = 0; i < NS; ++i) t[i][j] = sp[i];
+  }
+#pragma unroll
+  for (int i = 0; i < NS; ++i) {
+    out[i].x = t[i][0] | (static_cast<uint32_t>(t[i][1]) << 16);
+    out[i].y = t[i][2] | (static_cast<uint32_t>(t[i][3]) << 16);
+    out[i].z = t[i][4] | (static_cast<uint32_t>(t[i][5]) << 16);
+    out[i].w = t[i][6] | (static_cast<uint32_t>(t[i][7]) << 16);
+  }
+}
+
 struct TcArgs {
   GemmProblem p;
-  int split;     // CTAs per cluster along K
-  int kc;        // K extent per split (multiple of kBK)
-  int stages;    // FP32 A ring depth
-  int cbufs;     // converted-A ring depth
-  int n_pad;     // rows of one B plane in the workspace
+  int split;   // CTAs per cluster along K
+  int kc;      // K extent per split (multiple of kChunkK)
+  int stages;  // FP32 A ring depth
+  int n_pad;   // rows of one B plane in the workspace
   int *err;
 };
 
@@ -147,54 +192,55 @@ __global__ void split_b_kernel(const float *B, int64_t sbk, int64_t sbn, int K, 
        c += static_cast<int64_t>(gridDim.x) * blockDim.x) {
     const int n = static_cast<int>(c / (k_pad / 8));
     const int k0 = static_cast<int>(c % (k_pad / 8)) * 8;
-    unsigned short t[NS][8];
+    float x[8];
 #pragma unroll
     for (int j = 0; j < 8; ++j) {
       const int k = k0 + j;
-      const float x = (n < N && k < K) ? B[static_cast<int64_t>(k) * sbk + static_cast<int64_t>(n) * sbn] : 0.0f;
-      unsigned short s[NS];
-      split_bf16<NS>(x, s);
-#pragma unroll
-      for (int i = 0; i < NS; ++i) t[i][j] = s[i];
+      x[j] = (n < N && k < K)
+                 ? B[static_cast<int64_t>(k) * sbk + static_cast<int64_t>(n) * sbn]
+                 : 0.0f;
     }
+    uint4 v[NS];
+    pack8<NS>(x, v);
 #pragma unroll
-    for (int i = 0; i < NS; ++i) {
-      uint4 v;
-      v.x = t[i][0] | (static_cast<uint32_t>(t[i][1]) << 16);
-      v.y = t[i][2] | (static_cast<uint32_t>(t[i][3]) << 16);
-      v.z = t[i][4] | (static_cast<uint32_t>(t[i][5]) << 16);
-      v.w = t[i][6] | (static_cast<uint32_t>(t[i][7]) << 16);
-      *reinterpret_cast<uint4 *>(planes + (static_cast<int64_t>(i) * n_pad + n) * k_pad + k0) = v;
-    }
+    for (int i = 0; i < NS; ++i)
+      *reinterpret_cast<uint4 *>(planes + (static_cast<int64_t>(i) * n_pad + n) * k_pad + k0) =
+          v[i];
   }
 }
 
 // ------------------------------------------------------------- kernel
+// Warps 0-7: convert A, drain the accumulator, epilogue.  Warp 8: TMA.
+// Warp 9: TMEM allocation and MMA issue.
 template <int BN, int NS, bool AK>
 __global__ void __launch_bounds__(kThreads, 1)
     tc_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
               TcArgs args) {
-  constexpr int A32_BYTES = kBM * kBK * 4;          // FP32 A stage (32 KB)
-  constexpr int BPL_BYTES = BN * kBK * 2;           // one B plane tile
+  constexpr int A32_BYTES = kBM * kBK * 4;      // FP32 A slot (16 KB)
+  constexpr int BPL_BYTES = BN * kBK * 2;       // one B plane tile (64 B rows)
   constexpr int STAGE_BYTES = A32_BYTES + NS * BPL_BYTES;
-  constexpr int APL_BYTES = kBM * kBK * 2;          // one converted A plane (16 KB)
+  constexpr int APL_BYTES = kBM * kBK * 2;      // one converted A plane (8 KB)
   constexpr int CBUF_BYTES = NS * APL_BYTES;
-  constexpr uint32_t TMEM_COLS = BN < 32 ? 32 : BN;
+  constexpr int CB = 2;                         // converted-A buffers
+  constexpr int HALF = BN / 2;                  // columns drained per thread
+  constexpr uint32_t TMEM_COLS = 2 * BN < 32 ? 32 : 2 * BN;  // two accumulators
   constexpr uint32_t IDESC = idesc_bf16(BN);
+  constexpr int P = kChunkK / kBK;              // k-blocks per TMEM chunk
 
   extern __shared__ uint8_t smem_raw[];
   uint8_t *smem = reinterpret_cast<uint8_t *>(
       (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~static_cast<uintptr_t>(1023));
   const GemmProblem &p = args.p;
-  const int S = args.stages, CB = args.cbufs;
-  uint8_t *ring = smem;                       // S x STAGE_BYTES
-  uint8_t *cbuf = smem + S * STAGE_BYTES;     // CB x CBUF_BYTES (1024-aligned)
+  const int S = args.stages;
+  uint8_t *ring = smem;                        // S x STAGE_BYTES
+  uint8_t *cbuf = smem + S * STAGE_BYTES;      // CB x CBUF_BYTES (512-aligned)
   uint64_t *full = reinterpret_cast<uint64_t *>(cbuf + CB * CBUF_BYTES);
   uint64_t *empty = full + S;
-  uint64_t *cfull = empty + S;
-  uint64_t *cempty = cfull + CB;
-  uint64_t *accfull = cempty + CB;
-  uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(accfull + 1);
+  uint64_t *cfull = empty + S;    // [CB] converted buffer ready
+  uint64_t *cempty = cfull + CB;  // [CB] converted buffer consumed
+  uint64_t *afull = cempty + CB;  // [2] accumulator holds a finished chunk
+  uint64_t *aempty = afull + 2;   // [2] accumulator drained
+  uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(aempty + 2);
   int *bad_flag = reinterpret_cast<int *>(tmem_slot + 1);
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -205,6 +251,7 @@ __global__ void __launch_bounds__(kThreads, 1)
   const int kbeg = rank * args.kc;
   const int kend = min(p.K, kbeg + args.kc);
   const int nkb = kend > kbeg ? (kend - kbeg + kBK - 1) / kBK : 0;
+  const int nchunks = (nkb + P - 1) / P;
 
   if (tid == 0) {
     for (int s = 0; s < S; ++s) {
@@ -215,17 +262,24 @@ __global__ void __launch_bounds__(kThreads, 1)
       mbar_init(&cfull[c], kConvThreads);
       mbar_init(&cempty[c], 1);
     }
-    mbar_init(accfull, 1);
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(&afull[b], 1);
+      mbar_init(&aempty[b], kConvThreads);
+    }
     *bad_flag = 0;
     fence_mbar_init();
   }
-  if (warp == 5) tmem_alloc(tmem_slot, TMEM_COLS);
+  if (warp == kMmaWarp) tmem_alloc(tmem_slot, TMEM_COLS);
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem = *tmem_slot;
 
-  if (warp == 4) {
+  float sums[HALF];  // converter warps: FP32 running sums, half a row of C
+#pragma unroll
+  for (int i = 0; i < HALF; ++i) sums[i] = 0.0f;
+
+  if (warp == kTmaWarp) {
     // ---------------------------------------------------------- TMA
     if (lane == 0) {
       prefetch_tmap(&tmA);
@@ -239,133 +293,155 @@ __global__ void __launch_bounds__(kThreads, 1)
         uint8_t *st = ring + s * STAGE_BYTES;
         const int k0 = kbeg + kb * kBK;
         mbar_arrive_expect_tx(&full[s], STAGE_BYTES);
-        if (AK) {
-          // two 32-float wide boxes (128-byte swizzle), rows = 128 m
+        if (AK)  // 128 rows of 32 floats (128-byte swizzle)
           tma_load_2d(st, &tmA, &full[s], k0, static_cast<int>(m0));
-          tma_load_2d(st + A32_BYTES / 2, &tmA, &full[s], k0 + 32, static_cast<int>(m0));
-        } else {
+        else     // 32 rows (k) of 128 floats (m)
           tma_load_2d(st, &tmA, &full[s], static_cast<int>(m0), k0);
-        }
 #pragma unroll
         for (int i = 0; i < NS; ++i)
           tma_load_2d(st + A32_BYTES + i * BPL_BYTES, &tmB, &full[s], k0, i * args.n_pad + n0);
       }
     }
-  } else if (warp == 5) {
+  } else if (warp == kMmaWarp) {
     // ---------------------------------------------------------- MMA
     if (lane == 0) {
       for (int kb = 0; kb < nkb; ++kb) {
         const int s = kb % S, c = kb % CB;
-        if (!mbar_wait(&full[s], (kb / S) & 1, args.err, kDevErrFullBarrier) ||
+        const int q = kb / P, b = q & 1;
+        const bool first = (kb % P) == 0;
+        const bool last = (kb % P) == P - 1 || kb == nkb - 1;
+        if ((first &&
+             !mbar_wait(&aempty[b], ((q >> 1) & 1) ^ 1, args.err, kDevErrEmptyBarrier)) ||
+            !mbar_wait(&full[s], (kb / S) & 1, args.err, kDevErrFullBarrier) ||
             !mbar_wait(&cfull[c], (kb / CB) & 1, args.err, kDevErrFullBarrier)) {
           *bad_flag = 1;
           break;
         }
         tc_fence_after();
+        const uint32_t dacc = tmem + static_cast<uint32_t>(b * BN);
         const uint32_t a_base = smem_u32(cbuf + c * CBUF_BYTES);
         const uint32_t b_base = smem_u32(ring + s * STAGE_BYTES + A32_BYTES);
 #pragma unroll
         for (int kk = 0; kk < kBK / 16; ++kk) {
-          // products in increasing magnitude order is not needed: the FP32
-          // accumulator holds every term's 16 leading bits
 #pragma unroll
           for (int i = 0; i < NS; ++i)
 #pragma unroll
             for (int j = 0; j < NS - i; ++j) {
-              const uint64_t ad = sw128_desc(a_base + i * APL_BYTES + kk * 32);
-              const uint64_t bd = sw128_desc(b_base + j * BPL_BYTES + kk * 32);
-              const uint32_t acc = (kb > 0 || kk > 0 || i > 0 || j > 0) ? 1u : 0u;
-              mma_bf16(tmem, ad, bd, IDESC, acc);
+              const uint64_t ad = sw64_desc(a_base + i * APL_BYTES + kk * 32);
+              const uint64_t bd = sw64_desc(b_base + j * BPL_BYTES + kk * 32);
+              const uint32_t acc = (!first || kk > 0 || i > 0 || j > 0) ? 1u : 0u;
+              mma_bf16(dacc, ad, bd, IDESC, acc);
             }
         }
         mma_commit(&empty[s]);
         mma_commit(&cempty[c]);
+        if (last) mma_commit(&afull[b]);
       }
-      mma_commit(accfull);
     }
   } else {
-    // ---------------------------------------------------- converters
-    const int m = tid;  // row of the tile, 0..127
-    for (int kb = 0; kb < nkb; ++kb) {
+    // ------------------------------------- converters / drain (warps 0-7)
+    const int m = tid & (kBM - 1);  // row of the tile
+    const int h = tid >> 7;         // which half of each k-block and of the columns
+    const int quarter = warp & 3;   // TMEM lanes 32*quarter .. +31 == rows of this warp
+    bool ok = true;
+    auto drain = [&](int q) -> bool {
+      const int b = q & 1;
+      bool w = mbar_wait(&afull[b], (q >> 1) & 1, args.err, kDevErrMmaBarrier);
+      w = __all_sync(0xffffffffu, w);  // tcgen05.ld is warp-collective
+      if (!w) return false;
+      tc_fence_after();
+      const uint32_t taddr =
+          tmem + (static_cast<uint32_t>(quarter * 32) << 16) + b * BN + h * HALF;
+      if (HALF >= 16) {
+#pragma unroll
+        for (int nc = 0; nc < HALF; nc += 16) {
+          float v[16];
+          tmem_ld16(taddr + nc, v);
+#pragma unroll
+          for (int i = 0; i < 16; ++i) sums[nc + i] += v[i];
+        }
+      } else {
+        float v[8];
+        tmem_ld8(taddr, v);
+#pragma unroll
+        for (int i = 0; i < HALF; ++i) sums[i] += v[i];
+      }
+      tc_fence_before();
+      mbar_arrive(&aempty[b]);
+      return true;
+    };
+    int drained = 0;
+    for (int kb = 0; kb < nkb && ok; ++kb) {
       const int s = kb % S, c = kb % CB;
       if (!mbar_wait(&full[s], (kb / S) & 1, args.err, kDevErrFullBarrier) ||
           !mbar_wait(&cempty[c], ((kb / CB) & 1) ^ 1, args.err, kDevErrEmptyBarrier)) {
-        *bad_flag = 1;
+        ok = false;
         break;
       }
       const float *a32 = reinterpret_cast<const float *>(ring + s * STAGE_BYTES);
       uint8_t *dst = cbuf + c * CBUF_BYTES;
 #pragma unroll
-      for (int ch = 0; ch < kBK / 8; ++ch) {  // 8 chunks of 8 k values
+      for (int cc = 0; cc < 2; ++cc) {
+        const int ch = 2 * h + cc;  // 8-wide k chunk 0..3
         float x[8];
         if (AK) {
-          // box (ch / 4) holds k in [32*(ch/4), +32): 128-byte rows, swizzled
-          const float *box = a32 + (ch >> 2) * (kBM * 32);
+          // row m holds 32 floats in 128 bytes, 128-byte swizzle
 #pragma unroll
-          for (int h = 0; h < 2; ++h) {
-            const int q = ((ch & 3) * 2 + h) ^ (m & 7);  // 16-byte chunk within the row
-            const float4 v = *reinterpret_cast<const float4 *>(box + m * 32 + q * 4);
-            x[4 * h + 0] = v.x; x[4 * h + 1] = v.y; x[4 * h + 2] = v.z; x[4 * h + 3] = v.w;
+          for (int hh = 0; hh < 2; ++hh) {
+            const int qq = (2 * ch + hh) ^ (m & 7);
+            const float4 v = *reinterpret_cast<const float4 *>(a32 + m * 32 + qq * 4);
+            x[4 * hh + 0] = v.x; x[4 * hh + 1] = v.y; x[4 * hh + 2] = v.z; x[4 * hh + 3] = v.w;
           }
         } else {
 #pragma unroll
           for (int j = 0; j < 8; ++j) x[j] = a32[(ch * 8 + j) * kBM + m];
         }
-        unsigned short t[NS][8];
+        uint4 v[NS];
+        pack8<NS>(x, v);
+        const uint32_t off = sw64_off(m, ch);
 #pragma unroll
-        for (int j = 0; j < 8; ++j) {
-          unsigned short sp[NS];
-          split_bf16<NS>(x[j], sp);
-#pragma unroll
-          for (int i = 0; i < NS; ++i) t[i][j] = sp[i];
-        }
-        const uint32_t off = static_cast<uint32_t>(m * 128 + ((ch ^ (m & 7)) << 4));
-#pragma unroll
-        for (int i = 0; i < NS; ++i) {
-          uint4 v;
-          v.x = t[i][0] | (static_cast<uint32_t>(t[i][1]) << 16);
-          v.y = t[i][2] | (static_cast<uint32_t>(t[i][3]) << 16);
-          v.z = t[i][4] | (static_cast<uint32_t>(t[i][5]) << 16);
-          v.w = t[i][6] | (static_cast<uint32_t>(t[i][7]) << 16);
-          *reinterpret_cast<uint4 *>(dst + i * APL_BYTES + off) = v;
-        }
+        for (int i = 0; i < NS; ++i)
+          *reinterpret_cast<uint4 *>(dst + i * APL_BYTES + off) = v[i];
       }
       fence_proxy_async_smem();  // generic-proxy writes -> tensor-core reads
       mbar_arrive(&cfull[c]);
+      // after the last block of chunk q, drain chunk q-1 (one chunk of slack
+      // so the tensor core never waits for the drain)
+      const bool chunk_end = (kb % P) == P - 1 || kb == nkb - 1;
+      if (chunk_end && kb / P >= 1) {
+        if (!drain(drained)) { ok = false; break; }
+        ++drained;
+      }
     }
+    while (ok && drained < nchunks) {
+      if (!drain(drained)) { ok = false; break; }
+      ++drained;
+    }
+    if (!ok) *bad_flag = 1;
   }
 
   // ---------------------------------------------------------- epilogue
   __syncthreads();
   const bool failed = *bad_flag != 0;
   float *red = reinterpret_cast<float *>(ring);  // [BN][kBM], reuses the ring
-  if (warp < 4) {
-    bool ok = !failed;
-    if (ok && nkb > 0) ok = mbar_wait(accfull, 0, args.err, kDevErrMmaBarrier);
-    ok = __all_sync(0xffffffffu, ok);  // tcgen05.ld is warp-collective
-    tc_fence_after();
-    const int m = warp * 32 + lane;
+  if (warp < kConvWarps) {
+    const int m = tid & (kBM - 1);
+    const int h = tid >> 7;
     const int64_t gm = m0 + m;
-#pragma unroll 1
-    for (int nc = 0; nc < BN; nc += 16) {
-      float v[16];
-      if (ok && nkb > 0) {
-        tmem_ld16(tmem + (static_cast<uint32_t>(warp * 32) << 16) + nc, v);
-      } else {
+    if (failed) {
 #pragma unroll
-        for (int i = 0; i < 16; ++i) v[i] = 0.0f;
-      }
-      if (split > 1) {
+      for (int i = 0; i < HALF; ++i) sums[i] = 0.0f;
+    }
+    if (split > 1) {
 #pragma unroll
-        for (int i = 0; i < 16; ++i) red[(nc + i) * kBM + m] = v[i];
-      } else if (gm < p.M) {
+      for (int i = 0; i < HALF; ++i) red[(h * HALF + i) * kBM + m] = sums[i];
+    } else if (gm < p.M) {
 #pragma unroll
-        for (int i = 0; i < 16; ++i) {
-          const int gn = n0 + nc + i;
-          if (gn < p.N) {
-            float *cp = p.C + gm * p.scm + static_cast<int64_t>(gn) * p.scn;
-            *cp = axpby(p.alpha, v[i], p.beta, cp);
-          }
+      for (int i = 0; i < HALF; ++i) {
+        const int gn = n0 + h * HALF + i;
+        if (gn < p.N) {
+          float *cp = p.C + gm * p.scm + static_cast<int64_t>(gn) * p.scn;
+          *cp = axpby(p.alpha, sums[i], p.beta, cp);
         }
       }
     }
@@ -384,13 +460,13 @@ __global__ void __launch_bounds__(kThreads, 1)
       }
       const float sv[4] = {sum.x, sum.y, sum.z, sum.w};
 #pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        const int mm = (e + q) % kBM, nn = (e + q) / kBM;
+      for (int qq = 0; qq < 4; ++qq) {
+        const int mm = (e + qq) % kBM, nn = (e + qq) / kBM;
         const int64_t gm = m0 + mm;
         const int gn = n0 + nn;
         if (gm < p.M && gn < p.N) {
           float *cp = p.C + gm * p.scm + static_cast<int64_t>(gn) * p.scn;
-          *cp = axpby(p.alpha, sv[q], p.beta, cp);
+          *cp = axpby(p.alpha, sv[qq], p.beta, cp);
         }
       }
     }
@@ -398,30 +474,26 @@ __global__ void __launch_bounds__(kThreads, 1)
   }
   tc_fence_before();
   __syncthreads();
-  if (warp == 5) tmem_dealloc(tmem, TMEM_COLS);
+  if (warp == kMmaWarp) tmem_dealloc(tmem, TMEM_COLS);
 }
 
-size_t tc_smem_bytes(int bn, int ns, int stages, int cbufs) {
+size_t tc_smem_bytes(int bn, int ns, int stages) {
   const size_t stage = static_cast<size_t>(kBM) * kBK * 4 + static_cast<size_t>(ns) * bn * kBK * 2;
   const size_t cb = static_cast<size_t>(ns) * kBM * kBK * 2;
-  return 1024 + stages * stage + cbufs * cb + 8 * (2 * stages + 2 * cbufs + 1) + 16;
+  return 1024 + stages * stage + 2 * cb + 8 * (2 * stages + 2 * 2 + 4) + 16;
 }
 
 }  // namespace
 
 bool tc_config_fits(int bn, int ns, int stages) {
-  return tc_smem_bytes(bn, ns, stages, 1) <= 227 * 1024;
+  return tc_smem_bytes(bn, ns, stages) <= 227 * 1024;
 }
 
 namespace {
 
-int pick_cbufs(int bn, int ns, int stages) {
-  return tc_smem_bytes(bn, ns, stages, 2) <= 227 * 1024 ? 2 : 1;
-}
-
 template <int BN, int NS, bool AK>
 hml_status run_tc(const GemmProblem &p, const hml_sgemm_config &c, cudaStream_t s) {
-  const int k_pad = ((p.K + kBK - 1) / kBK) * kBK;
+  const int k_pad = ((p.K + kChunkK - 1) / kChunkK) * kChunkK;
   const int n_pad = ((p.N + BN - 1) / BN) * BN;
   // B planes in the stream's workspace
   const size_t plane_bytes = static_cast<size_t>(n_pad) * k_pad * 2;
@@ -445,7 +517,7 @@ hml_status run_tc(const GemmProblem &p, const hml_sgemm_config &c, cudaStream_t 
   memset(&tb, 0, sizeof tb);
   bool ok;
   if (AK)
-    ok = tensor_map_2d(&ta, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, p.A, p.K, p.M, p.sam * 4, 32, kBM,
+    ok = tensor_map_2d(&ta, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, p.A, p.K, p.M, p.sam * 4, kBK, kBM,
                        CU_TENSOR_MAP_SWIZZLE_128B);
   else
     ok = tensor_map_2d(&ta, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, p.A, p.M, p.K, p.sak * 4, kBM, kBK,
@@ -453,18 +525,17 @@ hml_status run_tc(const GemmProblem &p, const hml_sgemm_config &c, cudaStream_t 
   if (ok)
     ok = tensor_map_2d(&tb, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, planes, k_pad,
                        static_cast<uint64_t>(NS) * n_pad, static_cast<uint64_t>(k_pad) * 2, kBK, BN,
-                       CU_TENSOR_MAP_SWIZZLE_128B);
+                       CU_TENSOR_MAP_SWIZZLE_64B);
   if (!ok) return HML_STATUS_CUDA_ERROR;
   TcArgs args;
   args.p = p;
   args.split = c.split_k;
-  const int kblocks = k_pad / kBK;
-  args.kc = ((kblocks + c.split_k - 1) / c.split_k) * kBK;
+  const int kchunks = k_pad / kChunkK;
+  args.kc = ((kchunks + c.split_k - 1) / c.split_k) * kChunkK;
   args.stages = c.stages;
-  args.cbufs = pick_cbufs(BN, NS, c.stages);
   args.n_pad = n_pad;
   args.err = device_error_word();
-  const size_t smem = tc_smem_bytes(BN, NS, c.stages, args.cbufs);
+  const size_t smem = tc_smem_bytes(BN, NS, c.stages);
   auto kern = tc_kernel<BN, NS, AK>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        static_cast<int>(smem));
@@ -495,7 +566,6 @@ hml_status run_tc_ns(const GemmProblem &p, const hml_sgemm_config &c, cudaStream
     case 32: return run_tc_layout<32, NS>(p, c, s);
     case 64: return run_tc_layout<64, NS>(p, c, s);
     case 128: return run_tc_layout<128, NS>(p, c, s);
-    case 256: return run_tc_layout<256, NS>(p, c, s);
     default: return HML_STATUS_INVALID_VALUE;
   }
 }
@@ -516,9 +586,9 @@ hml_status check_tc(const GemmProblem &p, const hml_sgemm_config &c) {
   if (c.tile_m != kBM || c.tile_n != kTcShapes[c.variant].bn) return HML_STATUS_INVALID_VALUE;
   if (c.split_k < 1 || c.split_k > 16 || (c.split_k & (c.split_k - 1)) != 0)
     return HML_STATUS_INVALID_VALUE;
-  if (c.stages < 2 || c.stages > 4) return HML_STATUS_INVALID_VALUE;
+  if (c.stages < 2 || c.stages > 8) return HML_STATUS_INVALID_VALUE;
   const int ns = c.algo == HML_ALGO_BF16X3 ? 2 : 3;
-  if (tc_smem_bytes(c.tile_n, ns, c.stages, 1) > 227 * 1024) return HML_STATUS_INVALID_VALUE;
+  if (!tc_config_fits(c.tile_n, ns, c.stages)) return HML_STATUS_INVALID_VALUE;
   // the ring is reused for the split-K partial tile
   if (c.split_k > 1 &&
       static_cast<size_t>(kBM) * c.tile_n * 4 >

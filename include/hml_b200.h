@@ -95,6 +95,13 @@ hml_status hml_sgemm_ex_config(hml_order order, hml_op transA, hml_op transB,
 hml_status hml_sgemm_select(hml_order order, hml_op transA, hml_op transB,
                             int M, int N, int K, hml_sgemm_config *config);
 
+/* The heuristic configuration of one algorithm family for this problem
+ * (HML_ALGO_AUTO: same as hml_sgemm_select).  Returns the status of
+ * hml_sgemm_config_check for dense leading dimensions. */
+hml_status hml_sgemm_select_algo(hml_order order, hml_op transA, hml_op transB,
+                                 int M, int N, int K, int algo,
+                                 hml_sgemm_config *config);
+
 /* Whether a configuration can run this problem (status only, no launch). */
 hml_status hml_sgemm_config_check(hml_order order, hml_op transA, hml_op transB,
                                   int M, int N, int K, int lda, int ldb, int ldc,
