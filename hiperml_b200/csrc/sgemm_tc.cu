@@ -14,9 +14,11 @@
 //     K-contiguous in a workspace ([plane][N_pad][K_pad]); the kernel loads
 //     plane tiles with TMA straight into the UMMA canonical K-major layout
 //     (64-byte swizzle, 32 BF16 per row).
-//   * A streams from HBM exactly once: a TMA warp loads 128 x 32 FP32 tiles
-//     into a ring of `stages` slots.
-//   * eight converter warps split each FP32 tile into BF16 planes written in
+//   * A streams from HBM exactly once: a TMA thread loads 128 x 32 FP32 tiles
+//     into a ring of `stages` slots, each released as soon as the converter
+//     warps have read it (B tiles live in a separate ring released by the
+//     MMAs, so HBM latency is hidden by the A ring alone).
+//   * sixteen converter warps split each FP32 tile into BF16 planes written in
 //     the same canonical layout (a transpose when A is M-contiguous) into one
 //     of two converted buffers, then signal the MMA warp.
 //   * one thread of the MMA warp issues tcgen05.mma (M=128, N=BN, K=16, both
@@ -45,10 +47,9 @@ namespace {
 
 constexpr int kBM = 128;        // rows of C per CTA = UMMA M
 constexpr int kBK = 32;         // K per ring stage (one 64-byte BF16 swizzle row)
-constexpr int kConvWarps = 8;   // converters + accumulator drain + epilogue
-constexpr int kConvThreads = kConvWarps * 32;
-constexpr int kTmaWarp = kConvWarps, kMmaWarp = kConvWarps + 1;
-constexpr int kThreads = (kConvWarps + 2) * 32;
+constexpr int kConvWarps = 16;  // converters + accumulator drain + epilogue
+constexpr int kLoadAWarp = kConvWarps, kLoadBWarp = kConvWarps + 1, kMmaWarp = kConvWarps + 2;
+constexpr int kThreads = (kConvWarps + 3) * 32;
 constexpr int kChunkK = 64;     // K accumulated in TMEM before an FP32 drain
 
 struct TcShape {
@@ -95,7 +96,17 @@ __device__ __forceinline__ void mma_commit(uint64_t *bar) {
       : "memory");
 }
 
-// 32 lanes x 8 / 16 consecutive 32-bit columns of TMEM into registers.
+// 32 lanes x 4 / 8 / 16 consecutive 32-bit columns of TMEM into registers.
+__device__ __forceinline__ void tmem_ld4(uint32_t taddr, float *v) {
+  uint32_t r[4];
+  asm volatile("tcgen05.ld.sync.aligned.32x32b.x4.b32 {%0, %1, %2, %3}, [%4];"
+               : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
+               : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+  for (int i = 0; i < 4; ++i) v[i] = __uint_as_float(r[i]);
+}
+
 __device__ __forceinline__ void tmem_ld8(uint32_t taddr, float *v) {
   uint32_t r[8];
   asm volatile(
@@ -142,43 +153,41 @@ __host__ __device__ constexpr uint32_t idesc_bf16(int bn) {
          (static_cast<uint32_t>(kBM >> 4) << 24);
 }
 
-// Split x into NS BF16 terms: t0 = bf16(x), t1 = bf16(x - t0), ...
-template <int NS>
-__device__ __forceinline__ void split_bf16(float x, unsigned short (&t)[NS]) {
-  float r = x;
-#pragma unroll
-  for (int i = 0; i < NS; ++i) {
-    const __nv_bfloat16 h = __float2bfloat16_rn(r);
-    t[i] = __bfloat16_as_ushort(h);
-    r = r - __bfloat162float(h);
-  }
+// Split eight floats into NS BF16 planes, t0 = bf16(x), t1 = bf16(x - t0),
+// ... (each residual is exact in FP32), packed two per 32-bit word with
+// cvt.rn.bf16x2.f32.
+__device__ __forceinline__ uint32_t bf16x2_rn(float lo, float hi) {
+  uint32_t r;
+  asm("cvt.rn.bf16x2.f32 %0, %1, %2;" : "=r"(r) : "f"(hi), "f"(lo));
+  return r;
 }
 
 template <int NS>
 __device__ __forceinline__ void pack8(const float (&x)[8], uint4 (&out)[NS]) {
-  unsigned short t[NS][8];
+  uint32_t w[NS][4];
 #pragma unroll
-  for (int j = 0; j < 8; ++j) {
-    unsigned short sp[NS];
-    split_bf16<NS>(x[j], sp);
+  for (int j = 0; j < 4; ++j) {
+    float a = x[2 * j], b = x[2 * j + 1];
 #pragma unroll
-    for (int i = 0; i < NS; ++i) t[i][j] = sp[i];
+    for (int i = 0; i < NS; ++i) {
+      const uint32_t t = bf16x2_rn(a, b);
+      w[i][j] = t;
+      if (i + 1 < NS) {
+        a -= __uint_as_float(t << 16);
+        b -= __uint_as_float(t & 0xFFFF0000u);
+      }
+    }
   }
 #pragma unroll
-  for (int i = 0; i < NS; ++i) {
-    out[i].x = t[i][0] | (static_cast<uint32_t>(t[i][1]) << 16);
-    out[i].y = t[i][2] | (static_cast<uint32_t>(t[i][3]) << 16);
-    out[i].z = t[i][4] | (static_cast<uint32_t>(t[i][5]) << 16);
-    out[i].w = t[i][6] | (static_cast<uint32_t>(t[i][7]) << 16);
-  }
+  for (int i = 0; i < NS; ++i) out[i] = make_uint4(w[i][0], w[i][1], w[i][2], w[i][3]);
 }
 
 struct TcArgs {
   GemmProblem p;
-  int split;   // CTAs per cluster along K
-  int kc;      // K extent per split (multiple of kChunkK)
-  int stages;  // FP32 A ring depth
-  int n_pad;   // rows of one B plane in the workspace
+  int split;       // CTAs per cluster along K
+  int kc;          // K extent per split (multiple of kChunkK)
+  int sa, so;      // A ring and operand ring depths
+  int n_pad;       // rows of one B plane in the workspace
   int *err;
 };
 
@@ -210,37 +219,71 @@ __global__ void split_b_kernel(const float *B, int64_t sbk, int64_t sbn, int K, 
 }
 
 // ------------------------------------------------------------- kernel
-// Warps 0-7: convert A, drain the accumulator, epilogue.  Warp 8: TMA.
-// Warp 9: TMEM allocation and MMA issue.
+// Shared-memory plan of one CTA (all tiles 1024-byte aligned):
+//   A ring        sa slots of the FP32 A tile (16 KB), filled by TMA and
+//                 released by the converter warps as soon as they have read
+//                 it, so HBM latency is covered by this ring alone;
+//   operand ring  so slots, each holding the NS B-plane tiles of one K block
+//                 (filled by TMA) and the NS converted A planes of the same
+//                 block (written by the converter warps).  One tcgen05.commit
+//                 releases a whole slot: the MMA thread's issue rate (about
+//                 30 ns a tcgen05.mma, 70 ns a tcgen05.commit) bounds the
+//                 kernel for skinny N, so commits are kept to one per block.
+struct TcPlan {
+  int sa, so;
+};
+
+__host__ __device__ constexpr size_t tc_a_bytes() { return static_cast<size_t>(kBM) * kBK * 4; }
+__host__ __device__ constexpr size_t tc_op_bytes(int bn, int ns) {
+  return static_cast<size_t>(ns) * bn * kBK * 2 + static_cast<size_t>(ns) * kBM * kBK * 2;
+}
+size_t tc_plan_bytes(int bn, int ns, const TcPlan &pl) {
+  return 1024 + pl.sa * tc_a_bytes() + pl.so * tc_op_bytes(bn, ns) + 8 * (2 * pl.sa + 2 * pl.so + 4) +
+         16;
+}
+
+// The deepest operand ring (2..6 slots) that fits next to sa A slots.
+bool tc_plan(int bn, int ns, int sa, TcPlan *out) {
+  for (int so = 6; so >= 2; --so) {
+    const TcPlan pl = {sa, so};
+    if (tc_plan_bytes(bn, ns, pl) <= 227 * 1024) {
+      *out = pl;
+      return true;
+    }
+  }
+  return false;
+}
+
+// Warps 0-15: convert A, drain the accumulator, epilogue.  Warp 16 loads A,
+// warp 17 loads B (separate warps, so a load waiting on the MMA pipeline
+// never holds back the HBM stream), warp 18 allocates TMEM and issues MMAs.
 template <int BN, int NS, bool AK>
 __global__ void __launch_bounds__(kThreads, 1)
     tc_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
               TcArgs args) {
-  constexpr int A32_BYTES = kBM * kBK * 4;      // FP32 A slot (16 KB)
-  constexpr int BPL_BYTES = BN * kBK * 2;       // one B plane tile (64 B rows)
-  constexpr int STAGE_BYTES = A32_BYTES + NS * BPL_BYTES;
-  constexpr int APL_BYTES = kBM * kBK * 2;      // one converted A plane (8 KB)
-  constexpr int CBUF_BYTES = NS * APL_BYTES;
-  constexpr int CB = 2;                         // converted-A buffers
-  constexpr int HALF = BN / 2;                  // columns drained per thread
+  constexpr int A32_BYTES = static_cast<int>(tc_a_bytes());  // FP32 A slot (16 KB)
+  constexpr int BPL_BYTES = BN * kBK * 2;                    // one B plane tile
+  constexpr int APL_BYTES = kBM * kBK * 2;                   // one converted A plane (8 KB)
+  constexpr int OP_BYTES = NS * (BPL_BYTES + APL_BYTES);     // one operand slot
+  constexpr int QTR = BN / 4;                                // columns drained per thread
   constexpr uint32_t TMEM_COLS = 2 * BN < 32 ? 32 : 2 * BN;  // two accumulators
   constexpr uint32_t IDESC = idesc_bf16(BN);
-  constexpr int P = kChunkK / kBK;              // k-blocks per TMEM chunk
+  constexpr int P = kChunkK / kBK;                           // k-blocks per TMEM chunk
 
   extern __shared__ uint8_t smem_raw[];
   uint8_t *smem = reinterpret_cast<uint8_t *>(
       (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~static_cast<uintptr_t>(1023));
   const GemmProblem &p = args.p;
-  const int S = args.stages;
-  uint8_t *ring = smem;                        // S x STAGE_BYTES
-  uint8_t *cbuf = smem + S * STAGE_BYTES;      // CB x CBUF_BYTES (512-aligned)
-  uint64_t *full = reinterpret_cast<uint64_t *>(cbuf + CB * CBUF_BYTES);
-  uint64_t *empty = full + S;
-  uint64_t *cfull = empty + S;    // [CB] converted buffer ready
-  uint64_t *cempty = cfull + CB;  // [CB] converted buffer consumed
-  uint64_t *afull = cempty + CB;  // [2] accumulator holds a finished chunk
-  uint64_t *aempty = afull + 2;   // [2] accumulator drained
-  uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(aempty + 2);
+  const int SA = args.sa, SO = args.so;
+  uint8_t *aring = smem;
+  uint8_t *opring = aring + SA * A32_BYTES;  // slot: [A planes][B planes]
+  uint64_t *afull32 = reinterpret_cast<uint64_t *>(opring + SO * OP_BYTES);  // [SA]
+  uint64_t *aempty32 = afull32 + SA;                                         // [SA]
+  uint64_t *opfull = aempty32 + SA;  // [SO] B planes landed and A planes written
+  uint64_t *opempty = opfull + SO;   // [SO] the MMAs reading the slot are done
+  uint64_t *tfull = opempty + SO;    // [2] TMEM accumulator holds a finished chunk
+  uint64_t *tempty = tfull + 2;      // [2] TMEM accumulator drained
+  uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(tempty + 2);
   int *bad_flag = reinterpret_cast<int *>(tmem_slot + 1);
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -254,17 +297,17 @@ __global__ void __launch_bounds__(kThreads, 1)
   const int nchunks = (nkb + P - 1) / P;
 
   if (tid == 0) {
-    for (int s = 0; s < S; ++s) {
-      mbar_init(&full[s], 1);
-      mbar_init(&empty[s], 1);
+    for (int s = 0; s < SA; ++s) {
+      mbar_init(&afull32[s], 1);
+      mbar_init(&aempty32[s], kConvWarps);
     }
-    for (int c = 0; c < CB; ++c) {
-      mbar_init(&cfull[c], kConvThreads);
-      mbar_init(&cempty[c], 1);
+    for (int o = 0; o < SO; ++o) {
+      mbar_init(&opfull[o], kConvWarps + 1);  // converter warps + the B loader
+      mbar_init(&opempty[o], 1);
     }
     for (int b = 0; b < 2; ++b) {
-      mbar_init(&afull[b], 1);
-      mbar_init(&aempty[b], kConvThreads);
+      mbar_init(&tfull[b], 1);
+      mbar_init(&tempty[b], kConvWarps);
     }
     *bad_flag = 0;
     fence_mbar_init();
@@ -275,136 +318,164 @@ __global__ void __launch_bounds__(kThreads, 1)
   tc_fence_after();
   const uint32_t tmem = *tmem_slot;
 
-  float sums[HALF];  // converter warps: FP32 running sums, half a row of C
+  float sums[QTR];  // converter warps: FP32 running sums, a quarter row of C
 #pragma unroll
-  for (int i = 0; i < HALF; ++i) sums[i] = 0.0f;
+  for (int i = 0; i < QTR; ++i) sums[i] = 0.0f;
 
-  if (warp == kTmaWarp) {
-    // ---------------------------------------------------------- TMA
+  if (warp == kLoadAWarp) {
+    // -------------------------------------------------------- TMA, A
     if (lane == 0) {
       prefetch_tmap(&tmA);
-      prefetch_tmap(&tmB);
       for (int kb = 0; kb < nkb; ++kb) {
-        const int s = kb % S;
-        if (!mbar_wait(&empty[s], ((kb / S) & 1) ^ 1, args.err, kDevErrEmptyBarrier)) {
+        const int s = kb % SA;
+        if (!mbar_wait(&aempty32[s], ((kb / SA) & 1) ^ 1, args.err, kDevErrEmptyBarrier)) {
           *bad_flag = 1;
           break;
         }
-        uint8_t *st = ring + s * STAGE_BYTES;
+        uint8_t *dst = aring + s * A32_BYTES;
         const int k0 = kbeg + kb * kBK;
-        mbar_arrive_expect_tx(&full[s], STAGE_BYTES);
+        mbar_arrive_expect_tx(&afull32[s], A32_BYTES);
         if (AK)  // 128 rows of 32 floats (128-byte swizzle)
-          tma_load_2d(st, &tmA, &full[s], k0, static_cast<int>(m0));
+          tma_load_2d(dst, &tmA, &afull32[s], k0, static_cast<int>(m0));
         else     // 32 rows (k) of 128 floats (m)
-          tma_load_2d(st, &tmA, &full[s], static_cast<int>(m0), k0);
+          tma_load_2d(dst, &tmA, &afull32[s], static_cast<int>(m0), k0);
+      }
+    }
+  } else if (warp == kLoadBWarp) {
+    // -------------------------------------------------------- TMA, B
+    if (lane == 0) {
+      prefetch_tmap(&tmB);
+      for (int kb = 0; kb < nkb; ++kb) {
+        const int o = kb % SO;
+        if (!mbar_wait(&opempty[o], ((kb / SO) & 1) ^ 1, args.err, kDevErrEmptyBarrier)) {
+          *bad_flag = 1;
+          break;
+        }
+        uint8_t *dst = opring + o * OP_BYTES + NS * APL_BYTES;
+        const int k0 = kbeg + kb * kBK;
+        mbar_arrive_expect_tx(&opfull[o], NS * BPL_BYTES);
 #pragma unroll
         for (int i = 0; i < NS; ++i)
-          tma_load_2d(st + A32_BYTES + i * BPL_BYTES, &tmB, &full[s], k0, i * args.n_pad + n0);
+          tma_load_2d(dst + i * BPL_BYTES, &tmB, &opfull[o], k0, i * args.n_pad + n0);
       }
     }
   } else if (warp == kMmaWarp) {
     // ---------------------------------------------------------- MMA
     if (lane == 0) {
       for (int kb = 0; kb < nkb; ++kb) {
-        const int s = kb % S, c = kb % CB;
+        const int o = kb % SO;
         const int q = kb / P, b = q & 1;
         const bool first = (kb % P) == 0;
         const bool last = (kb % P) == P - 1 || kb == nkb - 1;
         if ((first &&
-             !mbar_wait(&aempty[b], ((q >> 1) & 1) ^ 1, args.err, kDevErrEmptyBarrier)) ||
-            !mbar_wait(&full[s], (kb / S) & 1, args.err, kDevErrFullBarrier) ||
-            !mbar_wait(&cfull[c], (kb / CB) & 1, args.err, kDevErrFullBarrier)) {
+             !mbar_wait(&tempty[b], ((q >> 1) & 1) ^ 1, args.err, kDevErrEmptyBarrier)) ||
+            !mbar_wait(&opfull[o], (kb / SO) & 1, args.err, kDevErrFullBarrier)) {
           *bad_flag = 1;
           break;
         }
         tc_fence_after();
         const uint32_t dacc = tmem + static_cast<uint32_t>(b * BN);
-        const uint32_t a_base = smem_u32(cbuf + c * CBUF_BYTES);
-        const uint32_t b_base = smem_u32(ring + s * STAGE_BYTES + A32_BYTES);
+        const uint64_t a_desc = sw64_desc(smem_u32(opring + o * OP_BYTES));
+        const uint64_t b_desc = sw64_desc(smem_u32(opring + o * OP_BYTES + NS * APL_BYTES));
 #pragma unroll
         for (int kk = 0; kk < kBK / 16; ++kk) {
 #pragma unroll
           for (int i = 0; i < NS; ++i)
 #pragma unroll
             for (int j = 0; j < NS - i; ++j) {
-              const uint64_t ad = sw64_desc(a_base + i * APL_BYTES + kk * 32);
-              const uint64_t bd = sw64_desc(b_base + j * BPL_BYTES + kk * 32);
+              // descriptor start addresses count 16-byte units
+              const uint64_t ad = a_desc + static_cast<uint64_t>((i * APL_BYTES + kk * 32) >> 4);
+              const uint64_t bd = b_desc + static_cast<uint64_t>((j * BPL_BYTES + kk * 32) >> 4);
               const uint32_t acc = (!first || kk > 0 || i > 0 || j > 0) ? 1u : 0u;
               mma_bf16(dacc, ad, bd, IDESC, acc);
             }
         }
-        mma_commit(&empty[s]);
-        mma_commit(&cempty[c]);
-        if (last) mma_commit(&afull[b]);
+        mma_commit(&opempty[o]);
+        if (last) mma_commit(&tfull[b]);
       }
     }
   } else {
-    // ------------------------------------- converters / drain (warps 0-7)
-    const int m = tid & (kBM - 1);  // row of the tile
-    const int h = tid >> 7;         // which half of each k-block and of the columns
+    // ------------------------------------ converters / drain (warps 0-15)
+    const int m = tid & (kBM - 1);  // row of the tile == TMEM lane
+    const int g = tid >> 7;         // 8-wide k chunk of each block, column quarter
     const int quarter = warp & 3;   // TMEM lanes 32*quarter .. +31 == rows of this warp
     bool ok = true;
     auto drain = [&](int q) -> bool {
       const int b = q & 1;
-      bool w = mbar_wait(&afull[b], (q >> 1) & 1, args.err, kDevErrMmaBarrier);
+      bool w = mbar_wait(&tfull[b], (q >> 1) & 1, args.err, kDevErrMmaBarrier);
       w = __all_sync(0xffffffffu, w);  // tcgen05.ld is warp-collective
       if (!w) return false;
       tc_fence_after();
       const uint32_t taddr =
-          tmem + (static_cast<uint32_t>(quarter * 32) << 16) + b * BN + h * HALF;
-      if (HALF >= 16) {
+          tmem + (static_cast<uint32_t>(quarter * 32) << 16) + b * BN + g * QTR;
+      if (QTR >= 16) {
 #pragma unroll
-        for (int nc = 0; nc < HALF; nc += 16) {
+        for (int nc = 0; nc < QTR; nc += 16) {
           float v[16];
           tmem_ld16(taddr + nc, v);
 #pragma unroll
           for (int i = 0; i < 16; ++i) sums[nc + i] += v[i];
         }
-      } else {
+      } else if (QTR == 8) {
         float v[8];
         tmem_ld8(taddr, v);
 #pragma unroll
-        for (int i = 0; i < HALF; ++i) sums[i] += v[i];
+        for (int i = 0; i < 8; ++i) sums[i] += v[i];
+      } else {
+        float v[4];
+        tmem_ld4(taddr, v);
+#pragma unroll
+        for (int i = 0; i < 4; ++i) sums[i] += v[i];
       }
       tc_fence_before();
-      mbar_arrive(&aempty[b]);
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&tempty[b]);
       return true;
     };
     int drained = 0;
     for (int kb = 0; kb < nkb && ok; ++kb) {
-      const int s = kb % S, c = kb % CB;
-      if (!mbar_wait(&full[s], (kb / S) & 1, args.err, kDevErrFullBarrier) ||
-          !mbar_wait(&cempty[c], ((kb / CB) & 1) ^ 1, args.err, kDevErrEmptyBarrier)) {
+      const int s = kb % SA, o = kb % SO;
+      // 1. the FP32 tile: read this thread's eight values and release the
+      //    slot at once, so the HBM stream never waits for the MMA pipeline
+      bool w = mbar_wait(&afull32[s], (kb / SA) & 1, args.err, kDevErrFullBarrier);
+      if (!__all_sync(0xffffffffu, w)) {
         ok = false;
         break;
       }
-      const float *a32 = reinterpret_cast<const float *>(ring + s * STAGE_BYTES);
-      uint8_t *dst = cbuf + c * CBUF_BYTES;
+      const float *a32 = reinterpret_cast<const float *>(aring + s * A32_BYTES);
+      float x[8];
+      if (AK) {
+        // row m holds 32 floats in 128 bytes, 128-byte swizzle
 #pragma unroll
-      for (int cc = 0; cc < 2; ++cc) {
-        const int ch = 2 * h + cc;  // 8-wide k chunk 0..3
-        float x[8];
-        if (AK) {
-          // row m holds 32 floats in 128 bytes, 128-byte swizzle
-#pragma unroll
-          for (int hh = 0; hh < 2; ++hh) {
-            const int qq = (2 * ch + hh) ^ (m & 7);
-            const float4 v = *reinterpret_cast<const float4 *>(a32 + m * 32 + qq * 4);
-            x[4 * hh + 0] = v.x; x[4 * hh + 1] = v.y; x[4 * hh + 2] = v.z; x[4 * hh + 3] = v.w;
-          }
-        } else {
-#pragma unroll
-          for (int j = 0; j < 8; ++j) x[j] = a32[(ch * 8 + j) * kBM + m];
+        for (int hh = 0; hh < 2; ++hh) {
+          const int qq = (2 * g + hh) ^ (m & 7);
+          const float4 v = *reinterpret_cast<const float4 *>(a32 + m * 32 + qq * 4);
+          x[4 * hh + 0] = v.x; x[4 * hh + 1] = v.y; x[4 * hh + 2] = v.z; x[4 * hh + 3] = v.w;
         }
-        uint4 v[NS];
-        pack8<NS>(x, v);
-        const uint32_t off = sw64_off(m, ch);
+      } else {
 #pragma unroll
-        for (int i = 0; i < NS; ++i)
-          *reinterpret_cast<uint4 *>(dst + i * APL_BYTES + off) = v[i];
+        for (int j = 0; j < 8; ++j) x[j] = a32[(g * 8 + j) * kBM + m];
       }
+      // consume the values before the warp releases the slot: one lane
+      // arrives for the warp, and __syncwarp alone does not wait for the
+      // other lanes' shared-memory loads to return
+      uint4 v[NS];
+      pack8<NS>(x, v);
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&aempty32[s]);
+      // 2. the operand slot: wait until the MMAs that read it are done
+      w = mbar_wait(&opempty[o], ((kb / SO) & 1) ^ 1, args.err, kDevErrEmptyBarrier);
+      if (!__all_sync(0xffffffffu, w)) {
+        ok = false;
+        break;
+      }
+      uint8_t *dst = opring + o * OP_BYTES;
+      const uint32_t off = sw64_off(m, g);
+#pragma unroll
+      for (int i = 0; i < NS; ++i) *reinterpret_cast<uint4 *>(dst + i * APL_BYTES + off) = v[i];
       fence_proxy_async_smem();  // generic-proxy writes -> tensor-core reads
-      mbar_arrive(&cfull[c]);
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&opfull[o]);
       // after the last block of chunk q, drain chunk q-1 (one chunk of slack
       // so the tensor core never waits for the drain)
       const bool chunk_end = (kb % P) == P - 1 || kb == nkb - 1;
@@ -423,22 +494,22 @@ __global__ void __launch_bounds__(kThreads, 1)
   // ---------------------------------------------------------- epilogue
   __syncthreads();
   const bool failed = *bad_flag != 0;
-  float *red = reinterpret_cast<float *>(ring);  // [BN][kBM], reuses the ring
+  float *red = reinterpret_cast<float *>(smem);  // [BN][kBM], reuses the rings
   if (warp < kConvWarps) {
     const int m = tid & (kBM - 1);
-    const int h = tid >> 7;
+    const int g = tid >> 7;
     const int64_t gm = m0 + m;
     if (failed) {
 #pragma unroll
-      for (int i = 0; i < HALF; ++i) sums[i] = 0.0f;
+      for (int i = 0; i < QTR; ++i) sums[i] = 0.0f;
     }
     if (split > 1) {
 #pragma unroll
-      for (int i = 0; i < HALF; ++i) red[(h * HALF + i) * kBM + m] = sums[i];
+      for (int i = 0; i < QTR; ++i) red[(g * QTR + i) * kBM + m] = sums[i];
     } else if (gm < p.M) {
 #pragma unroll
-      for (int i = 0; i < HALF; ++i) {
-        const int gn = n0 + h * HALF + i;
+      for (int i = 0; i < QTR; ++i) {
+        const int gn = n0 + g * QTR + i;
         if (gn < p.N) {
           float *cp = p.C + gm * p.scm + static_cast<int64_t>(gn) * p.scn;
           *cp = axpby(p.alpha, sums[i], p.beta, cp);
@@ -477,16 +548,11 @@ __global__ void __launch_bounds__(kThreads, 1)
   if (warp == kMmaWarp) tmem_dealloc(tmem, TMEM_COLS);
 }
 
-size_t tc_smem_bytes(int bn, int ns, int stages) {
-  const size_t stage = static_cast<size_t>(kBM) * kBK * 4 + static_cast<size_t>(ns) * bn * kBK * 2;
-  const size_t cb = static_cast<size_t>(ns) * kBM * kBK * 2;
-  return 1024 + stages * stage + 2 * cb + 8 * (2 * stages + 2 * 2 + 4) + 16;
-}
-
 }  // namespace
 
 bool tc_config_fits(int bn, int ns, int stages) {
-  return tc_smem_bytes(bn, ns, stages) <= 227 * 1024;
+  TcPlan pl;
+  return tc_plan(bn, ns, stages, &pl);
 }
 
 namespace {
@@ -532,10 +598,13 @@ hml_status run_tc(const GemmProblem &p, const hml_sgemm_config &c, cudaStream_t 
   args.split = c.split_k;
   const int kchunks = k_pad / kChunkK;
   args.kc = ((kchunks + c.split_k - 1) / c.split_k) * kChunkK;
-  args.stages = c.stages;
+  TcPlan plan;
+  if (!tc_plan(BN, NS, c.stages, &plan)) return HML_STATUS_INVALID_VALUE;
+  args.sa = plan.sa;
+  args.so = plan.so;
   args.n_pad = n_pad;
   args.err = device_error_word();
-  const size_t smem = tc_smem_bytes(BN, NS, c.stages);
+  const size_t smem = tc_plan_bytes(BN, NS, plan);
   auto kern = tc_kernel<BN, NS, AK>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        static_cast<int>(smem));
@@ -589,10 +658,9 @@ hml_status check_tc(const GemmProblem &p, const hml_sgemm_config &c) {
   if (c.stages < 2 || c.stages > 8) return HML_STATUS_INVALID_VALUE;
   const int ns = c.algo == HML_ALGO_BF16X3 ? 2 : 3;
   if (!tc_config_fits(c.tile_n, ns, c.stages)) return HML_STATUS_INVALID_VALUE;
-  // the ring is reused for the split-K partial tile
+  // the rings are reused for the split-K partial tile
   if (c.split_k > 1 &&
-      static_cast<size_t>(kBM) * c.tile_n * 4 >
-          static_cast<size_t>(c.stages) * (kBM * kBK * 4 + ns * c.tile_n * kBK * 2))
+      static_cast<size_t>(kBM) * c.tile_n * 4 > static_cast<size_t>(c.stages) * tc_a_bytes())
     return HML_STATUS_INVALID_VALUE;
   // TMA on A: 16-byte aligned base and row stride
   const int64_t sa = p.a_kcontig() ? p.sam : p.sak;
