@@ -74,6 +74,7 @@ inline hml_status cuda_status(cudaError_t e) {
 
 // Remember the last CUDA error text for diagnostics.
 void note_cuda_error(cudaError_t e, const char *where);
+void note_text_error(const char *text);
 const char *last_error_text();
 
 int sm_count();

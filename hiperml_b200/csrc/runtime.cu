@@ -50,6 +50,8 @@ void note_cuda_error(cudaError_t e, const char *where) {
 
 const char *last_error_text() { return t_last_error.c_str(); }
 
+void note_text_error(const char *text) { t_last_error = text; }
+
 int sm_count() {
   const int d = current_device();
   std::lock_guard<std::mutex> lk(g_mu);

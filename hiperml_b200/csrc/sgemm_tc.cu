@@ -38,6 +38,7 @@
 
 #include <algorithm>
 #include <cstring>
+#include <mutex>
 
 #include "hml_device.cuh"
 #include "hml_internal.h"
@@ -677,3 +678,167 @@ hml_status launch_tc(const GemmProblem &p, const hml_sgemm_config &c, cudaStream
 }
 
 }  // namespace hml
+
+// ----------------------------------------------------- no-allocation variant
+//
+// hml_sgemm_ex_config_noalloc runs the split-BF16 kernel above without any
+// device allocation.  Its only scratch, the BF16 planes of B, lives in a
+// fixed-size array in this file's module instead of the per-stream workspace
+// (which the library grows with cudaMalloc).  The array is part of the
+// library's device image, so every GPU that loads the library holds it until
+// the process exits.
+namespace hml {
+namespace {
+
+constexpr size_t kNoAllocScratchBytes = size_t(4) << 20;  // 4 MiB per device
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+constexpr int kNoAllocMaxDevices = 64;
+std::mutex g_noalloc_mu;
+void *g_noalloc_addr[kNoAllocMaxDevices];
+
+// Device address of the scratch array on the current device.  In host code
+// the array's name is only a host-side stand-in, so the address is looked up
+// once per device (with that device current) and cached.
+hml_status noalloc_scratch(void **out) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) {
+    note_cuda_error(e, "noalloc: cudaGetDevice");
+    return HML_STATUS_CUDA_ERROR;
+  }
+  if (dev < 0 || dev >= kNoAllocMaxDevices) return HML_STATUS_NOT_SUPPORTED;
+  std::lock_guard<std::mutex> lk(g_noalloc_mu);
+  if (!g_noalloc_addr[dev]) {
+    void *addr = nullptr;
+    e = cudaGetSymbolAddress(&addr, g_noalloc_scratch);
+    if (e != cudaSuccess || !addr) {
+      note_cuda_error(e != cudaSuccess ? e : cudaErrorInvalidSymbol,
+                      "noalloc: cudaGetSymbolAddress");
+      return HML_STATUS_CUDA_ERROR;
+    }
+    g_noalloc_addr[dev] = addr;
+  }
+  *out = g_noalloc_addr[dev];
+  return HML_STATUS_SUCCESS;
+}
+
+size_t noalloc_bytes_needed(const GemmProblem &p, const hml_sgemm_config &c) {
+  const int ns = c.algo == HML_ALGO_BF16X3 ? 2 : 3;
+  const size_t k_pad = ((static_cast<size_t>(p.K) + kChunkK - 1) / kChunkK) * kChunkK;
+  const size_t n_pad = ((static_cast<size_t>(p.N) + c.tile_n - 1) / c.tile_n) * c.tile_n;
+  return static_cast<size_t>(ns) * n_pad * k_pad * 2;
+}
+
+// The launch of run_tc with the B planes in `planes` (the static array) and
+// no device error word (bounded waits still end; nothing is recorded).
+template <int BN, int NS, bool AK>
+hml_status run_tc_static(const GemmProblem &p, const hml_sgemm_config &c, void *scratch,
+                         cudaStream_t s) {
+  const int k_pad = ((p.K + kChunkK - 1) / kChunkK) * kChunkK;
+  const int n_pad = ((p.N + BN - 1) / BN) * BN;
+  auto *planes = static_cast<__nv_bfloat16 *>(scratch);
+  {
+    const int64_t chunks = static_cast<int64_t>(n_pad) * (k_pad / 8);
+    const int blocks = static_cast<int>(std::min<int64_t>((chunks + 255) / 256, 4 * sm_count()));
+    count_launch();
+    split_b_kernel<NS><<<blocks, 256, 0, s>>>(p.B, p.sbk, p.sbn, p.K, p.N, planes, k_pad, n_pad);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) {
+      note_cuda_error(e, "noalloc split_b");
+      return HML_STATUS_CUDA_ERROR;
+    }
+  }
+  CUtensorMap ta, tb;
+  memset(&ta, 0, sizeof ta);
+  memset(&tb, 0, sizeof tb);
+  bool ok;
+  if (AK)
+    ok = tensor_map_2d(&ta, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, p.A, p.K, p.M, p.sam * 4, kBK, kBM,
+                       CU_TENSOR_MAP_SWIZZLE_128B);
+  else
+    ok = tensor_map_2d(&ta, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, p.A, p.M, p.K, p.sak * 4, kBM, kBK,
+                       CU_TENSOR_MAP_SWIZZLE_NONE);
+  if (ok)
+    ok = tensor_map_2d(&tb, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, planes, k_pad,
+                       static_cast<uint64_t>(NS) * n_pad, static_cast<uint64_t>(k_pad) * 2, kBK, BN,
+                       CU_TENSOR_MAP_SWIZZLE_64B);
+  if (!ok) return HML_STATUS_CUDA_ERROR;
+  TcArgs args;
+  args.p = p;
+  args.split = c.split_k;
+  const int kchunks = k_pad / kChunkK;
+  args.kc = ((kchunks + c.split_k - 1) / c.split_k) * kChunkK;
+  TcPlan plan;
+  if (!tc_plan(BN, NS, c.stages, &plan)) return HML_STATUS_INVALID_VALUE;
+  args.sa = plan.sa;
+  args.so = plan.so;
+  args.n_pad = n_pad;
+  args.err = nullptr;
+  const size_t smem = tc_plan_bytes(BN, NS, plan);
+  auto kern = tc_kernel<BN, NS, AK>;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       static_cast<int>(smem));
+  if (e == cudaSuccess && c.split_k > 8)
+    e = cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+  if (e != cudaSuccess) {
+    note_cuda_error(e, "noalloc tc attributes");
+    return HML_STATUS_CUDA_ERROR;
+  }
+  const int64_t tiles_m = (static_cast<int64_t>(p.M) + kBM - 1) / kBM;
+  const int64_t tiles_n = n_pad / BN;
+  if (tiles_m * c.split_k > 0x7fffffff || tiles_n > 65535) return HML_STATUS_NOT_SUPPORTED;
+  dim3 grid(static_cast<unsigned>(tiles_m * c.split_k), static_cast<unsigned>(tiles_n));
+  e = launch_k(kern, grid, dim3(kThreads), smem, s, c.split_k, ta, tb, args);
+  note_cuda_error(e, "noalloc tc launch");
+  return cuda_status(e);
+}
+
+template <int NS>
+hml_status run_tc_static_ns(const GemmProblem &p, const hml_sgemm_config &c, void *scratch,
+                            cudaStream_t s) {
+  const bool ak = p.a_kcontig();
+  switch (c.tile_n) {
+    case 16: return ak ? run_tc_static<16, NS, true>(p, c, scratch, s)
+                       : run_tc_static<16, NS, false>(p, c, scratch, s);
+    case 32: return ak ? run_tc_static<32, NS, true>(p, c, scratch, s)
+                       : run_tc_static<32, NS, false>(p, c, scratch, s);
+    case 64: return ak ? run_tc_static<64, NS, true>(p, c, scratch, s)
+                       : run_tc_static<64, NS, false>(p, c, scratch, s);
+    case 128: return ak ? run_tc_static<128, NS, true>(p, c, scratch, s)
+                        : run_tc_static<128, NS, false>(p, c, scratch, s);
+    default: return HML_STATUS_INVALID_VALUE;
+  }
+}
+
+}  // namespace
+}  // namespace hml
+
+extern "C" hml_status hml_sgemm_ex_config_noalloc(hml_order order, hml_op transA, hml_op transB,
+                                                  int M, int N, int K, float alpha, const float *A,
+                                                  int lda, const float *B, int ldb, float beta,
+                                                  float *C, int ldc, const hml_sgemm_config *config,
+                                                  void *stream) {
+  using namespace hml;
+  if (!config || (config->algo != HML_ALGO_BF16X3 && config->algo != HML_ALGO_BF16X6))
+    return HML_STATUS_INVALID_VALUE;
+  GemmProblem p;
+  hml_status st = gemm_from_blas(order, transA, transB, M, N, K, alpha, A, lda, B, ldb, beta, C,
+                                 ldc, &p);
+  if (st != HML_STATUS_SUCCESS) return st;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  if (p.M == 0 || p.N == 0) return HML_STATUS_SUCCESS;
+  if (p.K == 0 || p.alpha == 0.0f) return launch_scale(p.C, p.M, p.N, p.scm, p.scn, p.beta, s);
+  st = check_tc(p, *config);
+  if (st != HML_STATUS_SUCCESS) return st;
+  if (noalloc_bytes_needed(p, *config) > kNoAllocScratchBytes) {
+    note_text_error("noalloc: the BF16 planes of B need more than the 4 MiB static scratch "
+                    "(planes x ceil(N/tile_n)*tile_n x ceil(K/64)*64 x 2 bytes)");
+    return HML_STATUS_INVALID_VALUE;
+  }
+  void *scratch = nullptr;
+  st = noalloc_scratch(&scratch);
+  if (st != HML_STATUS_SUCCESS) return st;
+  return config->algo == HML_ALGO_BF16X3 ? run_tc_static_ns<2>(p, *config, scratch, s)
+                                         : run_tc_static_ns<3>(p, *config, scratch, s);
+}

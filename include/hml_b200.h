@@ -95,6 +95,36 @@ hml_status hml_sgemm_ex_config(hml_order order, hml_op transA, hml_op transB,
 hml_status hml_sgemm_select(hml_order order, hml_op transA, hml_op transB,
                             int M, int N, int K, hml_sgemm_config *config);
 
+/* Split-BF16 SGEMM that allocates nothing.  No counterpart in the
+ * reference: it exists for callers that must not allocate device memory
+ * during a call -- processes that reserve their whole HBM budget up front for
+ * their own pool, latency-critical paths where cudaMalloc's implicit device
+ * synchronisation is not acceptable, and hosts that forbid allocation after
+ * start-up.  hml_sgemm_ex_config with the same configuration computes the
+ * same result but keeps the BF16 planes of B in a workspace it grows with
+ * cudaMalloc; this variant keeps them in a fixed 4 MiB array compiled into
+ * the library (every GPU that loads the library holds it until exit).
+ *   - config->algo must be HML_ALGO_BF16X3 or HML_ALGO_BF16X6.
+ *   - Limit: planes x ceil(N / tile_n) * tile_n x ceil(K / 64) * 64 x 2 bytes
+ *     <= 4 MiB (planes = 2 for BF16X3, 3 for BF16X6); larger problems are
+ *     rejected with HML_STATUS_INVALID_VALUE and a message in
+ *     hml_last_error().
+ *   - The first call on a device looks up the array's device address
+ *     (cudaGetSymbolAddress) with that device current; make that first call
+ *     before any stream capture.
+ *   - Every call shares the one array: calls that overlap on the GPU (on
+ *     different streams) race.  Nothing in it needs to start at zero; each
+ *     call rewrites the part it uses.
+ *   - No device error word is kept: a bounded wait that expires still ends
+ *     the kernel, but is not recorded for hml_device_error(). */
+hml_status hml_sgemm_ex_config_noalloc(hml_order order, hml_op transA,
+                                       hml_op transB, int M, int N, int K,
+                                       float alpha, const float *A, int lda,
+                                       const float *B, int ldb, float beta,
+                                       float *C, int ldc,
+                                       const hml_sgemm_config *config,
+                                       void *stream);
+
 /* The heuristic configuration of one algorithm family for this problem
  * (HML_ALGO_AUTO: same as hml_sgemm_select).  Returns the status of
  * hml_sgemm_config_check for dense leading dimensions. */
