@@ -10,6 +10,7 @@ from .api import (  # noqa: F401
     ALGO_AUTO, ALGO_BF16X3, ALGO_BF16X6, ALGO_SIMT, COL_MAJOR, OP_N, OP_T, ROW_MAJOR,
     config_check, configs, device_error, error_fp64, fill_random, hmlSgemm, hmlSgemmBasic,
     hmlSgemmKernelConfig, hmlSgemv, hmlSgemvBasic, hmlSgemvKernelConfig, select, select_algo, sgemm,
-    sgemm_ex, sgemv_ex)
+    sgemm_ex, sgemv_ex, autotune, tune_save, tune_load, tune_clear, set_math_mode, MATH_FP32,
+    MATH_FAST)
 
 __version__ = lib.hml_version().decode()

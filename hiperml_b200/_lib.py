@@ -38,6 +38,11 @@ class SgemmConfig(ctypes.Structure):
                 f"split_k={self.split_k}, stages={self.stages}, variant={self.variant})")
 
 
+class TuneEntry(ctypes.Structure):
+    """``hml_tune_entry``."""
+    _fields_ = [("config", SgemmConfig), ("time_us", ctypes.c_float), ("status", ctypes.c_int32)]
+
+
 _SIGS = {
     "hml_status_string": (c_char_p, [c_int]),
     "hml_version": (c_char_p, []),
@@ -76,6 +81,13 @@ _SIGS = {
     "hml_device_error": (c_int, [c_int_p]),
     "hml_release_resources": (c_int, []),
     "hml_launch_count": (c_uint64, []),
+    "hml_autotune_sgemm": (c_int, [c_int, c_int, c_int, c_int, c_int, c_int, ctypes.c_uint32,
+                                   c_int, ctypes.POINTER(TuneEntry), c_int, c_int_p, c_void_p]),
+    "hml_tune_save": (c_int, [c_char_p]),
+    "hml_tune_load": (c_int, [c_char_p, c_int_p]),
+    "hml_tune_clear": (c_int, []),
+    "hml_tune_size": (c_int, []),
+    "hml_set_math_mode": (c_int, [c_int]),
 }
 
 for _name, (_res, _args) in _SIGS.items():

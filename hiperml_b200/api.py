@@ -18,7 +18,7 @@ from typing import Optional
 
 import numpy as np
 
-from ._lib import SgemmConfig, check, lib
+from ._lib import SgemmConfig, TuneEntry, check, lib
 
 COL_MAJOR, ROW_MAJOR = 0, 1
 OP_N, OP_T = 0, 1
@@ -222,3 +222,38 @@ def device_error() -> int:
     code = ctypes.c_int()
     check(lib.hml_device_error(ctypes.byref(code)), "hml_device_error")
     return code.value
+
+
+# ------------------------------------------------------------- autotuning
+MATH_FP32, MATH_FAST = 0, 1
+
+
+def autotune(order, transA, transB, M, N, K, families=0, reps=5, stream=None):
+    """Measure the configuration space on this shape (``hml_autotune_sgemm``).
+    Returns a list of (SgemmConfig, time_us, status); the fastest allowed
+    configuration is recorded in the library's tuned table."""
+    cap = lib.hml_sgemm_num_configs()
+    ents = (TuneEntry * cap)()
+    n = ctypes.c_int()
+    st = lib.hml_autotune_sgemm(order, transA, transB, M, N, K, families, reps, ents, cap,
+                                ctypes.byref(n), _stream(stream))
+    check(st, "hml_autotune_sgemm")
+    return [(ents[i].config, ents[i].time_us, ents[i].status) for i in range(n.value)]
+
+
+def tune_save(path: str) -> None:
+    check(lib.hml_tune_save(path.encode()), "hml_tune_save")
+
+
+def tune_load(path: str) -> int:
+    n = ctypes.c_int()
+    check(lib.hml_tune_load(path.encode(), ctypes.byref(n)), "hml_tune_load")
+    return n.value
+
+
+def tune_clear() -> None:
+    check(lib.hml_tune_clear(), "hml_tune_clear")
+
+
+def set_math_mode(mode: int) -> None:
+    check(lib.hml_set_math_mode(mode), "hml_set_math_mode")

@@ -10,4 +10,5 @@ bool check_config_ok(const GemmProblem &p, const hml_sgemm_config &c);
 // an answer for this problem.
 bool tuned_lookup(const GemmProblem &p, hml_sgemm_config *c);
 bool predictor_lookup(const GemmProblem &p, hml_sgemm_config *c);
+int math_mode();
 }  // namespace hml

@@ -86,6 +86,18 @@ hml_sgemm_config heuristic_config(const GemmProblem &p, int algo) {
 hml_status select_config(const GemmProblem &p, hml_sgemm_config *c) {
   if (tuned_lookup(p, c) && check_config_ok(p, *c)) return HML_STATUS_SUCCESS;
   if (predictor_lookup(p, c) && check_config_ok(p, *c)) return HML_STATUS_SUCCESS;
+  // Measured on B200 (M = 65536, K = 4096): FP32 SIMT wins at N <= 16 (the
+  // HBM-bound GEMV-like shapes); the split-BF16 tensor-core forms win from
+  // N = 32 on.  BF16X6 keeps FP32-level accuracy; BF16X3 (faster, ~2**-17)
+  // only in the fast math mode.
+  if (p.N > 16 && p.M >= 1024 && p.K >= 64) {
+    const int algo = math_mode() == HML_MATH_FAST ? HML_ALGO_BF16X3 : HML_ALGO_BF16X6;
+    const hml_sgemm_config tc = heuristic_config(p, algo);
+    if (check_config_ok(p, tc)) {
+      *c = tc;
+      return HML_STATUS_SUCCESS;
+    }
+  }
   *c = heuristic_config(p, HML_ALGO_SIMT);
   return HML_STATUS_SUCCESS;
 }

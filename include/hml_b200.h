@@ -54,6 +54,12 @@ typedef enum hml_algo {
   HML_ALGO_BF16X6 = 3  /* tcgen05: hi/mid/lo split, 6 products            */
 } hml_algo;
 
+/* Accuracy policy of hml_sgemm_ex's automatic choice. */
+typedef enum hml_math_mode {
+  HML_MATH_FP32 = 0, /* default: FP32 SIMT or BF16X6 (FP32-level accuracy)   */
+  HML_MATH_FAST = 1  /* BF16X3 allowed (about 2**-17 relative per product)  */
+} hml_math_mode;
+
 /* One point of the SGEMM configuration space. */
 typedef struct hml_sgemm_config {
   int32_t algo;    /* hml_algo                                            */
@@ -142,6 +148,41 @@ hml_status hml_sgemm_config_check(hml_order order, hml_op transA, hml_op transB,
 int hml_sgemm_num_configs(void);
 hml_status hml_sgemm_get_config(int index, hml_sgemm_config *config);
 int hml_sgemm_config_index(const hml_sgemm_config *config);
+
+/* --------------------------------------------------------- autotuning */
+
+/* One measured configuration. */
+typedef struct hml_tune_entry {
+  hml_sgemm_config config;
+  float time_us;  /* median device time of one call, -1 when not timed      */
+  int32_t status; /* hml_status of the trial (non-zero: refused or failed) */
+} hml_tune_entry;
+
+/* Measures every configuration of the space (restricted to the algorithm
+ * families in the bitmask `families`, bit = 1 << hml_algo; 0 = all) on this
+ * problem shape with dense leading dimensions and uniform[-1,1] operands:
+ * one warm-up call, then `reps` calls timed with CUDA events on the stream,
+ * L2 flushed before each when the operands fit in it, median kept.  A
+ * configuration that cannot run or fails is recorded with its status and
+ * skipped.  Writes up to max_entries results (*n_entries = count) and
+ * records the fastest configuration the math mode allows in the tuned table
+ * that hml_sgemm_ex consults first.  Replaces the reference's online tuner
+ * (src/hml_sgemm_kernel.cu:356-555). */
+hml_status hml_autotune_sgemm(hml_order order, hml_op transA, hml_op transB,
+                              int M, int N, int K, uint32_t families, int reps,
+                              hml_tune_entry *entries, int max_entries,
+                              int *n_entries, void *stream);
+
+/* The tuned table on disk ("#HML-B200 tuning v2"; the reference's v1
+ * .cfg grammar is read by hml_cfg_v1_load), replacing the reference's
+ * hmlSgemmKernelConfigPrint / ReadFile (src/hml_sgemm_kernel.cu:557-602). */
+hml_status hml_tune_save(const char *path);
+hml_status hml_tune_load(const char *path, int *records);
+hml_status hml_tune_clear(void);
+int hml_tune_size(void);
+
+/* Selects the accuracy policy (hml_math_mode) of automatic selection. */
+hml_status hml_set_math_mode(int mode);
 
 /* ---------------------------------------------------------------- SGEMV */
 

@@ -179,8 +179,7 @@ def test_precision_sweep_full_size_simt(cuda, N):
     for dist in (dg.UNIFORM, dg.LOGUNIFORM):
         hml.fill_random(A, 2, 0, dist)
         hml.fill_random(B, 2, 1, dist)
-        cfg = hml.select(0, 0, 0, M, N, K)
-        assert cfg.algo == hml.ALGO_SIMT
+        cfg = hml.select_algo(0, 0, 0, M, N, K, hml.ALGO_SIMT)
         hml.sgemm_ex(0, 0, 0, M, N, K, 1.0, A, M, B, K, 0.0, C, M, config=cfg)
         err = hml.error_fp64(0, 0, 0, M, N, K, 1.0, A, M, B, K, 0.0, None, C, M)
         assert err[2] <= 2 * (K + 2) * 2.0 ** -24, err

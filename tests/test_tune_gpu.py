@@ -1,0 +1,74 @@
+"""The measuring autotuner on a B200 (replaces the reference's online tuner,
+src/hml_sgemm_kernel.cu:356-555, which times every repository kernel on the
+caller's shape and keeps the fastest)."""
+import numpy as np
+import pytest
+
+import hiperml_b200 as hml
+from hiperml_b200._lib import lib
+
+pytestmark = pytest.mark.gpu
+
+
+def _median_us(fn, reps=20):
+    import torch
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2 * reps)]
+    for i in range(reps):
+        ev[2 * i].record()
+        fn()
+        ev[2 * i + 1].record()
+    torch.cuda.synchronize()
+    return float(np.median([ev[2 * i].elapsed_time(ev[2 * i + 1]) * 1e3 for i in range(reps)]))
+
+
+def test_autotune_records_fastest_allowed(cuda, tmp_path):
+    hml.tune_clear()
+    M, N, K = 8192, 64, 1024
+    ents = hml.autotune(0, 0, 0, M, N, K, reps=3)
+    assert len(ents) == lib.hml_sgemm_num_configs()
+    ok = [(c, t) for c, t, s in ents if s == 0]
+    assert len(ok) >= 50
+    assert all(t > 0 for _, t in ok)
+    # the recorded choice is the fastest FP32-accurate configuration measured
+    allowed = [(c, t) for c, t in ok if c.algo in (hml.ALGO_SIMT, hml.ALGO_BF16X6)]
+    best = min(allowed, key=lambda e: e[1])[0]
+    assert lib.hml_tune_size() == 1
+    assert hml.select(0, 0, 0, M, N, K).as_tuple() == best.as_tuple()
+    f = tmp_path / "tuned.cfg"
+    hml.tune_save(str(f))
+    hml.tune_clear()
+    assert hml.tune_load(str(f)) == 1
+    assert hml.select(0, 0, 0, M, N, K).as_tuple() == best.as_tuple()
+    hml.tune_clear()
+
+
+def test_tuned_choice_not_slower_than_heuristic(cuda):
+    """After tuning, hml_sgemm_ex on the shape runs within noise of the best
+    configuration and no slower than the untuned heuristic's choice."""
+    import torch
+    hml.tune_clear()
+    M, N, K = 16384, 32, 2048
+    A = torch.empty(M * K, device="cuda")
+    B = torch.empty(K * N, device="cuda")
+    C = torch.zeros(M * N, device="cuda")
+    hml.fill_random(A, 5, 0)
+    hml.fill_random(B, 5, 1)
+    run = lambda: hml.sgemm_ex(0, 0, 0, M, N, K, 1.0, A, M, B, K, 0.0, C, M)
+    run()
+    t_heur = _median_us(run)
+    ents = hml.autotune(0, 0, 0, M, N, K, families=1 << hml.ALGO_SIMT, reps=5)
+    t_best = min(t for c, t, s in ents if s == 0)
+    run()
+    t_tuned = _median_us(run)
+    hml.tune_clear()
+    assert t_tuned <= t_heur * 1.10 + 2.0, (t_tuned, t_heur)
+    assert t_tuned <= t_best * 1.25 + 2.0, (t_tuned, t_best)
+
+
+def test_autotune_family_mask_and_bad_arguments(cuda):
+    hml.tune_clear()
+    ents = hml.autotune(1, 1, 0, 3000, 20, 512, families=1 << hml.ALGO_SIMT, reps=2)
+    assert ents and all(c.algo == hml.ALGO_SIMT for c, _, _ in ents)
+    with pytest.raises(hml.HmlError):
+        hml.autotune(0, 0, 0, -1, 20, 512)
+    hml.tune_clear()
