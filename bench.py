@@ -48,7 +48,7 @@ def parse():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="sweep",
-                    choices=["sweep", "c1", "gemv_n", "gemv_t", "square"])
+                    choices=["sweep", "c1", "gemv_n", "gemv_t", "square", "batched"])
     ap.add_argument("--algo", default="auto", choices=["auto", "simt", "bf16x3", "bf16x6"],
                     help="force one algorithm family (default: the library's choice)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -153,7 +153,27 @@ def workload_problems(name):
         return [("gemv_t", 32768, 1, 4096)]
     if name == "square":
         return [("sgemm", 8192, 8192, 8192)]
+    if name == "batched":
+        return [("sgemm", M, N, K) for (_ta, _tb, M, N, K) in batch_shapes()]
     raise ValueError(name)
+
+
+BATCH_COUNT, BATCH_SEED = 1024, 3
+
+
+def batch_shapes(count=BATCH_COUNT, seed=BATCH_SEED):
+    """The batched workload: `count` problems (transA, transB, M, N, K) with
+    M log-uniform in [256, 16384], N uniform in 1..128, K log-uniform in
+    [64, 4096] and Bernoulli(0.5) transposes, drawn from numpy's PCG64 with
+    the given seed."""
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    M = np.exp(rng.uniform(np.log(256), np.log(16384), count)).astype(np.int64)
+    N = rng.integers(1, 129, count)
+    K = np.exp(rng.uniform(np.log(64), np.log(4096), count)).astype(np.int64)
+    ta = rng.integers(0, 2, count)
+    tb = rng.integers(0, 2, count)
+    return [(int(ta[i]), int(tb[i]), int(M[i]), int(N[i]), int(K[i])) for i in range(count)]
 
 
 def flops_of(kind, M, N, K):
@@ -184,6 +204,15 @@ def config_desc(name):
         return {"workload": f"SGEMV y={'A' if name == 'gemv_n' else 'A^T'}*x, A 32768x4096 "
                             "col-major", "inputs": "N(0,1), seed 1",
                 "l2": "A is 512 MiB (> L2): no flush"}
+    if name == "batched":
+        return {"workload": f"batched: {BATCH_COUNT} independent FP32 GEMMs C=op(A)op(B), "
+                            "col-major, one persistent graph-captured launch",
+                "M": "log-uniform [256, 16384]", "N": "uniform {1..128}",
+                "K": "log-uniform [64, 4096]", "trans": "Bernoulli(0.5) each",
+                "alpha": 1.0, "beta": 0.0, "count": BATCH_COUNT,
+                "shapes_seed": BATCH_SEED, "inputs": "N(0,1), seed 3",
+                "storage": "leading dimensions rounded up to 4 floats, 256-byte aligned bases",
+                "l2": "about 15 GB of operands per step (> 126 MB L2): no flush"}
     return {"workload": "square SGEMM 8192^3 col-major", "inputs": "uniform[-1,1], seed 0",
             "l2": "compute bound; inputs 256 MiB each"}
 
@@ -498,10 +527,196 @@ def run_ours(args):
     return 0
 
 
+def run_batched(args):
+    """The batched workload: one persistent launch (replayed from a CUDA
+    graph) per step, against the same 1024 problems as separate calls."""
+    import numpy as np
+    import torch
+
+    import hiperml_b200 as hml
+    from hiperml_b200 import datagen as dg
+    from hiperml_b200._lib import check
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist_on = world > 1
+    if dist_on:
+        import datetime
+
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    stream = torch.cuda.current_stream()
+
+    shapes = batch_shapes()
+    r4 = lambda x: (x + 3) // 4 * 4
+    a64 = lambda x: (x + 63) // 64 * 64
+    layout = []  # (ta, tb, M, N, K, lda, ldb, ldc, offA, offB, offC)
+    oa = ob = oc = 0
+    for (ta, tb, M, N, K) in shapes:
+        lda = r4(K if ta else M)
+        ldb = r4(N if tb else K)
+        ldc = r4(M)
+        layout.append((ta, tb, M, N, K, lda, ldb, ldc, oa, ob, oc))
+        oa += a64(lda * (M if ta else K))
+        ob += a64(ldb * (K if tb else N))
+        oc += a64(ldc * N)
+    poolA = torch.empty(oa, dtype=torch.float32, device=dev)
+    poolB = torch.empty(ob, dtype=torch.float32, device=dev)
+    poolC = torch.zeros(oc, dtype=torch.float32, device=dev)
+    hml.fill_random(poolA, BATCH_SEED + rank * 1000, 0, dg.NORMAL)
+    hml.fill_random(poolB, BATCH_SEED + rank * 1000, 1, dg.NORMAL)
+    pa, pb, pc = poolA.data_ptr(), poolB.data_ptr(), poolC.data_ptr()
+    descs = [(ta, tb, M, N, K, 1.0, pa + 4 * oa_, lda, pb + 4 * ob_, ldb, 0.0, pc + 4 * oc_, ldc)
+             for (ta, tb, M, N, K, lda, ldb, ldc, oa_, ob_, oc_) in layout]
+    plan = hml.BatchPlan(hml.COL_MAJOR, descs)
+    info = plan.info()
+
+    for _ in range(args.warmup):
+        plan.graph_launch(stream)
+    torch.cuda.synchronize()
+    if dist_on:
+        dist.barrier()
+    torch.cuda.synchronize()
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+           for _ in range(args.steps)]
+    launches0 = hml.lib.hml_launch_count()
+    t0 = torch.cuda.Event(enable_timing=True)
+    t1 = torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clocks:
+        t0.record(stream)
+        for i in range(args.steps):
+            evs[i][0].record(stream)
+            plan.graph_launch(stream)
+            evs[i][1].record(stream)
+        t1.record(stream)
+        torch.cuda.synchronize()
+    launches = hml.lib.hml_launch_count() - launches0
+    if dist_on:
+        dist.barrier()
+    elapsed_ms = t0.elapsed_time(t1)
+    per_launch_ms = statistics.mean(a.elapsed_time(b) for a, b in evs)
+    if dist_on:
+        t = torch.tensor([elapsed_ms], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        elapsed_ms = float(t.item())
+    step_flops = info["flops"]
+    value = step_flops * args.steps * world / (elapsed_ms * 1e-3) / 1e12
+
+    # ---- accuracy on a sample of problems (FP64 on the GPU)
+    errs = []
+    if rank == 0:
+        for (ta, tb, M, N, K, lda, ldb, ldc, oa_, ob_, oc_) in layout[:: max(1, len(layout) // 16)]:
+            e = hml.error_fp64(0, ta, tb, M, N, K, 1.0, pa + 4 * oa_, lda, pb + 4 * ob_, ldb, 0.0,
+                               None, pc + 4 * oc_, ldc)
+            errs.append(e)
+
+    # ---- the same problems as 1024 separate calls (device pointers)
+    def separate(config_of):
+        reps = max(1, min(args.steps, 3))
+        cfgs = [config_of(d) for d in descs]
+        for d, c in zip(descs, cfgs):  # warm-up
+            hml.sgemm_ex(0, d[0], d[1], d[2], d[3], d[4], 1.0, d[6], d[7], d[8], d[9], 0.0, d[11],
+                         d[12], stream=stream, config=c)
+        torch.cuda.synchronize()
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        for _ in range(reps):
+            for d, c in zip(descs, cfgs):
+                hml.sgemm_ex(0, d[0], d[1], d[2], d[3], d[4], 1.0, d[6], d[7], d[8], d[9], 0.0,
+                             d[11], d[12], stream=stream, config=c)
+        b.record(stream)
+        torch.cuda.synchronize()
+        return step_flops * reps / (a.elapsed_time(b) * 1e-3) / 1e12
+
+    sep_simt = separate(lambda d: hml.select_algo(0, d[0], d[1], d[2], d[3], d[4], hml.ALGO_SIMT))
+    sep_auto = separate(lambda d: None)
+
+    # ---- end to end: pinned host operands copied in, one graph launch,
+    # every C copied back
+    e2e = None
+    if not args.no_e2e:
+        hA = poolA.cpu().pin_memory()
+        hB = poolB.cpu().pin_memory()
+        hC = torch.empty(poolC.numel(), dtype=torch.float32).pin_memory()
+        reps = max(1, min(args.steps, 2))
+
+        def e2e_step():
+            poolA.copy_(hA, non_blocking=True)
+            poolB.copy_(hB, non_blocking=True)
+            plan.graph_launch(stream)
+            hC.copy_(poolC, non_blocking=True)
+            torch.cuda.synchronize()
+
+        e2e_step()
+        ts = time.perf_counter()
+        for _ in range(reps):
+            e2e_step()
+        te = (time.perf_counter() - ts) / reps
+        if dist_on:
+            t = torch.tensor([te], device=dev, dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            te = float(t.item())
+        e2e = {"value": step_flops * world / te / 1e12, "unit": UNIT,
+               "h2d_bytes_per_step": 4 * (poolA.numel() + poolB.numel()),
+               "d2h_bytes_per_step": 4 * poolC.numel(),
+               "api": "hml_batch_plan_graph_launch, operands from pinned host memory", "steps": reps}
+        del hA, hB, hC
+
+    pk = peaks()
+    alg_bytes = info["bytes"]
+    dom_s = per_launch_ms * 1e-3
+    roof = {"bound": "hbm", "achieved": alg_bytes / dom_s / 1e9, "peak": pk["hbm_gbs"],
+            "unit": "GB/s", "frac": alg_bytes / dom_s / 1e9 / pk["hbm_gbs"],
+            "traffic": traffic_table().get("batched"), "kernel": "batched_kernel",
+            "alg_bytes_per_launch": alg_bytes, "alg_flops_per_launch": step_flops,
+            "ms_per_launch": per_launch_ms, "peak_source": pk["source"],
+            "simt_fp32_tflops": step_flops / dom_s / 1e12,
+            "simt_fp32_peak_nominal": 148 * 128 * 2 * 1.965e-3,
+            "note": "mixed batch: HBM-bound (small N) and FP32-bound (large N) tiles"}
+
+    cpu = None
+    if not args.no_cpu_baseline and rank == 0 and world == 1:
+        sample = [("sgemm", M, N, K) for (_ta, _tb, M, N, K) in shapes[:64]]
+        v, cores, kind, desc = cpu_reference_sample(sample, seconds=10.0)
+        cpu = {"value": v, "unit": UNIT, "cores": cores, "kind": kind,
+               "sample": "first 64 problems of the batch: " + desc}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": elapsed_ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": dict(config_desc("batched"),
+                           parallelism=f"independent per-GPU batches x{world}"),
+            "roofline": roof, "cpu_baseline": cpu, "e2e": e2e,
+            "clocks": clocks.summary(), "gpu_launches": int(launches),
+            "batch": {"tiles": info["tiles"], "ctas": info["ctas"],
+                      "separate_simt_calls_tflops": sep_simt,
+                      "separate_auto_calls_tflops": sep_auto,
+                      "speedup_vs_separate_simt": value / world / sep_simt,
+                      "max_rel_err_fp64_sample": max(e[0] for e in errs) if errs else None,
+                      "max_compwise_err_fp64_sample": max(e[2] for e in errs) if errs else None},
+        }
+        print(json.dumps(line), flush=True)
+    plan.close()
+    if dist_on:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         return run_reference(args)
+    if args.workload == "batched":
+        return run_batched(args)
     return run_ours(args)
 
 

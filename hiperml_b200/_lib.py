@@ -43,6 +43,15 @@ class TuneEntry(ctypes.Structure):
     _fields_ = [("config", SgemmConfig), ("time_us", ctypes.c_float), ("status", ctypes.c_int32)]
 
 
+class GemmDesc(ctypes.Structure):
+    """``hml_gemm_desc``: one problem of a batch (device pointers)."""
+    _fields_ = [("transA", ctypes.c_int32), ("transB", ctypes.c_int32), ("M", ctypes.c_int32),
+                ("N", ctypes.c_int32), ("K", ctypes.c_int32), ("lda", ctypes.c_int32),
+                ("ldb", ctypes.c_int32), ("ldc", ctypes.c_int32), ("alpha", ctypes.c_float),
+                ("beta", ctypes.c_float), ("A", ctypes.c_void_p), ("B", ctypes.c_void_p),
+                ("C", ctypes.c_void_p)]
+
+
 _SIGS = {
     "hml_status_string": (c_char_p, [c_int]),
     "hml_version": (c_char_p, []),
@@ -88,6 +97,14 @@ _SIGS = {
     "hml_tune_clear": (c_int, []),
     "hml_tune_size": (c_int, []),
     "hml_set_math_mode": (c_int, [c_int]),
+    "hml_batch_plan_create": (c_int, [c_int, ctypes.POINTER(GemmDesc), c_int,
+                                      ctypes.POINTER(c_void_p)]),
+    "hml_batch_plan_run": (c_int, [c_void_p, c_void_p]),
+    "hml_batch_plan_graph_launch": (c_int, [c_void_p, c_void_p]),
+    "hml_batch_plan_info": (c_int, [c_void_p, c_int_p, c_int_p, ctypes.POINTER(ctypes.c_double),
+                                    ctypes.POINTER(ctypes.c_double)]),
+    "hml_batch_plan_destroy": (c_int, [c_void_p]),
+    "hml_sgemm_batched": (c_int, [c_int, ctypes.POINTER(GemmDesc), c_int, c_void_p]),
 }
 
 for _name, (_res, _args) in _SIGS.items():

@@ -18,7 +18,7 @@ from typing import Optional
 
 import numpy as np
 
-from ._lib import SgemmConfig, TuneEntry, check, lib
+from ._lib import GemmDesc, SgemmConfig, TuneEntry, check, lib
 
 COL_MAJOR, ROW_MAJOR = 0, 1
 OP_N, OP_T = 0, 1
@@ -257,3 +257,62 @@ def tune_clear() -> None:
 
 def set_math_mode(mode: int) -> None:
     check(lib.hml_set_math_mode(mode), "hml_set_math_mode")
+
+
+# ----------------------------------------------------------------- batched
+def gemm_descs(problems):
+    """ctypes array of ``hml_gemm_desc`` from tuples
+    (transA, transB, M, N, K, alpha, A, lda, B, ldb, beta, C, ldc); A, B, C
+    are device pointers (ints) or CUDA tensors."""
+    arr = (GemmDesc * max(1, len(problems)))()
+    for i, (ta, tb, M, N, K, alpha, A, lda, B, ldb, beta, C, ldc) in enumerate(problems):
+        arr[i] = GemmDesc(ta, tb, M, N, K, lda, ldb, ldc, alpha, beta, _ptr(A), _ptr(B), _ptr(C))
+    return arr
+
+
+class BatchPlan:
+    """``hml_batch_plan``: a batch of SGEMMs run by one persistent launch."""
+
+    def __init__(self, order, problems):
+        self._descs = gemm_descs(problems)
+        h = ctypes.c_void_p()
+        check(lib.hml_batch_plan_create(order, self._descs, len(problems), ctypes.byref(h)),
+              "hml_batch_plan_create")
+        self._h = h
+
+    def run(self, stream=None):
+        check(lib.hml_batch_plan_run(self._h, _stream(stream)), "hml_batch_plan_run")
+
+    def graph_launch(self, stream=None):
+        check(lib.hml_batch_plan_graph_launch(self._h, _stream(stream)),
+              "hml_batch_plan_graph_launch")
+
+    def info(self):
+        t, c = ctypes.c_int(), ctypes.c_int()
+        f, b = ctypes.c_double(), ctypes.c_double()
+        check(lib.hml_batch_plan_info(self._h, ctypes.byref(t), ctypes.byref(c), ctypes.byref(f),
+                                      ctypes.byref(b)), "hml_batch_plan_info")
+        return {"tiles": t.value, "ctas": c.value, "flops": f.value, "bytes": b.value}
+
+    def close(self):
+        if self._h:
+            lib.hml_batch_plan_destroy(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def sgemm_batched(order, problems, stream=None):
+    """``hml_sgemm_batched``: one-shot batch, stream ordered."""
+    descs = gemm_descs(problems)
+    check(lib.hml_sgemm_batched(order, descs, len(problems), _stream(stream)), "hml_sgemm_batched")

@@ -159,8 +159,10 @@ __device__ __forceinline__ float warp_sum(float v) {
 }
 
 // BLAS epilogue: beta == 0 never reads the old value.
+// alpha * acc + beta * c with one fixed rounding sequence, so that every
+// kernel that finishes a C element the same way gives the same bits.
 __device__ __forceinline__ float axpby(float alpha, float acc, float beta, const float *c) {
-  return beta == 0.0f ? alpha * acc : alpha * acc + beta * (*c);
+  return beta == 0.0f ? __fmul_rn(alpha, acc) : __fmaf_rn(alpha, acc, __fmul_rn(beta, *c));
 }
 
 }  // namespace hml

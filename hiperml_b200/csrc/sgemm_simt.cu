@@ -30,41 +30,10 @@
 
 #include "hml_device.cuh"
 #include "hml_internal.h"
+#include "simt_tile.cuh"
 
 namespace hml {
 namespace {
-
-constexpr int kBK = 32;  // K depth of one pipeline stage (128 bytes of FP32)
-
-struct SimtShape {
-  int tm, tn, wm, wn, wk;
-  int bm() const { return wm * 32 * tm; }
-  int bn() const { return wn * tn; }
-};
-
-// The micro-tile table (index = hml_sgemm_config.variant for HML_ALGO_SIMT).
-constexpr SimtShape kSimtShapes[] = {
-    {4, 16, 1, 1, 8},  // 0: 128 x 16,  K split 8 ways across warps
-    {4, 8, 1, 1, 8},   // 1: 128 x 8
-    {4, 16, 1, 2, 4},  // 2: 128 x 32
-    {8, 16, 1, 2, 4},  // 3: 256 x 32
-    {8, 16, 1, 4, 2},  // 4: 256 x 64
-    {8, 16, 1, 8, 1},  // 5: 256 x 128
-    {4, 16, 2, 4, 1},  // 6: 256 x 64, two row groups
-    {4, 16, 1, 4, 2},  // 7: 128 x 64
-    {4, 16, 1, 8, 1},  // 8: 128 x 128
-};
-constexpr int kNumSimtShapes = sizeof(kSimtShapes) / sizeof(kSimtShapes[0]);
-
-__device__ __forceinline__ float4 lds128(const float *p) {
-  return *reinterpret_cast<const float4 *>(p);
-}
-
-__device__ __forceinline__ void cp_async4(uint32_t dst, const float *src, bool valid) {
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;" ::"r"(dst), "l"(src),
-               "r"(valid ? 4 : 0)
-               : "memory");
-}
 
 struct SimtArgs {
   GemmProblem p;
@@ -74,37 +43,13 @@ struct SimtArgs {
   int *err;
 };
 
-__device__ __forceinline__ void cp_async_commit() {
-  asm volatile("cp.async.commit_group;" ::: "memory");
-}
-
-// cp.async.wait_group takes an immediate: dispatch the runtime ring depth.
-__device__ __forceinline__ void cp_async_wait_ring(int stages) {
-  switch (stages) {
-    case 2: asm volatile("cp.async.wait_group 0;" ::: "memory"); break;
-    case 3: asm volatile("cp.async.wait_group 1;" ::: "memory"); break;
-    case 4: asm volatile("cp.async.wait_group 2;" ::: "memory"); break;
-    case 5: asm volatile("cp.async.wait_group 3;" ::: "memory"); break;
-    case 6: asm volatile("cp.async.wait_group 4;" ::: "memory"); break;
-    case 7: asm volatile("cp.async.wait_group 5;" ::: "memory"); break;
-    default: asm volatile("cp.async.wait_group 6;" ::: "memory"); break;
-  }
-}
-
 template <int TM, int TN, int WM, int WN, int WK, bool AK, bool BK_, bool TMA>
 __global__ void __launch_bounds__(256, 1)
     simt_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
                 SimtArgs args) {
-  constexpr int BM = WM * 32 * TM;
-  constexpr int BN = WN * TN;
-  constexpr int NCW = WM * WN * WK;  // warps
-  static_assert(NCW == 8, "8 warps");
-  constexpr int NT = NCW * 32;
-  constexpr int KW = kBK / WK;  // K values per warp per stage
-  constexpr int A_BYTES = BM * kBK * 4;
-  constexpr int B_BYTES = BN * kBK * 4;
-  constexpr int STAGE_BYTES = A_BYTES + B_BYTES;
-  constexpr int RED_BYTES = WK * BM * BN * 4;  // epilogue reuse of the ring
+  using T = SimtTile<TM, TN, WM, WN, WK, AK, BK_>;
+  constexpr int BM = T::BM, BN = T::BN, NT = T::NT;
+  constexpr int A_BYTES = T::A_BYTES, STAGE_BYTES = T::STAGE_BYTES;
 
   extern __shared__ uint8_t smem_raw[];
   uint8_t *smem = reinterpret_cast<uint8_t *>(
@@ -112,10 +57,9 @@ __global__ void __launch_bounds__(256, 1)
   const GemmProblem &p = args.p;
   const int stages = args.stages;
   // barriers sit past both the ring and the epilogue's reduction buffer
-  uint64_t *full = reinterpret_cast<uint64_t *>(smem + max(stages * STAGE_BYTES, RED_BYTES));
+  uint64_t *full = reinterpret_cast<uint64_t *>(smem + max(stages * STAGE_BYTES, T::RED_BYTES));
 
   const int tid = threadIdx.x;
-  const int warp = tid >> 5, lane = tid & 31;
   const int split = args.split;
   const int rank = split > 1 ? static_cast<int>(cluster_ctarank()) : 0;
   const int64_t m0 = static_cast<int64_t>(blockIdx.x / split) * BM;
@@ -151,50 +95,29 @@ __global__ void __launch_bounds__(256, 1)
     } else {
       const uint32_t ua = smem_u32(sa), ub = smem_u32(sb);
       for (int e = tid; e < BM * kBK; e += NT) {
-        int m, k;
-        uint32_t off;
-        if (AK) {  // same 128-byte swizzle as the TMA path
-          k = e % kBK;
-          m = e / kBK;
-          off = static_cast<uint32_t>(m * 128 + k * 4) ^ static_cast<uint32_t>((m & 7) << 4);
-        } else {
-          m = e % BM;
-          k = e / BM;
-          off = static_cast<uint32_t>((k * BM + m) * 4);
-        }
+        const int m = AK ? e / kBK : e % BM;
+        const int k = AK ? e % kBK : e / BM;
         const int64_t gm = m0 + m;
         const int gk = k0 + k;
         const bool ok = gm < p.M && gk < kend;
         const float *src = ok ? p.A + gm * p.sam + static_cast<int64_t>(gk) * p.sak : p.A;
-        cp_async4(ua + off, src, ok);
+        cp_async4(ua + T::a_off(m, k), src, ok);
       }
       for (int e = tid; e < BN * kBK; e += NT) {
-        int n, k;
-        uint32_t off;
-        if (BK_) {
-          k = e % kBK;
-          n = e / kBK;
-          off = static_cast<uint32_t>((n * kBK + k) * 4);
-        } else {
-          n = e % BN;
-          k = e / BN;
-          off = static_cast<uint32_t>((k * BN + n) * 4);
-        }
+        const int n = BK_ ? e / kBK : e % BN;
+        const int k = BK_ ? e % kBK : e / BN;
         const int gn = n0 + n;
         const int gk = k0 + k;
         const bool ok = gn < p.N && gk < kend;
         const float *src =
             ok ? p.B + static_cast<int64_t>(gk) * p.sbk + static_cast<int64_t>(gn) * p.sbn : p.B;
-        cp_async4(ub + off, src, ok);
+        cp_async4(ub + T::b_off(n, k), src, ok);
       }
     }
   };
 
   float acc[TM][TN];
-#pragma unroll
-  for (int i = 0; i < TM; ++i)
-#pragma unroll
-    for (int j = 0; j < TN; ++j) acc[i][j] = 0.0f;
+  T::zero(acc);
 
   // prologue: stages-1 slabs in flight
   if (TMA) {
@@ -207,11 +130,7 @@ __global__ void __launch_bounds__(256, 1)
     }
   }
 
-  const int wk = warp % WK;
-  const int wn = (warp / WK) % WN;
-  const int wm = warp / (WK * WN);
-  const int mrow = wm * 32 * TM;
-  const int ncol = wn * TN;
+  const typename T::Coord co = T::coord(tid);
   bool bad = false;
   for (int it = 0; it < nk; ++it) {
     const int s = it % stages;
@@ -227,84 +146,18 @@ __global__ void __launch_bounds__(256, 1)
       if (it + stages - 1 < nk) issue(it + stages - 1);
       cp_async_commit();
     }
-    const float *sa = reinterpret_cast<const float *>(smem + s * STAGE_BYTES);
-    const float *sb = reinterpret_cast<const float *>(smem + s * STAGE_BYTES + A_BYTES);
-#pragma unroll 2
-    for (int k4 = 0; k4 < KW / 4; ++k4) {
-      const int kb = wk * KW + k4 * 4;
-      // A K-contiguous: one 16-byte read per row gives 4 k values
-      float4 a4[AK ? TM : 1];
-      if (AK) {
-#pragma unroll
-        for (int i = 0; i < TM; ++i) {
-          const int m = mrow + lane + 32 * i;
-          a4[i] = lds128(sa + m * kBK + (((kb >> 2) ^ (m & 7)) << 2));
-        }
-      }
-#pragma unroll
-      for (int kk = 0; kk < 4; ++kk) {
-        float a[TM];
-        if (AK) {
-#pragma unroll
-          for (int i = 0; i < TM; ++i)
-            a[i] = kk == 0 ? a4[i].x : kk == 1 ? a4[i].y : kk == 2 ? a4[i].z : a4[i].w;
-        } else {
-#pragma unroll
-          for (int j = 0; j < TM / 4; ++j) {
-            const float4 v = lds128(sa + (kb + kk) * BM + mrow + 4 * lane + 128 * j);
-            a[4 * j + 0] = v.x; a[4 * j + 1] = v.y; a[4 * j + 2] = v.z; a[4 * j + 3] = v.w;
-          }
-        }
-        float b[TN];
-        if (BK_) {
-#pragma unroll
-          for (int j = 0; j < TN; ++j) b[j] = sb[(ncol + j) * kBK + kb + kk];
-        } else {
-#pragma unroll
-          for (int j = 0; j < TN / 4; ++j) {
-            const float4 v = lds128(sb + (kb + kk) * BN + ncol + 4 * j);
-            b[4 * j + 0] = v.x; b[4 * j + 1] = v.y; b[4 * j + 2] = v.z; b[4 * j + 3] = v.w;
-          }
-        }
-#pragma unroll
-        for (int i = 0; i < TM; ++i)
-#pragma unroll
-          for (int j = 0; j < TN; ++j) acc[i][j] = fmaf(a[i], b[j], acc[i][j]);
-      }
-    }
+    T::slab(reinterpret_cast<const float *>(smem + s * STAGE_BYTES),
+            reinterpret_cast<const float *>(smem + s * STAGE_BYTES + A_BYTES), acc, co);
   }
   if (!TMA) asm volatile("cp.async.wait_all;" ::: "memory");
 
   // ---------------------------------------------------------- epilogue
   __syncthreads();  // every stage consumed: the ring can be reused
   float *red = reinterpret_cast<float *>(smem);  // [WK][BN][BM]
-  {
-    float *r = red + static_cast<size_t>(wk) * BM * BN;
-#pragma unroll
-    for (int j = 0; j < TN; ++j) {
-      float *col = r + (wn * TN + j) * BM + wm * 32 * TM;
-      if (AK) {
-#pragma unroll
-        for (int i = 0; i < TM; ++i) col[lane + 32 * i] = acc[i][j];
-      } else {
-#pragma unroll
-        for (int q = 0; q < TM / 4; ++q)
-          *reinterpret_cast<float4 *>(col + 4 * lane + 128 * q) =
-              make_float4(acc[4 * q][j], acc[4 * q + 1][j], acc[4 * q + 2][j], acc[4 * q + 3][j]);
-      }
-    }
-  }
+  T::stash(red, acc, co);
   __syncthreads();
+  T::reduce_wk(red, tid);
   constexpr int E = BM * BN;
-  if (WK > 1) {
-    for (int e = tid; e < E; e += NT) {
-      float s = red[e];
-#pragma unroll
-      for (int w = 1; w < WK; ++w) s += red[w * E + e];
-      red[e] = s;
-    }
-  }
-  const bool c_ncontig = p.scn == 1 && p.scm != 1;
   if (split > 1) {
     cluster_sync();
     const int per = E / split;  // split divides E (E is a multiple of 1024)
@@ -331,29 +184,7 @@ __global__ void __launch_bounds__(256, 1)
     cluster_sync();
   } else {
     __syncthreads();
-    if (c_ncontig) {
-      // row-major C: walk n fastest so consecutive threads write adjacent
-      // addresses (red is [n][m]; the strided smem read is the cheaper side)
-      for (int e = tid; e < E; e += NT) {
-        const int n = e % BN, m = e / BN;
-        const int64_t gm = m0 + m;
-        const int gn = n0 + n;
-        if (gm < p.M && gn < p.N) {
-          float *c = p.C + gm * p.scm + gn;
-          *c = axpby(p.alpha, red[n * BM + m], p.beta, c);
-        }
-      }
-    } else {
-      for (int e = tid; e < E; e += NT) {
-        const int m = e % BM, n = e / BM;
-        const int64_t gm = m0 + m;
-        const int gn = n0 + n;
-        if (gm < p.M && gn < p.N) {
-          float *c = p.C + gm * p.scm + static_cast<int64_t>(gn) * p.scn;
-          *c = axpby(p.alpha, red[e], p.beta, c);
-        }
-      }
-    }
+    T::store_c(red, tid, m0, n0, p.M, p.N, p.C, p.scm, p.scn, p.alpha, p.beta);
   }
 }
 

@@ -184,6 +184,53 @@ int hml_tune_size(void);
 /* Selects the accuracy policy (hml_math_mode) of automatic selection. */
 hml_status hml_set_math_mode(int mode);
 
+/* ------------------------------------------------------------- batched */
+
+/* One problem of a batch: C = alpha * op(A) * op(B) + beta * C on device
+ * pointers, stored in the batch's hml_order (same argument meaning as
+ * hml_sgemm_ex).  The C matrices of one batch must not overlap. */
+typedef struct hml_gemm_desc {
+  int32_t transA, transB; /* hml_op */
+  int32_t M, N, K;
+  int32_t lda, ldb, ldc;
+  float alpha, beta;
+  const float *A;
+  const float *B;
+  float *C;
+} hml_gemm_desc;
+
+typedef struct hml_batch_plan_s *hml_batch_plan;
+
+/* Builds a plan for a batch: validates every problem, cuts all of them into
+ * tile work items ordered longest first, and uploads the items to the
+ * device.  The reference has no batched form: its callers loop over
+ * hmlSgemm, one launch and one synchronisation per problem
+ * (src/hml_sgemm.cu:120-211).  The descriptors are copied; the matrices they
+ * point to are read when the plan runs. */
+hml_status hml_batch_plan_create(hml_order order, const hml_gemm_desc *descs,
+                                 int count, hml_batch_plan *plan);
+
+/* Runs every problem of the plan in ONE persistent kernel launch whose CTAs
+ * take tiles from a device work queue.  Stream ordered; capturable.  One
+ * plan runs on one stream at a time. */
+hml_status hml_batch_plan_run(hml_batch_plan plan, void *stream);
+
+/* Same, through a CUDA graph holding the launch: the first call captures
+ * it (not while the calling thread is capturing a stream in global mode),
+ * every call launches the graph on `stream`. */
+hml_status hml_batch_plan_graph_launch(hml_batch_plan plan, void *stream);
+
+/* Work items, CTAs of the launch, useful FLOPs (2MNK summed) and
+ * algorithmic bytes (A, B read once, C written once, read too when
+ * beta != 0). Any output pointer may be NULL. */
+hml_status hml_batch_plan_info(hml_batch_plan plan, int *tiles, int *ctas,
+                               double *flops, double *bytes);
+hml_status hml_batch_plan_destroy(hml_batch_plan plan);
+
+/* One-shot batch: plan, one launch and release, all stream ordered. */
+hml_status hml_sgemm_batched(hml_order order, const hml_gemm_desc *descs,
+                             int count, void *stream);
+
 /* ---------------------------------------------------------------- SGEMV */
 
 /* y = alpha * op(A) * x + beta * y on device pointers; A is M x N in storage,
