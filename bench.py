@@ -51,6 +51,10 @@ def parse():
                     choices=["sweep", "c1", "gemv_n", "gemv_t", "square", "batched"])
     ap.add_argument("--algo", default="auto", choices=["auto", "simt", "bf16x3", "bf16x6"],
                     help="force one algorithm family (default: the library's choice)")
+    ap.add_argument("--rows", type=int, default=None,
+                    help="sweep workload: M other than 65536 (small cases for profiler captures)")
+    ap.add_argument("--only-n", type=int, default=None,
+                    help="sweep workload: run only this N (profiler captures)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     return ap.parse_args()
@@ -141,10 +145,11 @@ class ClockSampler:
 
 
 # ------------------------------------------------------------- workloads
-def workload_problems(name):
+def workload_problems(name, rows=None, only_n=None):
     """List of (kind, M, N, K) problems making one step."""
     if name == "sweep":
-        return [("sgemm", SWEEP_M, n, SWEEP_K) for n in SWEEP_N]
+        return [("sgemm", rows or SWEEP_M, n, SWEEP_K) for n in SWEEP_N
+                if only_n is None or n == only_n]
     if name == "c1":
         return [("sgemm", 4096, 16, 4096)]
     if name == "gemv_n":
@@ -290,6 +295,10 @@ def run_reference(args):
     if rank != 0:
         return 0
     problems = workload_problems(args.workload)
+    if args.workload == "batched":
+        # the reference has no batched form: its callers loop over hmlSgemm,
+        # here over its CPU loop, on the first 64 problems of the batch
+        problems = problems[:64]
     per_step = max(1.0, 120.0 / max(1, args.steps + args.warmup))
     per_step = min(per_step, 10.0)
     vals = []
@@ -302,6 +311,7 @@ def run_reference(args):
     step_flops = sum(flops_of(*p) for p in problems)
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT,
+        "sample_problems": len(problems),
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": step_flops / (value * 1e12) * 1e3, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
@@ -320,6 +330,7 @@ def run_ours(args):
 
     import hiperml_b200 as hml
     from hiperml_b200 import datagen as dg
+    from hiperml_b200.dist import max_over_ranks
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -335,7 +346,7 @@ def run_ours(args):
     torch.cuda.set_device(dev)
     stream = torch.cuda.current_stream()
 
-    problems = workload_problems(args.workload)
+    problems = workload_problems(args.workload, args.rows, args.only_n)
     algo = {"auto": None, "simt": 1, "bf16x3": 2, "bf16x6": 3}[args.algo]
 
     # ---- device operands (one A shared by the sweep's GEMMs)
@@ -417,10 +428,7 @@ def run_ours(args):
         # the flush is outside the measured GEMM events; time only the GEMMs
         elapsed_ms = sum(sum(ev[i][j][0].elapsed_time(ev[i][j][1]) for j in range(n_items))
                          for i in range(args.steps))
-    if dist_on:
-        t = torch.tensor([elapsed_ms], device=dev, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        elapsed_ms = float(t.item())
+    elapsed_ms = max_over_ranks(elapsed_ms, dev)
     if hml.device_error() != 0:
         raise RuntimeError("device wait expired in the timed region")
 
@@ -491,10 +499,7 @@ def run_ours(args):
         for _ in range(e2e_steps):
             e2e_step()
         te = time.perf_counter() - ts
-        if dist_on:
-            t = torch.tensor([te], device=dev, dtype=torch.float64)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            te = float(t.item())
+        te = max_over_ranks(te, dev)
         h2d = sum(4 * (M * K + K * N) for (_, _, _, M, N, K) in hosts)
         d2h = sum(4 * M * N for (_, _, _, M, N, K) in hosts)
         e2e = {"value": step_flops * e2e_steps * world / te / 1e12, "unit": UNIT,
@@ -515,7 +520,9 @@ def run_ours(args):
             "ms_per_step": elapsed_ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": dict(config_desc(args.workload),
-                           parallelism=f"independent per-GPU problems x{world}"),
+                           parallelism=f"independent per-GPU problems x{world}",
+                           **({"rows_override": args.rows} if args.rows else {}),
+                           **({"only_n": args.only_n} if args.only_n else {})),
             "roofline": roof, "cpu_baseline": cpu, "e2e": e2e,
             "clocks": clocks.summary(), "gpu_launches": int(launches),
             "per_shape": per_shape,
@@ -535,7 +542,7 @@ def run_batched(args):
 
     import hiperml_b200 as hml
     from hiperml_b200 import datagen as dg
-    from hiperml_b200._lib import check
+    from hiperml_b200.dist import max_over_ranks
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -599,10 +606,7 @@ def run_batched(args):
         dist.barrier()
     elapsed_ms = t0.elapsed_time(t1)
     per_launch_ms = statistics.mean(a.elapsed_time(b) for a, b in evs)
-    if dist_on:
-        t = torch.tensor([elapsed_ms], device=dev, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        elapsed_ms = float(t.item())
+    elapsed_ms = max_over_ranks(elapsed_ms, dev)
     step_flops = info["flops"]
     value = step_flops * args.steps * world / (elapsed_ms * 1e-3) / 1e12
 
@@ -657,10 +661,7 @@ def run_batched(args):
         for _ in range(reps):
             e2e_step()
         te = (time.perf_counter() - ts) / reps
-        if dist_on:
-            t = torch.tensor([te], device=dev, dtype=torch.float64)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            te = float(t.item())
+        te = max_over_ranks(te, dev)
         e2e = {"value": step_flops * world / te / 1e12, "unit": UNIT,
                "h2d_bytes_per_step": 4 * (poolA.numel() + poolB.numel()),
                "d2h_bytes_per_step": 4 * poolC.numel(),

@@ -52,6 +52,13 @@ class GemmDesc(ctypes.Structure):
                 ("C", ctypes.c_void_p)]
 
 
+class PredictorOptions(ctypes.Structure):
+    """``hml_predictor_options``."""
+    _fields_ = [("epochs", ctypes.c_int32), ("batch", ctypes.c_int32), ("lr", ctypes.c_float),
+                ("weight_decay", ctypes.c_float), ("target_clip", ctypes.c_float),
+                ("seed", ctypes.c_uint64)]
+
+
 _SIGS = {
     "hml_status_string": (c_char_p, [c_int]),
     "hml_version": (c_char_p, []),
@@ -105,6 +112,17 @@ _SIGS = {
                                     ctypes.POINTER(ctypes.c_double)]),
     "hml_batch_plan_destroy": (c_int, [c_void_p]),
     "hml_sgemm_batched": (c_int, [c_int, ctypes.POINTER(GemmDesc), c_int, c_void_p]),
+    "hml_predictor_train": (c_int, [c_int, c_void_p, c_void_p, c_int, ctypes.POINTER(SgemmConfig),
+                                    c_int, ctypes.POINTER(PredictorOptions), c_void_p]),
+    "hml_predictor_loss_grad": (c_int, [c_void_p, c_int, c_void_p, c_void_p, c_void_p, c_int,
+                                        c_void_p, c_void_p]),
+    "hml_predictor_predict_batch": (c_int, [c_int, c_void_p, c_int, c_void_p]),
+    "hml_predictor_save": (c_int, [c_char_p]),
+    "hml_predictor_load": (c_int, [c_char_p]),
+    "hml_predictor_clear": (c_int, []),
+    "hml_predictor_outputs": (c_int, []),
+    "hml_predictor_params": (c_int, [c_void_p, ctypes.c_size_t, ctypes.POINTER(ctypes.c_size_t)]),
+    "hml_predictor_features": (c_int, [c_int, c_int, c_int, c_int, c_int, c_int, c_void_p]),
 }
 
 for _name, (_res, _args) in _SIGS.items():

@@ -215,7 +215,7 @@ hml_status hml_sgemm_ex(hml_order order, hml_op transA, hml_op transB, int M, in
   GemvProblem g;
   if (as_gemv(p, &g)) return launch_gemv(g, 0, s);
   hml_sgemm_config c;
-  st = select_config(p, &c);
+  st = select_config(p, &c, s);
   if (st != HML_STATUS_SUCCESS) return st;
   return run_config(p, c, s);
 }
@@ -241,7 +241,7 @@ hml_status hml_sgemm_select(hml_order order, hml_op transA, hml_op transB, int M
   const int lda = std::max(1, cm ? (transA == HML_OP_N ? M : K) : (transA == HML_OP_N ? K : M));
   const int ldb = std::max(1, cm ? (transB == HML_OP_N ? K : N) : (transB == HML_OP_N ? N : K));
   const int ldc = std::max(1, cm ? M : N);
-  static float dummy[4];
+  alignas(16) static float dummy[4];
   hml_status st = gemm_from_blas(order, transA, transB, M, N, K, 1.0f, dummy, lda, dummy, ldb,
                                  0.0f, dummy, ldc, &p);
   if (st != HML_STATUS_SUCCESS) return st;

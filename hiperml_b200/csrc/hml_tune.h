@@ -9,6 +9,9 @@ bool check_config_ok(const GemmProblem &p, const hml_sgemm_config &c);
 // Fill *c from the measured table / the predictor; false when neither holds
 // an answer for this problem.
 bool tuned_lookup(const GemmProblem &p, hml_sgemm_config *c);
-bool predictor_lookup(const GemmProblem &p, hml_sgemm_config *c);
+// The predictor runs its inference kernel on a private stream the first
+// time it sees a shape class; `s` is the caller's stream, checked so that a
+// stream under capture is not made to wait.
+bool predictor_lookup(const GemmProblem &p, hml_sgemm_config *c, cudaStream_t s);
 int math_mode();
 }  // namespace hml

@@ -83,9 +83,9 @@ hml_sgemm_config heuristic_config(const GemmProblem &p, int algo) {
   return c;
 }
 
-hml_status select_config(const GemmProblem &p, hml_sgemm_config *c) {
+hml_status select_config(const GemmProblem &p, hml_sgemm_config *c, cudaStream_t s) {
   if (tuned_lookup(p, c) && check_config_ok(p, *c)) return HML_STATUS_SUCCESS;
-  if (predictor_lookup(p, c) && check_config_ok(p, *c)) return HML_STATUS_SUCCESS;
+  if (predictor_lookup(p, c, s) && check_config_ok(p, *c)) return HML_STATUS_SUCCESS;
   // Measured on B200 (M = 65536, K = 4096): FP32 SIMT wins at N <= 16 (the
   // HBM-bound GEMV-like shapes); the split-BF16 tensor-core forms win from
   // N = 32 on.  BF16X6 keeps FP32-level accuracy; BF16X3 (faster, ~2**-17)

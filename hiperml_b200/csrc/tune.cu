@@ -203,9 +203,17 @@ hml_status autotune(hml_order order, hml_op ta, hml_op tb, int M, int N, int K,
   if (M < 1 || N < 1 || K < 1 || reps < 1 || reps > 50) return HML_STATUS_INVALID_VALUE;
   if (families == 0) families = (1u << HML_ALGO_SIMT) | (1u << HML_ALGO_BF16X3) | (1u << HML_ALGO_BF16X6);
   const bool cm = order == HML_COL_MAJOR;
-  const int lda = std::max(1, cm ? (ta == HML_OP_N ? M : K) : (ta == HML_OP_N ? K : M));
-  const int ldb = std::max(1, cm ? (tb == HML_OP_N ? K : N) : (tb == HML_OP_N ? N : K));
-  const int ldc = std::max(1, cm ? M : N);
+  // leading dimensions rounded up to 16 bytes, the layout every kernel
+  // family (TMA included) can address
+  auto r4 = [](int x) { return (std::max(1, x) + 3) / 4 * 4; };
+  const int lda = r4(cm ? (ta == HML_OP_N ? M : K) : (ta == HML_OP_N ? K : M));
+  const int ldb = r4(cm ? (tb == HML_OP_N ? K : N) : (tb == HML_OP_N ? N : K));
+  const int ldc = r4(cm ? M : N);
+  // stored extents: ld x (number of ld-strided lines: columns in
+  // column-major order, rows in row-major order)
+  const size_t a_lines = cm ? (ta == HML_OP_N ? K : M) : (ta == HML_OP_N ? M : K);
+  const size_t b_lines = cm ? (tb == HML_OP_N ? N : K) : (tb == HML_OP_N ? K : N);
+  const size_t c_lines = cm ? N : M;
   std::lock_guard<std::mutex> lk(g_mu);  // one tuning at a time
   int dev = 0;
   cudaGetDevice(&dev);
@@ -215,9 +223,9 @@ hml_status autotune(hml_order order, hml_op ta, hml_op tb, int M, int N, int K,
     g_bufs.dev = dev;
   }
   hml_status st;
-  if ((st = grow(&g_bufs.A, &g_bufs.nA, static_cast<size_t>(M) * K, s, 101)) != HML_STATUS_SUCCESS ||
-      (st = grow(&g_bufs.B, &g_bufs.nB, static_cast<size_t>(K) * N, s, 102)) != HML_STATUS_SUCCESS ||
-      (st = grow(&g_bufs.C, &g_bufs.nC, static_cast<size_t>(M) * N, s, 103)) != HML_STATUS_SUCCESS ||
+  if ((st = grow(&g_bufs.A, &g_bufs.nA, a_lines * lda, s, 101)) != HML_STATUS_SUCCESS ||
+      (st = grow(&g_bufs.B, &g_bufs.nB, b_lines * ldb, s, 102)) != HML_STATUS_SUCCESS ||
+      (st = grow(&g_bufs.C, &g_bufs.nC, c_lines * ldc, s, 103)) != HML_STATUS_SUCCESS ||
       (st = grow(&g_bufs.flush, &g_bufs.nflush, size_t(64) << 20, s, 104)) != HML_STATUS_SUCCESS)
     return st;
   GemmProblem p;

@@ -1,0 +1,129 @@
+"""Measured tuning data for the configuration predictor.
+
+The predictor learns from what the autotuner (``hml_autotune_sgemm``)
+measures: for each sampled problem shape, the median device time of every
+configuration of the library's space (-1 where a configuration cannot run the
+shape).  This module draws the shapes and runs the measurements; the result
+is an ``.npz`` file with
+
+    shapes   int64 [n, 5]   M, N, K, transA, transB (column-major storage)
+    times_us float32 [n, C] measured time per configuration, -1 = not run
+    configs  int32 [C, 6]   the configuration space (algo, tile_m, tile_n,
+                            split_k, stages, variant), column order of times_us
+    device   str
+
+Usage (on the GPU):  python -m hiperml_b200.tuning_data OUT.npz --count 5000
+"""
+from __future__ import annotations
+
+import argparse
+import time
+
+import numpy as np
+
+# Shape distribution: M, N, K log-uniform in [1, 65536] x [1, 256] x
+# [16, 16384], transposes Bernoulli(0.5).
+M_RANGE, N_RANGE, K_RANGE = (1, 65536), (1, 256), (16, 16384)
+
+
+def _log_uniform(rng, lo, hi, n):
+    v = np.exp(rng.uniform(np.log(lo), np.log(hi + 1), n))
+    return np.clip(np.floor(v), lo, hi).astype(np.int64)
+
+
+def sample_shapes(count: int, seed: int) -> np.ndarray:
+    """`count` shapes (M, N, K, transA, transB) from the distribution above,
+    leaving out GEMV shapes (min(M, N) == 1, served by the GEMV kernels, where
+    no configuration applies): draws are repeated until `count` remain."""
+    rng = np.random.default_rng(seed)
+    out = []
+    while len(out) < count:
+        n = 2 * (count - len(out)) + 16
+        M = _log_uniform(rng, *M_RANGE, n)
+        N = _log_uniform(rng, *N_RANGE, n)
+        K = _log_uniform(rng, *K_RANGE, n)
+        ta = rng.integers(0, 2, n)
+        tb = rng.integers(0, 2, n)
+        for i in range(n):
+            if min(M[i], N[i]) > 1:
+                out.append((M[i], N[i], K[i], ta[i], tb[i]))
+                if len(out) == count:
+                    break
+    return np.asarray(out, dtype=np.int64)
+
+
+def config_table() -> np.ndarray:
+    from . import api
+    return np.asarray([c.as_tuple() for c in api.configs()], dtype=np.int32)
+
+
+def measure(shapes: np.ndarray, reps: int = 3, deadline: float | None = None,
+            progress=None) -> np.ndarray:
+    """Autotunes every shape (all algorithm families).  Returns times_us
+    [n, C]; rows of shapes not reached before `deadline` (time.time()) stay
+    NaN."""
+    from . import api
+    cfgs = config_table()
+    index = {tuple(c): i for i, c in enumerate(cfgs)}
+    times = np.full((len(shapes), len(cfgs)), np.nan, dtype=np.float32)
+    for r, (M, N, K, ta, tb) in enumerate(shapes):
+        if deadline is not None and time.time() > deadline:
+            break
+        ents = api.autotune(api.COL_MAJOR, int(ta), int(tb), int(M), int(N), int(K), reps=reps)
+        row = np.full(len(cfgs), -1.0, dtype=np.float32)
+        for c, t, st in ents:
+            if st == 0 and t > 0:
+                row[index[c.as_tuple()]] = t
+        times[r] = row
+        api.tune_clear()  # the dataset, not the tuned table, keeps the results
+        if progress is not None:
+            progress(r)
+    return times
+
+
+def save(path, shapes, times, cfgs, device):
+    np.savez_compressed(path, shapes=shapes, times_us=times.astype(np.float32), configs=cfgs,
+                        device=np.asarray(device))
+
+
+def load(path):
+    d = np.load(path, allow_pickle=False)
+    return {k: d[k] for k in d.files}
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("out")
+    ap.add_argument("--count", type=int, default=5000)
+    ap.add_argument("--seed", type=int, default=5)
+    ap.add_argument("--reps", type=int, default=3)
+    ap.add_argument("--max-seconds", type=float, default=3000.0)
+    ap.add_argument("--save-every", type=int, default=250)
+    args = ap.parse_args(argv)
+    import torch
+    shapes = sample_shapes(args.count, args.seed)
+    cfgs = config_table()
+    device = torch.cuda.get_device_name(0)
+    deadline = time.time() + args.max_seconds
+    t0 = time.time()
+    state = {"times": None}
+
+    def progress(r):
+        if (r + 1) % args.save_every == 0:
+            print(f"{r + 1} shapes, {time.time() - t0:.0f} s", flush=True)
+
+    # measure in blocks so partial results are saved
+    times = np.full((len(shapes), len(cfgs)), np.nan, dtype=np.float32)
+    for b0 in range(0, len(shapes), args.save_every):
+        blk = measure(shapes[b0:b0 + args.save_every], reps=args.reps, deadline=deadline)
+        times[b0:b0 + len(blk)] = blk
+        done = ~np.isnan(times[:, 0])
+        save(args.out, shapes[done], times[done], cfgs, device)
+        print(f"{done.sum()} shapes measured, {time.time() - t0:.0f} s", flush=True)
+        if time.time() > deadline:
+            break
+    return 0
+
+
+if __name__ == "__main__":
+    raise SystemExit(main())

@@ -79,8 +79,12 @@ const char *hml_version(void);
 
 /* C = alpha * op(A) * op(B) + beta * C on device pointers.  op(A) is M x K,
  * op(B) is K x N, C is M x N.  The configuration comes from the tuned table
- * (hml_tune_load / hml_autotune_sgemm), else the learned predictor when one
- * is loaded, else the built-in heuristic.  Replaces the launch half of
+ * (hml_tune_load / hml_autotune_sgemm), else the learned predictor, else the
+ * built-in heuristic.  The predictor is the one loaded by hml_predictor_load
+ * or trained by hml_predictor_train; without either, the first selection
+ * loads the network shipped as data/predictor_b200.txt beside the library
+ * (environment: HML_PREDICTOR=<file> names another, HML_PREDICTOR=none
+ * disables it).  Replaces the launch half of
  * hmlSgemm (src/hml_sgemm.cu:120-211 in the reference), generalised to
  * both storage orders, transposes and leading dimensions. */
 hml_status hml_sgemm_ex(hml_order order, hml_op transA, hml_op transB, int M,
@@ -160,7 +164,8 @@ typedef struct hml_tune_entry {
 
 /* Measures every configuration of the space (restricted to the algorithm
  * families in the bitmask `families`, bit = 1 << hml_algo; 0 = all) on this
- * problem shape with dense leading dimensions and uniform[-1,1] operands:
+ * problem shape with leading dimensions rounded up to a multiple of 4 floats
+ * (16 bytes, addressable by every kernel family) and uniform[-1,1] operands:
  * one warm-up call, then `reps` calls timed with CUDA events on the stream,
  * L2 flushed before each when the operands fit in it, median kept.  A
  * configuration that cannot run or fails is recorded with its status and
@@ -183,6 +188,64 @@ int hml_tune_size(void);
 
 /* Selects the accuracy policy (hml_math_mode) of automatic selection. */
 hml_status hml_set_math_mode(int mode);
+
+/* ---------------------------------------------------- learned predictor */
+
+/* A small MLP (5 -> 64 -> 64 -> one score per configuration) that predicts
+ * the fastest configuration of an unseen shape from autotuner measurements,
+ * replacing the reference's static per-GPU tables
+ * (src/hml_sgemm_kernel.cu:189-237).  Features of the canonical (long-M)
+ * problem: log2 M / 16, log2 N / 8, log2 K / 14, A K-contiguous,
+ * B K-contiguous.  Scores regress y = min(log(t / t_best), target_clip) per
+ * measured configuration (masked mean squared error); the prediction is the
+ * lowest score among the configurations that can run the problem and that
+ * the math mode allows.  Training and inference run on the GPU in this
+ * library's own kernels. */
+typedef struct hml_predictor_options {
+  int32_t epochs;      /* passes over the training shapes                   */
+  int32_t batch;       /* shapes per AdamW step                             */
+  float lr;            /* peak learning rate (cosine decay to 5 %)          */
+  float weight_decay;  /* AdamW decoupled weight decay                      */
+  float target_clip;   /* cap on log(t / t_best)                            */
+  uint64_t seed;       /* initialisation and shuffling (SplitMix64)         */
+} hml_predictor_options;
+
+/* Trains on n shapes (shapes: n x 5 int32 rows M, N, K, transA, transB in
+ * `order` with 16-byte-rounded leading dimensions, the autotuner's layout)
+ * and their measured times (times_us: n x n_configs, <= 0 where a
+ * configuration was not measured; column j belongs to configs[j]).  The
+ * trained network becomes the active predictor; loss_history (may be NULL)
+ * receives the mean training loss of each epoch. */
+hml_status hml_predictor_train(hml_order order, const int32_t *shapes,
+                               const float *times_us, int n,
+                               const hml_sgemm_config *configs, int n_configs,
+                               const hml_predictor_options *options,
+                               float *loss_history);
+
+/* Loss and gradient of the network with parameters `params` (layout W1[64][5]
+ * b1[64] W2[64][64] b2[64] W3[C][64] b3[C]) on n rows of features (n x 5),
+ * targets and weights (n x C), computed by the training kernels.  Host
+ * arrays; synchronous.  loss = sum w (s - y)^2 / sum w. */
+hml_status hml_predictor_loss_grad(const float *params, int n_configs,
+                                   const float *features, const float *targets,
+                                   const float *weights, int n, float *grad,
+                                   float *loss);
+
+/* The active predictor's choice (an index into its configuration list, -1
+ * when none can run) for n shapes in one inference launch. */
+hml_status hml_predictor_predict_batch(hml_order order, const int32_t *shapes,
+                                       int n, int32_t *config_index);
+
+hml_status hml_predictor_save(const char *path);
+hml_status hml_predictor_load(const char *path);
+hml_status hml_predictor_clear(void);
+/* Number of configurations the active predictor scores (0: none loaded). */
+int hml_predictor_outputs(void);
+/* Copies the active predictor's parameters (count = their number). */
+hml_status hml_predictor_params(float *out, size_t capacity, size_t *count);
+/* The feature vector of a shape (same layout convention as training). */
+hml_status hml_predictor_features(hml_order order, int transA, int transB,
+                                  int M, int N, int K, float features[5]);
 
 /* ------------------------------------------------------------- batched */
 

@@ -4,6 +4,11 @@ import sys
 import pytest
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+# Selection tests check the built-in heuristic; the shipped predictor network
+# (loaded by the library on first use unless HML_PREDICTOR says otherwise) is
+# exercised by its own tests, which load it explicitly.
+os.environ.setdefault("HML_PREDICTOR", "none")
 if ROOT not in sys.path:
     sys.path.insert(0, ROOT)
 
