@@ -58,10 +58,10 @@ def config_table() -> np.ndarray:
 
 
 def measure(shapes: np.ndarray, reps: int = 3, deadline: float | None = None,
-            progress=None) -> np.ndarray:
-    """Autotunes every shape (all algorithm families).  Returns times_us
-    [n, C]; rows of shapes not reached before `deadline` (time.time()) stay
-    NaN."""
+            progress=None, families: int = 0) -> np.ndarray:
+    """Autotunes every shape (the algorithm families of the bitmask, 0 = all).
+    Returns times_us [n, C]; configurations outside the families are -1, and
+    rows of shapes not reached before `deadline` (time.time()) stay NaN."""
     from . import api
     cfgs = config_table()
     index = {tuple(c): i for i, c in enumerate(cfgs)}
@@ -69,7 +69,8 @@ def measure(shapes: np.ndarray, reps: int = 3, deadline: float | None = None,
     for r, (M, N, K, ta, tb) in enumerate(shapes):
         if deadline is not None and time.time() > deadline:
             break
-        ents = api.autotune(api.COL_MAJOR, int(ta), int(tb), int(M), int(N), int(K), reps=reps)
+        ents = api.autotune(api.COL_MAJOR, int(ta), int(tb), int(M), int(N), int(K),
+                            families=families, reps=reps)
         row = np.full(len(cfgs), -1.0, dtype=np.float32)
         for c, t, st in ents:
             if st == 0 and t > 0:
@@ -99,23 +100,33 @@ def main(argv=None):
     ap.add_argument("--reps", type=int, default=3)
     ap.add_argument("--max-seconds", type=float, default=3000.0)
     ap.add_argument("--save-every", type=int, default=250)
+    ap.add_argument("--families", type=int, default=0,
+                    help="bitmask of algorithm families to measure (1 << hml_algo; 0 = all)")
+    ap.add_argument("--merge", default=None,
+                    help="existing dataset: its shapes are re-measured for --families only "
+                         "and its other columns kept")
     args = ap.parse_args(argv)
     import torch
-    shapes = sample_shapes(args.count, args.seed)
+    base = load(args.merge) if args.merge else None
+    shapes = base["shapes"] if base is not None else sample_shapes(args.count, args.seed)
     cfgs = config_table()
+    if base is not None and not np.array_equal(base["configs"], cfgs):
+        raise SystemExit("--merge: the dataset was measured on another configuration space")
+    fam_cols = (np.ones(len(cfgs), bool) if args.families == 0
+                else ((1 << cfgs[:, 0]) & args.families) != 0)
     device = torch.cuda.get_device_name(0)
     deadline = time.time() + args.max_seconds
     t0 = time.time()
-    state = {"times": None}
-
-    def progress(r):
-        if (r + 1) % args.save_every == 0:
-            print(f"{r + 1} shapes, {time.time() - t0:.0f} s", flush=True)
-
-    # measure in blocks so partial results are saved
+    # measure in blocks so partial results are saved (with --merge, a shape
+    # not reached before the deadline is left out rather than kept stale)
     times = np.full((len(shapes), len(cfgs)), np.nan, dtype=np.float32)
     for b0 in range(0, len(shapes), args.save_every):
-        blk = measure(shapes[b0:b0 + args.save_every], reps=args.reps, deadline=deadline)
+        blk = measure(shapes[b0:b0 + args.save_every], reps=args.reps, deadline=deadline,
+                      families=args.families)
+        if base is not None:
+            done_blk = ~np.isnan(blk[:, 0])
+            old = base["times_us"][b0:b0 + len(blk)]
+            blk = np.where(fam_cols[None, :] | ~done_blk[:, None], blk, old)
         times[b0:b0 + len(blk)] = blk
         done = ~np.isnan(times[:, 0])
         save(args.out, shapes[done], times[done], cfgs, device)
