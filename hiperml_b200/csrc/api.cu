@@ -115,7 +115,7 @@ std::vector<hml_sgemm_config> build_space() {
       int bm, bn;
       tc_shape(var, &bm, &bn);
       for (int split : {1, 2, 4, 8, 16})
-        for (int stages : {2, 3, 4, 6}) {
+        for (int stages : {2, 4, 6, 8}) {  // A-ring depths: multiples of the converter groups
           if (!tc_config_fits(bn, algo == HML_ALGO_BF16X3 ? 2 : 3, stages)) continue;
           hml_sgemm_config c = {algo, bm, bn, split, stages, var};
           v.push_back(c);

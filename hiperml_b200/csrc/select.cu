@@ -56,7 +56,7 @@ hml_sgemm_config heuristic_config(const GemmProblem &p, int algo) {
       tc_shape(best, &bm, &bn);
       const int64_t tiles = ((p.M + bm - 1) / bm) * static_cast<int64_t>((p.N + bn - 1) / bn);
       int stages = 2;
-      for (int st : {3, 4, 6})
+      for (int st : {4, 6, 8})
         if (tc_config_fits(bn, algo == HML_ALGO_BF16X3 ? 2 : 3, st)) stages = st;
       c = {algo, bm, bn, choose_split(tiles, p.K, 1, 256), stages, best};
       return c;

@@ -9,31 +9,36 @@
 // The result is C = alpha * A * B + beta * C in FP32, the reference's
 // hmlSgemm contract (src/hml_sgemm.cu:120-211) on a different machine.
 //
-// Data flow of one CTA (a 128-row tile of C, BN columns, a K range):
+// Data flow of one CTA (a 128-row tile of C, BN columns, a K range), in
+// 32-deep K blocks:
 //   * B is small (K x N): a pre-pass splits it once into BF16 planes stored
-//     K-contiguous in a workspace ([plane][N_pad][K_pad]); the kernel loads
-//     plane tiles with TMA straight into the UMMA canonical K-major layout
-//     (64-byte swizzle, 32 BF16 per row).
-//   * A streams from HBM exactly once: a TMA thread loads 128 x 32 FP32 tiles
-//     into a ring of `stages` slots, each released as soon as the converter
-//     warps have read it (B tiles live in a separate ring released by the
-//     MMAs, so HBM latency is hidden by the A ring alone).
-//   * sixteen converter warps split each FP32 tile into BF16 planes written in
-//     the same canonical layout (a transpose when A is M-contiguous) into one
-//     of two converted buffers, then signal the MMA warp.
-//   * one thread of the MMA warp issues tcgen05.mma (M=128, N=BN, K=16, both
-//     operands from shared memory, FP32 accumulator in TMEM) and releases
-//     ring slots and buffers with tcgen05.commit.
+//     K-contiguous in a workspace ([plane][N_pad][K_pad]); a TMA warp loads
+//     plane tiles straight into the UMMA canonical K-major layout (64-byte
+//     swizzle, 32 BF16 per row).
+//   * A streams from HBM exactly once: a TMA warp loads 128 x 32 FP32 tiles
+//     into a ring of shared-memory slots.
+//   * G converter warpgroups take the blocks round-robin (group g converts
+//     blocks g, g+G, ...), so G blocks are in conversion at once.  Thread m of
+//     a group owns row m of the tile, which is also TMEM lane m: it reads the
+//     row's 32 FP32 values, splits them, and writes the BF16 planes into a
+//     TMEM stage with tcgen05.st (two BF16 per 32-bit column).  The MMAs read
+//     A from TMEM (the tcgen05.mma form with A in tensor memory), so the
+//     converted planes never touch shared memory.
+//   * NI threads (2 to 4, one per accumulator) issue tcgen05.mma (M=128,
+//     N=BN, K=16; A from TMEM, B from shared memory; FP32 accumulator in
+//     TMEM), each for every NI-th 64-deep chunk, and release each operand
+//     stage (B slot + A stage) with one tcgen05.commit.
 //   * the tensor core's FP32 accumulation truncates, so a long accumulation
 //     chain in TMEM loses accuracy as K grows.  Each 64-deep chunk of K is
-//     accumulated into one of two TMEM accumulators; the converter warps then
-//     read it (tcgen05.ld) and add it into FP32 running sums held in
-//     registers (round to nearest) while the tensor core fills the other.
-//   * the converter warps apply alpha/beta from the running sums; with
-//     split_k > 1 the CTAs of one thread-block cluster sum their tiles in
-//     rank order through distributed shared memory.
+//     accumulated into one of NI TMEM accumulators; drain warpgroups read it
+//     (tcgen05.ld) and add it into FP32 running sums held in registers
+//     (round to nearest) while the tensor core fills the others.
+//   * the drain warps apply alpha/beta; with split_k > 1 the CTAs of one
+//     thread-block cluster sum their tiles in rank order through distributed
+//     shared memory.
 // Every wait is bounded (2 s of %globaltimer); on expiry the device error
-// word is set, the CTA skips ahead, frees its TMEM and returns.
+// word is set, the CTA skips ahead, waits for its issued MMAs, frees its TMEM
+// and returns.
 #include <cuda_bf16.h>
 
 #include <algorithm>
@@ -46,18 +51,63 @@
 namespace hml {
 namespace {
 
-constexpr int kBM = 128;        // rows of C per CTA = UMMA M
-constexpr int kBK = 32;         // K per ring stage (one 64-byte BF16 swizzle row)
-constexpr int kConvWarps = 16;  // converters + accumulator drain + epilogue
-constexpr int kLoadAWarp = kConvWarps, kLoadBWarp = kConvWarps + 1, kMmaWarp = kConvWarps + 2;
-constexpr int kThreads = (kConvWarps + 3) * 32;
-constexpr int kChunkK = 64;     // K accumulated in TMEM before an FP32 drain
+constexpr int kBM = 128;      // rows of C per CTA = UMMA M = TMEM lanes
+constexpr int kBK = 32;       // K per block (one 64-byte BF16 swizzle row)
+constexpr int kChunkK = 64;   // K accumulated in TMEM before an FP32 drain
+constexpr int kTmemCols = 512;
 
 struct TcShape {
   int bn;
 };
 constexpr TcShape kTcShapes[] = {{16}, {32}, {64}, {128}};
 constexpr int kNumTcShapes = sizeof(kTcShapes) / sizeof(kTcShapes[0]);
+
+// Warp roles of one CTA:
+//   warp 0       TMA loads of A (FP32 tiles)
+//   warp 1       TMA loads of B (BF16 plane tiles)
+//   warps 2..    NI MMA issuers (warp 2 also allocates TMEM); issuer i takes
+//                the 64-deep chunks q = i, i+NI, ... into accumulator i
+//   then, from the next warp index divisible by 4: G converter warpgroups,
+//   then D drain warpgroups.
+// A warp can reach only TMEM lanes 32 * (warp % 4) .. +31, so every
+// warpgroup that touches TMEM starts at a warp index divisible by 4 and its
+// warp q covers rows 32q .. 32q+31.
+//
+// Each thread's tcgen05.mma issue is serial (tens of ns an instruction), so
+// at small N one thread cannot keep up with the HBM stream; NI threads issue
+// into NI accumulators.  TMEM holds the NI accumulators (BN columns each)
+// and so A stages (NS x 16 columns each, two BF16 per 32-bit column).
+__host__ __device__ constexpr int tc_groups() { return 2; }
+__host__ __device__ constexpr int tc_drain_groups(int bn) { return bn > 64 ? 2 : 1; }
+// TMEM columns of one converted A block: NS planes x 32 BF16 (2 per column).
+__host__ __device__ constexpr int tc_stage_cols(int ns) { return ns * kBK / 2; }
+// Operand stages (B slot + A TMEM stage) with ni issuers: a multiple of
+// 2 * ni (blocks per chunk x issuers), so that every stage is only ever used
+// by one issuer and, as 2 * ni is even, by one converter group; at most 8.
+__host__ __device__ constexpr int tc_stage_mult(int ni) { return 2 * ni; }
+__host__ __device__ constexpr int tc_stages_for(int bn, int ns, int ni) {
+  return (((kTmemCols - ni * bn) / tc_stage_cols(ns) < 8 ? (kTmemCols - ni * bn) /
+                                                               tc_stage_cols(ns)
+                                                         : 8) /
+          tc_stage_mult(ni)) *
+         tc_stage_mult(ni);
+}
+// The most issuers (4 at most, 2 at least) whose accumulators leave room
+// for at least one stage multiple.
+__host__ __device__ constexpr int tc_issuers(int bn, int ns) {
+  return tc_stages_for(bn, ns, 4) >= tc_stage_mult(4)   ? 4
+         : tc_stages_for(bn, ns, 3) >= tc_stage_mult(3) ? 3
+                                                        : 2;
+}
+__host__ __device__ constexpr int tc_max_stages(int bn, int ns) {
+  return tc_stages_for(bn, ns, tc_issuers(bn, ns));
+}
+__host__ __device__ constexpr int tc_conv_warp0(int bn, int ns) {
+  return ((2 + tc_issuers(bn, ns) + 3) / 4) * 4;
+}
+__host__ __device__ constexpr int tc_warps(int bn, int ns) {
+  return tc_conv_warp0(bn, ns) + 4 * tc_groups() + 4 * tc_drain_groups(bn);
+}
 
 // ------------------------------------------------------------ tcgen05
 __device__ __forceinline__ void tmem_alloc(uint32_t *dst_smem, uint32_t ncols) {
@@ -80,13 +130,15 @@ __device__ __forceinline__ void tc_fence_after() {
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
 }
 
-__device__ __forceinline__ void mma_bf16(uint32_t dtmem, uint64_t adesc, uint64_t bdesc,
-                                         uint32_t idesc, uint32_t accumulate) {
+// D (TMEM) (+)= A (TMEM, 128 lanes x 16 BF16 in 8 columns) * B (shared
+// memory descriptor), kind::f16 with BF16 inputs and an FP32 accumulator.
+__device__ __forceinline__ void mma_bf16_ts(uint32_t dtmem, uint32_t atmem, uint64_t bdesc,
+                                            uint32_t idesc, uint32_t accumulate) {
   asm volatile(
       "{\n\t.reg .pred p;\n\t"
       "setp.ne.b32 p, %4, 0;\n\t"
-      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(dtmem),
-      "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], [%1], %2, %3, p;\n\t}" ::"r"(dtmem),
+      "r"(atmem), "l"(bdesc), "r"(idesc), "r"(accumulate)
       : "memory");
 }
 
@@ -97,31 +149,17 @@ __device__ __forceinline__ void mma_commit(uint64_t *bar) {
       : "memory");
 }
 
-// 32 lanes x 4 / 8 / 16 consecutive 32-bit columns of TMEM into registers.
-__device__ __forceinline__ void tmem_ld4(uint32_t taddr, float *v) {
-  uint32_t r[4];
-  asm volatile("tcgen05.ld.sync.aligned.32x32b.x4.b32 {%0, %1, %2, %3}, [%4];"
-               : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
-               : "r"(taddr));
-  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-#pragma unroll
-  for (int i = 0; i < 4; ++i) v[i] = __uint_as_float(r[i]);
-}
-
-__device__ __forceinline__ void tmem_ld8(uint32_t taddr, float *v) {
-  uint32_t r[8];
+// 32 lanes x 8 / 16 consecutive 32-bit columns of TMEM into registers (the
+// caller issues tmem_wait_ld before using them).
+__device__ __forceinline__ void tmem_ld8(uint32_t taddr, uint32_t (&r)[8]) {
   asm volatile(
       "tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
       : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
         "=r"(r[7])
       : "r"(taddr));
-  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-#pragma unroll
-  for (int i = 0; i < 8; ++i) v[i] = __uint_as_float(r[i]);
 }
 
-__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float *v) {
-  uint32_t r[16];
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&r)[16]) {
   asm volatile(
       "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, "
       "%11, %12, %13, %14, %15}, [%16];"
@@ -129,9 +167,25 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float *v) {
         "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]),
         "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
       : "r"(taddr));
+}
+
+__device__ __forceinline__ void tmem_wait_ld() {
   asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-#pragma unroll
-  for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+// 32 lanes x 16 consecutive 32-bit columns from registers into TMEM.
+__device__ __forceinline__ void tmem_st16(uint32_t taddr, const uint32_t (&r)[16]) {
+  asm volatile(
+      "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8, %9, "
+      "%10, %11, %12, %13, %14, %15, %16};" ::"r"(taddr),
+      "r"(r[0]), "r"(r[1]), "r"(r[2]), "r"(r[3]), "r"(r[4]), "r"(r[5]), "r"(r[6]), "r"(r[7]),
+      "r"(r[8]), "r"(r[9]), "r"(r[10]), "r"(r[11]), "r"(r[12]), "r"(r[13]), "r"(r[14]),
+      "r"(r[15])
+      : "memory");
+}
+
+__device__ __forceinline__ void tmem_wait_st() {
+  asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
 }
 
 // Shared-memory matrix descriptor: K-major, 64-byte swizzle (rows of 64 B),
@@ -142,12 +196,6 @@ __device__ __forceinline__ uint64_t sw64_desc(uint32_t saddr) {
          (static_cast<uint64_t>(4) << 61);
 }
 
-// Byte offset of the 16-byte chunk `c` (0..3) of row `r` in a 64-byte-row
-// tile with the 64-byte swizzle (chunk bits 4-5 XOR address bits 7-8).
-__device__ __forceinline__ uint32_t sw64_off(int r, int c) {
-  return static_cast<uint32_t>(r * 64 + ((c ^ ((r >> 1) & 3)) << 4));
-}
-
 // Instruction descriptor: BF16 x BF16 -> F32, both K-major, M = 128, N = bn.
 __host__ __device__ constexpr uint32_t idesc_bf16(int bn) {
   return (1u << 4) | (1u << 7) | (1u << 10) | (static_cast<uint32_t>(bn >> 3) << 17) |
@@ -156,7 +204,7 @@ __host__ __device__ constexpr uint32_t idesc_bf16(int bn) {
 
 // Split eight floats into NS BF16 planes, t0 = bf16(x), t1 = bf16(x - t0),
 // ... (each residual is exact in FP32), packed two per 32-bit word with
-// cvt.rn.bf16x2.f32.
+// cvt.rn.bf16x2.f32 (the lower k in the low half, as in memory order).
 __device__ __forceinline__ uint32_t bf16x2_rn(float lo, float hi) {
   uint32_t r;
   asm("cvt.rn.bf16x2.f32 %0, %1, %2;" : "=r"(r) : "f"(hi), "f"(lo));
@@ -183,11 +231,27 @@ __device__ __forceinline__ void pack8(const float (&x)[8], uint4 (&out)[NS]) {
   for (int i = 0; i < NS; ++i) out[i] = make_uint4(w[i][0], w[i][1], w[i][2], w[i][3]);
 }
 
+// One plane of the same split for 32 consecutive values of one row: word j
+// holds elements 2j and 2j+1 rounded to BF16; unless this is the last plane,
+// x is left holding the residuals for the next one.
+template <bool LAST>
+__device__ __forceinline__ void split_plane32(float (&x)[32], uint32_t (&w)[16]) {
+#pragma unroll
+  for (int j = 0; j < 16; ++j) {
+    const uint32_t t = bf16x2_rn(x[2 * j], x[2 * j + 1]);
+    w[j] = t;
+    if (!LAST) {
+      x[2 * j] -= __uint_as_float(t << 16);
+      x[2 * j + 1] -= __uint_as_float(t & 0xFFFF0000u);
+    }
+  }
+}
+
 struct TcArgs {
   GemmProblem p;
   int split;       // CTAs per cluster along K
   int kc;          // K extent per split (multiple of kChunkK)
-  int sa, so;      // A ring and operand ring depths
+  int sa, so;      // A ring and operand-stage depths
   int n_pad;       // rows of one B plane in the workspace
   int *err;
 };
@@ -220,32 +284,35 @@ __global__ void split_b_kernel(const float *B, int64_t sbk, int64_t sbn, int K, 
 }
 
 // ------------------------------------------------------------- kernel
-// Shared-memory plan of one CTA (all tiles 1024-byte aligned):
-//   A ring        sa slots of the FP32 A tile (16 KB), filled by TMA and
-//                 released by the converter warps as soon as they have read
-//                 it, so HBM latency is covered by this ring alone;
-//   operand ring  so slots, each holding the NS B-plane tiles of one K block
-//                 (filled by TMA) and the NS converted A planes of the same
-//                 block (written by the converter warps).  One tcgen05.commit
-//                 releases a whole slot: the MMA thread's issue rate (about
-//                 30 ns a tcgen05.mma, 70 ns a tcgen05.commit) bounds the
-//                 kernel for skinny N, so commits are kept to one per block.
+// Shared-memory plan of one CTA (tiles 1024-byte aligned):
+//   A ring    sa slots of the FP32 A tile (16 KB), filled by TMA, released
+//             by the converter group that read it;
+//   B ring    so slots, each the NS B-plane tiles of one K block (TMA).
+// TMEM: NI accumulators of BN columns, then so A stages of NS x 16 columns.
+// Operand stage o = B slot o + A stage o, released together by one commit.
+// sa is a multiple of G and so a multiple of 2 * NI, so each slot is only
+// ever used by one converter group and each stage by one MMA issuer: a
+// waiter has always seen the previous phase of its barrier complete.
 struct TcPlan {
   int sa, so;
 };
 
 __host__ __device__ constexpr size_t tc_a_bytes() { return static_cast<size_t>(kBM) * kBK * 4; }
-__host__ __device__ constexpr size_t tc_op_bytes(int bn, int ns) {
-  return static_cast<size_t>(ns) * bn * kBK * 2 + static_cast<size_t>(ns) * kBM * kBK * 2;
+__host__ __device__ constexpr size_t tc_b_bytes(int bn, int ns) {
+  return static_cast<size_t>(ns) * bn * kBK * 2;
 }
 size_t tc_plan_bytes(int bn, int ns, const TcPlan &pl) {
-  return 1024 + pl.sa * tc_a_bytes() + pl.so * tc_op_bytes(bn, ns) + 8 * (2 * pl.sa + 2 * pl.so + 4) +
-         16;
+  return 1024 + pl.sa * tc_a_bytes() + pl.so * tc_b_bytes(bn, ns) +
+         8 * (2 * pl.sa + 2 * pl.so + 2 * 4 + 1) + 16;
 }
 
-// The deepest operand ring (2..6 slots) that fits next to sa A slots.
+// The deepest operand-stage ring that fits TMEM and shared memory next to
+// sa A slots; sa must be a multiple of G.
 bool tc_plan(int bn, int ns, int sa, TcPlan *out) {
-  for (int so = 6; so >= 2; --so) {
+  const int g = tc_groups();
+  if (sa < g || sa % g != 0) return false;
+  const int mult = tc_stage_mult(tc_issuers(bn, ns));
+  for (int so = tc_max_stages(bn, ns); so >= mult; so -= mult) {
     const TcPlan pl = {sa, so};
     if (tc_plan_bytes(bn, ns, pl) <= 227 * 1024) {
       *out = pl;
@@ -255,21 +322,29 @@ bool tc_plan(int bn, int ns, int sa, TcPlan *out) {
   return false;
 }
 
-// Warps 0-15: convert A, drain the accumulator, epilogue.  Warp 16 loads A,
-// warp 17 loads B (separate warps, so a load waiting on the MMA pipeline
-// never holds back the HBM stream), warp 18 allocates TMEM and issues MMAs.
+__host__ __device__ constexpr uint32_t tc_pow2_cols(int cols) {
+  return cols <= 32 ? 32 : cols <= 64 ? 64 : cols <= 128 ? 128 : cols <= 256 ? 256 : 512;
+}
+__host__ __device__ constexpr uint32_t tc_tmem_alloc_cols(int bn, int ns, int so) {
+  return tc_pow2_cols(tc_issuers(bn, ns) * bn + so * tc_stage_cols(ns));
+}
+
 template <int BN, int NS, bool AK>
-__global__ void __launch_bounds__(kThreads, 1)
+__global__ void __launch_bounds__(tc_warps(BN, NS) * 32, 1)
     tc_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
               TcArgs args) {
+  constexpr int G = tc_groups();
+  constexpr int D = tc_drain_groups(BN);
+  constexpr int DC = BN / D;                                 // columns per drain thread
+  constexpr int NI = tc_issuers(BN, NS);                     // MMA issuers = accumulators
+  constexpr int kThreads = tc_warps(BN, NS) * 32;
+  constexpr int kConvWarp0 = tc_conv_warp0(BN, NS), kDrainWarp0 = kConvWarp0 + 4 * G;
   constexpr int A32_BYTES = static_cast<int>(tc_a_bytes());  // FP32 A slot (16 KB)
   constexpr int BPL_BYTES = BN * kBK * 2;                    // one B plane tile
-  constexpr int APL_BYTES = kBM * kBK * 2;                   // one converted A plane (8 KB)
-  constexpr int OP_BYTES = NS * (BPL_BYTES + APL_BYTES);     // one operand slot
-  constexpr int QTR = BN / 4;                                // columns drained per thread
-  constexpr uint32_t TMEM_COLS = 2 * BN < 32 ? 32 : 2 * BN;  // two accumulators
+  constexpr int BSLOT = NS * BPL_BYTES;                      // one B slot
+  constexpr int SC = tc_stage_cols(NS);                      // TMEM columns of an A stage
   constexpr uint32_t IDESC = idesc_bf16(BN);
-  constexpr int P = kChunkK / kBK;                           // k-blocks per TMEM chunk
+  constexpr int P = kChunkK / kBK;                           // blocks per TMEM chunk
 
   extern __shared__ uint8_t smem_raw[];
   uint8_t *smem = reinterpret_cast<uint8_t *>(
@@ -277,14 +352,15 @@ __global__ void __launch_bounds__(kThreads, 1)
   const GemmProblem &p = args.p;
   const int SA = args.sa, SO = args.so;
   uint8_t *aring = smem;
-  uint8_t *opring = aring + SA * A32_BYTES;  // slot: [A planes][B planes]
-  uint64_t *afull32 = reinterpret_cast<uint64_t *>(opring + SO * OP_BYTES);  // [SA]
-  uint64_t *aempty32 = afull32 + SA;                                         // [SA]
-  uint64_t *opfull = aempty32 + SA;  // [SO] B planes landed and A planes written
-  uint64_t *opempty = opfull + SO;   // [SO] the MMAs reading the slot are done
-  uint64_t *tfull = opempty + SO;    // [2] TMEM accumulator holds a finished chunk
-  uint64_t *tempty = tfull + 2;      // [2] TMEM accumulator drained
-  uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(tempty + 2);
+  uint8_t *bring = aring + SA * A32_BYTES;
+  uint64_t *afull = reinterpret_cast<uint64_t *>(bring + SO * BSLOT);  // [SA] tile landed
+  uint64_t *aempty = afull + SA;     // [SA] the converter group has read the tile
+  uint64_t *opfull = aempty + SA;    // [SO] B tiles landed and the A stage written
+  uint64_t *opempty = opfull + SO;   // [SO] the MMAs reading the stage are done
+  uint64_t *accfull = opempty + SO;   // [NI] accumulator holds a finished chunk
+  uint64_t *accempty = accfull + NI;  // [NI] accumulator drained
+  uint64_t *mmadone = accempty + NI;  // every issued MMA has completed
+  uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(mmadone + 1);
   int *bad_flag = reinterpret_cast<int *>(tmem_slot + 1);
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -296,53 +372,53 @@ __global__ void __launch_bounds__(kThreads, 1)
   const int kend = min(p.K, kbeg + args.kc);
   const int nkb = kend > kbeg ? (kend - kbeg + kBK - 1) / kBK : 0;
   const int nchunks = (nkb + P - 1) / P;
+  const uint32_t tmem_cols = tc_tmem_alloc_cols(BN, NS, SO);
 
   if (tid == 0) {
     for (int s = 0; s < SA; ++s) {
-      mbar_init(&afull32[s], 1);
-      mbar_init(&aempty32[s], kConvWarps);
+      mbar_init(&afull[s], 1);
+      mbar_init(&aempty[s], 4);
     }
     for (int o = 0; o < SO; ++o) {
-      mbar_init(&opfull[o], kConvWarps + 1);  // converter warps + the B loader
+      mbar_init(&opfull[o], 4 + 1);  // the converter group's warps + the B loader
       mbar_init(&opempty[o], 1);
     }
-    for (int b = 0; b < 2; ++b) {
-      mbar_init(&tfull[b], 1);
-      mbar_init(&tempty[b], kConvWarps);
+    for (int b = 0; b < NI; ++b) {
+      mbar_init(&accfull[b], 1);
+      mbar_init(&accempty[b], 4 * D);
     }
+    mbar_init(mmadone, NI);  // one commit per MMA issuer
     *bad_flag = 0;
     fence_mbar_init();
   }
-  if (warp == kMmaWarp) tmem_alloc(tmem_slot, TMEM_COLS);
+  if (warp == 2) tmem_alloc(tmem_slot, tmem_cols);
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem = *tmem_slot;
+  const uint32_t tacc = tmem;           // accumulator b: columns b*BN .. +BN-1
+  const uint32_t tA = tmem + NI * BN;   // A stage o: columns NI*BN + o*SC .. +SC-1
 
-  float sums[QTR];  // converter warps: FP32 running sums, a quarter row of C
-#pragma unroll
-  for (int i = 0; i < QTR; ++i) sums[i] = 0.0f;
-
-  if (warp == kLoadAWarp) {
+  if (warp == 0) {
     // -------------------------------------------------------- TMA, A
     if (lane == 0) {
       prefetch_tmap(&tmA);
       for (int kb = 0; kb < nkb; ++kb) {
         const int s = kb % SA;
-        if (!mbar_wait(&aempty32[s], ((kb / SA) & 1) ^ 1, args.err, kDevErrEmptyBarrier)) {
+        if (!mbar_wait(&aempty[s], ((kb / SA) & 1) ^ 1, args.err, kDevErrEmptyBarrier)) {
           *bad_flag = 1;
           break;
         }
         uint8_t *dst = aring + s * A32_BYTES;
         const int k0 = kbeg + kb * kBK;
-        mbar_arrive_expect_tx(&afull32[s], A32_BYTES);
+        mbar_arrive_expect_tx(&afull[s], A32_BYTES);
         if (AK)  // 128 rows of 32 floats (128-byte swizzle)
-          tma_load_2d(dst, &tmA, &afull32[s], k0, static_cast<int>(m0));
+          tma_load_2d(dst, &tmA, &afull[s], k0, static_cast<int>(m0));
         else     // 32 rows (k) of 128 floats (m)
-          tma_load_2d(dst, &tmA, &afull32[s], static_cast<int>(m0), k0);
+          tma_load_2d(dst, &tmA, &afull[s], static_cast<int>(m0), k0);
       }
     }
-  } else if (warp == kLoadBWarp) {
+  } else if (warp == 1) {
     // -------------------------------------------------------- TMA, B
     if (lane == 0) {
       prefetch_tmap(&tmB);
@@ -352,165 +428,170 @@ __global__ void __launch_bounds__(kThreads, 1)
           *bad_flag = 1;
           break;
         }
-        uint8_t *dst = opring + o * OP_BYTES + NS * APL_BYTES;
+        uint8_t *dst = bring + o * BSLOT;
         const int k0 = kbeg + kb * kBK;
-        mbar_arrive_expect_tx(&opfull[o], NS * BPL_BYTES);
+        mbar_arrive_expect_tx(&opfull[o], BSLOT);
 #pragma unroll
         for (int i = 0; i < NS; ++i)
           tma_load_2d(dst + i * BPL_BYTES, &tmB, &opfull[o], k0, i * args.n_pad + n0);
       }
     }
-  } else if (warp == kMmaWarp) {
+  } else if (warp >= 2 && warp < 2 + NI) {
     // ---------------------------------------------------------- MMA
+    // NI issuing threads, one per accumulator: issuer b takes the chunks
+    // q = b, b+NI, ...  A commit tracks only the MMAs of the thread that
+    // issues it.
     if (lane == 0) {
-      for (int kb = 0; kb < nkb; ++kb) {
-        const int o = kb % SO;
-        const int q = kb / P, b = q & 1;
-        const bool first = (kb % P) == 0;
-        const bool last = (kb % P) == P - 1 || kb == nkb - 1;
-        if ((first &&
-             !mbar_wait(&tempty[b], ((q >> 1) & 1) ^ 1, args.err, kDevErrEmptyBarrier)) ||
-            !mbar_wait(&opfull[o], (kb / SO) & 1, args.err, kDevErrFullBarrier)) {
-          *bad_flag = 1;
+      const int b = warp - 2;
+      const uint32_t dacc = tacc + static_cast<uint32_t>(b * BN);
+      bool ok = true;
+      for (int q = b; q < nchunks && ok; q += NI) {
+        if (!mbar_wait(&accempty[b], ((q / NI) & 1) ^ 1, args.err, kDevErrEmptyBarrier)) {
+          ok = false;
           break;
         }
-        tc_fence_after();
-        const uint32_t dacc = tmem + static_cast<uint32_t>(b * BN);
-        const uint64_t a_desc = sw64_desc(smem_u32(opring + o * OP_BYTES));
-        const uint64_t b_desc = sw64_desc(smem_u32(opring + o * OP_BYTES + NS * APL_BYTES));
+        const int kb1 = min(nkb, (q + 1) * P);
+        for (int kb = q * P; kb < kb1; ++kb) {
+          const int o = kb % SO;
+          const bool first = kb == q * P;
+          if (!mbar_wait(&opfull[o], (kb / SO) & 1, args.err, kDevErrFullBarrier)) {
+            ok = false;
+            break;
+          }
+          tc_fence_after();
+          const uint32_t astage = tA + static_cast<uint32_t>(o * SC);
+          const uint64_t b_desc = sw64_desc(smem_u32(bring + o * BSLOT));
 #pragma unroll
-        for (int kk = 0; kk < kBK / 16; ++kk) {
+          for (int kk = 0; kk < kBK / 16; ++kk) {
 #pragma unroll
-          for (int i = 0; i < NS; ++i)
+            for (int i = 0; i < NS; ++i)
 #pragma unroll
-            for (int j = 0; j < NS - i; ++j) {
-              // descriptor start addresses count 16-byte units
-              const uint64_t ad = a_desc + static_cast<uint64_t>((i * APL_BYTES + kk * 32) >> 4);
-              const uint64_t bd = b_desc + static_cast<uint64_t>((j * BPL_BYTES + kk * 32) >> 4);
-              const uint32_t acc = (!first || kk > 0 || i > 0 || j > 0) ? 1u : 0u;
-              mma_bf16(dacc, ad, bd, IDESC, acc);
-            }
+              for (int j = 0; j < NS - i; ++j) {
+                // A plane i: 16 columns per plane, 8 per 16-deep step;
+                // descriptor start addresses count 16-byte units
+                const uint32_t at = astage + static_cast<uint32_t>(i * 16 + kk * 8);
+                const uint64_t bd =
+                    b_desc + static_cast<uint64_t>((j * BPL_BYTES + kk * 32) >> 4);
+                const uint32_t acc = (!first || kk > 0 || i > 0 || j > 0) ? 1u : 0u;
+                mma_bf16_ts(dacc, at, bd, IDESC, acc);
+              }
+          }
+          mma_commit(&opempty[o]);
         }
-        mma_commit(&opempty[o]);
-        if (last) mma_commit(&tfull[b]);
+        if (ok) mma_commit(&accfull[b]);
       }
+      if (!ok) *bad_flag = 1;
+      mma_commit(mmadone);  // tracks every MMA this thread issued
     }
-  } else {
-    // ------------------------------------ converters / drain (warps 0-15)
+  } else if (warp >= kConvWarp0 && warp < kDrainWarp0) {
+    // ------------------------------------------ converters (G groups)
+    const int g = (warp - kConvWarp0) >> 2;
     const int m = tid & (kBM - 1);  // row of the tile == TMEM lane
-    const int g = tid >> 7;         // 8-wide k chunk of each block, column quarter
-    const int quarter = warp & 3;   // TMEM lanes 32*quarter .. +31 == rows of this warp
-    bool ok = true;
-    auto drain = [&](int q) -> bool {
-      const int b = q & 1;
-      bool w = mbar_wait(&tfull[b], (q >> 1) & 1, args.err, kDevErrMmaBarrier);
-      w = __all_sync(0xffffffffu, w);  // tcgen05.ld is warp-collective
-      if (!w) return false;
-      tc_fence_after();
-      const uint32_t taddr =
-          tmem + (static_cast<uint32_t>(quarter * 32) << 16) + b * BN + g * QTR;
-      if (QTR >= 16) {
-#pragma unroll
-        for (int nc = 0; nc < QTR; nc += 16) {
-          float v[16];
-          tmem_ld16(taddr + nc, v);
-#pragma unroll
-          for (int i = 0; i < 16; ++i) sums[nc + i] += v[i];
-        }
-      } else if (QTR == 8) {
-        float v[8];
-        tmem_ld8(taddr, v);
-#pragma unroll
-        for (int i = 0; i < 8; ++i) sums[i] += v[i];
-      } else {
-        float v[4];
-        tmem_ld4(taddr, v);
-#pragma unroll
-        for (int i = 0; i < 4; ++i) sums[i] += v[i];
-      }
-      tc_fence_before();
-      __syncwarp();
-      if (lane == 0) mbar_arrive(&tempty[b]);
-      return true;
-    };
-    int drained = 0;
-    for (int kb = 0; kb < nkb && ok; ++kb) {
+    const uint32_t lanes = static_cast<uint32_t>((warp & 3) * 32) << 16;
+    for (int kb = g; kb < nkb; kb += G) {
       const int s = kb % SA, o = kb % SO;
-      // 1. the FP32 tile: read this thread's eight values and release the
-      //    slot at once, so the HBM stream never waits for the MMA pipeline
-      bool w = mbar_wait(&afull32[s], (kb / SA) & 1, args.err, kDevErrFullBarrier);
+      bool w = mbar_wait(&afull[s], (kb / SA) & 1, args.err, kDevErrFullBarrier);
       if (!__all_sync(0xffffffffu, w)) {
-        ok = false;
+        *bad_flag = 1;
         break;
       }
       const float *a32 = reinterpret_cast<const float *>(aring + s * A32_BYTES);
-      float x[8];
+      float x[32];
       if (AK) {
         // row m holds 32 floats in 128 bytes, 128-byte swizzle
 #pragma unroll
-        for (int hh = 0; hh < 2; ++hh) {
-          const int qq = (2 * g + hh) ^ (m & 7);
-          const float4 v = *reinterpret_cast<const float4 *>(a32 + m * 32 + qq * 4);
-          x[4 * hh + 0] = v.x; x[4 * hh + 1] = v.y; x[4 * hh + 2] = v.z; x[4 * hh + 3] = v.w;
+        for (int c = 0; c < 8; ++c) {
+          const float4 v = *reinterpret_cast<const float4 *>(a32 + m * 32 + ((c ^ (m & 7)) * 4));
+          x[4 * c + 0] = v.x; x[4 * c + 1] = v.y; x[4 * c + 2] = v.z; x[4 * c + 3] = v.w;
         }
       } else {
 #pragma unroll
-        for (int j = 0; j < 8; ++j) x[j] = a32[(g * 8 + j) * kBM + m];
+        for (int k = 0; k < 32; ++k) x[k] = a32[k * kBM + m];
       }
-      // consume the values before the warp releases the slot: one lane
-      // arrives for the warp, and __syncwarp alone does not wait for the
-      // other lanes' shared-memory loads to return
-      uint4 v[NS];
-      pack8<NS>(x, v);
+      // consume the values (the first plane's split reads every one) before
+      // the warp releases the slot: one lane arrives for the warp, and
+      // __syncwarp alone does not wait for the other lanes' shared-memory
+      // loads to return
+      uint32_t wv[16];
+      split_plane32<NS == 1>(x, wv);
       __syncwarp();
-      if (lane == 0) mbar_arrive(&aempty32[s]);
-      // 2. the operand slot: wait until the MMAs that read it are done
+      if (lane == 0) mbar_arrive(&aempty[s]);
+      // the A stage: wait until the MMAs that read it are done
       w = mbar_wait(&opempty[o], ((kb / SO) & 1) ^ 1, args.err, kDevErrEmptyBarrier);
       if (!__all_sync(0xffffffffu, w)) {
-        ok = false;
+        *bad_flag = 1;
         break;
       }
-      uint8_t *dst = opring + o * OP_BYTES;
-      const uint32_t off = sw64_off(m, g);
-#pragma unroll
-      for (int i = 0; i < NS; ++i) *reinterpret_cast<uint4 *>(dst + i * APL_BYTES + off) = v[i];
-      fence_proxy_async_smem();  // generic-proxy writes -> tensor-core reads
+      tc_fence_after();
+      const uint32_t dst = tA + lanes + static_cast<uint32_t>(o * SC);
+      tmem_st16(dst, wv);
+      split_plane32<NS == 2>(x, wv);
+      tmem_st16(dst + 16u, wv);
+      if constexpr (NS == 3) {
+        split_plane32<true>(x, wv);
+        tmem_st16(dst + 32u, wv);
+      }
+      tmem_wait_st();
+      tc_fence_before();
       __syncwarp();
       if (lane == 0) mbar_arrive(&opfull[o]);
-      // after the last block of chunk q, drain chunk q-1 (one chunk of slack
-      // so the tensor core never waits for the drain)
-      const bool chunk_end = (kb % P) == P - 1 || kb == nkb - 1;
-      if (chunk_end && kb / P >= 1) {
-        if (!drain(drained)) { ok = false; break; }
-        ++drained;
+    }
+  } else if (warp >= kDrainWarp0) {
+    // ------------------------------------------ drain (D groups)
+    const int d = (warp - kDrainWarp0) >> 2;
+    const uint32_t lanes = static_cast<uint32_t>((warp & 3) * 32) << 16;
+    float sums[DC];  // FP32 running sums of row m, DC columns
+#pragma unroll
+    for (int i = 0; i < DC; ++i) sums[i] = 0.0f;
+    for (int q = 0; q < nchunks; ++q) {
+      const int b = q % NI;
+      bool w = mbar_wait(&accfull[b], (q / NI) & 1, args.err, kDevErrMmaBarrier);
+      if (!__all_sync(0xffffffffu, w)) {  // tcgen05.ld is warp-collective
+        *bad_flag = 1;
+        break;
       }
+      tc_fence_after();
+      const uint32_t src = tacc + lanes + static_cast<uint32_t>(b * BN + d * DC);
+      if constexpr (DC >= 16) {
+#pragma unroll
+        for (int c = 0; c < DC; c += 16) {
+          uint32_t r0[16];
+          tmem_ld16(src + c, r0);
+          tmem_wait_ld();
+#pragma unroll
+          for (int i = 0; i < 16; ++i) sums[c + i] += __uint_as_float(r0[i]);
+        }
+      } else {
+        static_assert(DC % 8 == 0, "drain width");
+        uint32_t r0[8];
+        tmem_ld8(src, r0);
+        tmem_wait_ld();
+#pragma unroll
+        for (int i = 0; i < 8; ++i) sums[i] += __uint_as_float(r0[i]);
+      }
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&accempty[b]);
     }
-    while (ok && drained < nchunks) {
-      if (!drain(drained)) { ok = false; break; }
-      ++drained;
-    }
-    if (!ok) *bad_flag = 1;
-  }
-
-  // ---------------------------------------------------------- epilogue
-  __syncthreads();
-  const bool failed = *bad_flag != 0;
-  float *red = reinterpret_cast<float *>(smem);  // [BN][kBM], reuses the rings
-  if (warp < kConvWarps) {
+    // ---------------------------------------------------- epilogue
+    // (the running sums stay in this branch's registers; the barrier is the
+    // one every other thread reaches below)
+    __syncthreads();
+    const bool failed = *bad_flag != 0;
+    float *red = reinterpret_cast<float *>(smem);  // [BN][kBM], reuses the A ring
     const int m = tid & (kBM - 1);
-    const int g = tid >> 7;
     const int64_t gm = m0 + m;
     if (failed) {
 #pragma unroll
-      for (int i = 0; i < QTR; ++i) sums[i] = 0.0f;
+      for (int i = 0; i < DC; ++i) sums[i] = 0.0f;
     }
     if (split > 1) {
 #pragma unroll
-      for (int i = 0; i < QTR; ++i) red[(g * QTR + i) * kBM + m] = sums[i];
+      for (int i = 0; i < DC; ++i) red[(d * DC + i) * kBM + m] = sums[i];
     } else if (gm < p.M) {
 #pragma unroll
-      for (int i = 0; i < QTR; ++i) {
-        const int gn = n0 + g * QTR + i;
+      for (int i = 0; i < DC; ++i) {
+        const int gn = n0 + d * DC + i;
         if (gn < p.N) {
           float *cp = p.C + gm * p.scm + static_cast<int64_t>(gn) * p.scn;
           *cp = axpby(p.alpha, sums[i], p.beta, cp);
@@ -518,8 +599,10 @@ __global__ void __launch_bounds__(kThreads, 1)
       }
     }
   }
+  if (warp < kDrainWarp0) __syncthreads();
   if (split > 1) {
     cluster_sync();
+    const float *red = reinterpret_cast<const float *>(smem);
     constexpr int E = kBM * BN;
     const int per = E / split;
     const uint32_t base = smem_u32(red);
@@ -546,7 +629,15 @@ __global__ void __launch_bounds__(kThreads, 1)
   }
   tc_fence_before();
   __syncthreads();
-  if (warp == kMmaWarp) tmem_dealloc(tmem, TMEM_COLS);
+  if (warp == 2) {
+    // the TMEM is freed only once every issued MMA has completed
+    bool w = true;
+    if (lane == 0) w = mbar_wait(mmadone, 0, args.err, kDevErrMmaBarrier);
+    __syncwarp();
+    (void)w;
+    tc_fence_after();
+    tmem_dealloc(tmem, tmem_cols);
+  }
 }
 
 }  // namespace
@@ -558,27 +649,11 @@ bool tc_config_fits(int bn, int ns, int stages) {
 
 namespace {
 
+// Launch of the kernel with the B planes already split into `planes`.
 template <int BN, int NS, bool AK>
-hml_status run_tc(const GemmProblem &p, const hml_sgemm_config &c, cudaStream_t s) {
-  const int k_pad = ((p.K + kChunkK - 1) / kChunkK) * kChunkK;
-  const int n_pad = ((p.N + BN - 1) / BN) * BN;
-  // B planes in the stream's workspace
-  const size_t plane_bytes = static_cast<size_t>(n_pad) * k_pad * 2;
-  void *ws = nullptr;
-  hml_status st = workspace(NS * plane_bytes, s, &ws);
-  if (st != HML_STATUS_SUCCESS) return st;
-  auto *planes = static_cast<__nv_bfloat16 *>(ws);
-  {
-    const int64_t chunks = static_cast<int64_t>(n_pad) * (k_pad / 8);
-    const int blocks = static_cast<int>(std::min<int64_t>((chunks + 255) / 256, 4 * sm_count()));
-    count_launch();
-    split_b_kernel<NS><<<blocks, 256, 0, s>>>(p.B, p.sbk, p.sbn, p.K, p.N, planes, k_pad, n_pad);
-    cudaError_t e = cudaGetLastError();
-    if (e != cudaSuccess) {
-      note_cuda_error(e, "split_b");
-      return HML_STATUS_CUDA_ERROR;
-    }
-  }
+hml_status launch_tc_planes(const GemmProblem &p, const hml_sgemm_config &c,
+                            const __nv_bfloat16 *planes, int k_pad, int n_pad, int *err,
+                            cudaStream_t s) {
   CUtensorMap ta, tb;
   memset(&ta, 0, sizeof ta);
   memset(&tb, 0, sizeof tb);
@@ -604,7 +679,7 @@ hml_status run_tc(const GemmProblem &p, const hml_sgemm_config &c, cudaStream_t 
   args.sa = plan.sa;
   args.so = plan.so;
   args.n_pad = n_pad;
-  args.err = device_error_word();
+  args.err = err;
   const size_t smem = tc_plan_bytes(BN, NS, plan);
   auto kern = tc_kernel<BN, NS, AK>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -619,9 +694,40 @@ hml_status run_tc(const GemmProblem &p, const hml_sgemm_config &c, cudaStream_t 
   const int64_t tiles_n = n_pad / BN;
   if (tiles_m * c.split_k > 0x7fffffff || tiles_n > 65535) return HML_STATUS_NOT_SUPPORTED;
   dim3 grid(static_cast<unsigned>(tiles_m * c.split_k), static_cast<unsigned>(tiles_n));
-  e = launch_k(kern, grid, dim3(kThreads), smem, s, c.split_k, ta, tb, args);
+  e = launch_k(kern, grid, dim3(tc_warps(BN, NS) * 32), smem, s, c.split_k, ta, tb, args);
   note_cuda_error(e, "tc launch");
   return cuda_status(e);
+}
+
+// B -> BF16 planes in `planes` ([NS][n_pad][k_pad]).
+template <int NS>
+hml_status split_b(const GemmProblem &p, __nv_bfloat16 *planes, int k_pad, int n_pad,
+                   cudaStream_t s) {
+  const int64_t chunks = static_cast<int64_t>(n_pad) * (k_pad / 8);
+  const int blocks = static_cast<int>(std::min<int64_t>((chunks + 255) / 256, 4 * sm_count()));
+  count_launch();
+  split_b_kernel<NS><<<blocks, 256, 0, s>>>(p.B, p.sbk, p.sbn, p.K, p.N, planes, k_pad, n_pad);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) {
+    note_cuda_error(e, "split_b");
+    return HML_STATUS_CUDA_ERROR;
+  }
+  return HML_STATUS_SUCCESS;
+}
+
+template <int BN, int NS, bool AK>
+hml_status run_tc(const GemmProblem &p, const hml_sgemm_config &c, cudaStream_t s) {
+  const int k_pad = ((p.K + kChunkK - 1) / kChunkK) * kChunkK;
+  const int n_pad = ((p.N + BN - 1) / BN) * BN;
+  // B planes in the stream's workspace
+  const size_t plane_bytes = static_cast<size_t>(n_pad) * k_pad * 2;
+  void *ws = nullptr;
+  hml_status st = workspace(NS * plane_bytes, s, &ws);
+  if (st != HML_STATUS_SUCCESS) return st;
+  auto *planes = static_cast<__nv_bfloat16 *>(ws);
+  st = split_b<NS>(p, planes, k_pad, n_pad, s);
+  if (st != HML_STATUS_SUCCESS) return st;
+  return launch_tc_planes<BN, NS, AK>(p, c, planes, k_pad, n_pad, device_error_word(), s);
 }
 
 template <int BN, int NS>
@@ -659,7 +765,7 @@ hml_status check_tc(const GemmProblem &p, const hml_sgemm_config &c) {
   if (c.stages < 2 || c.stages > 8) return HML_STATUS_INVALID_VALUE;
   const int ns = c.algo == HML_ALGO_BF16X3 ? 2 : 3;
   if (!tc_config_fits(c.tile_n, ns, c.stages)) return HML_STATUS_INVALID_VALUE;
-  // the rings are reused for the split-K partial tile
+  // the A ring is reused for the split-K partial tile
   if (c.split_k > 1 &&
       static_cast<size_t>(kBM) * c.tile_n * 4 > static_cast<size_t>(c.stages) * tc_a_bytes())
     return HML_STATUS_INVALID_VALUE;
@@ -738,60 +844,9 @@ hml_status run_tc_static(const GemmProblem &p, const hml_sgemm_config &c, void *
   const int k_pad = ((p.K + kChunkK - 1) / kChunkK) * kChunkK;
   const int n_pad = ((p.N + BN - 1) / BN) * BN;
   auto *planes = static_cast<__nv_bfloat16 *>(scratch);
-  {
-    const int64_t chunks = static_cast<int64_t>(n_pad) * (k_pad / 8);
-    const int blocks = static_cast<int>(std::min<int64_t>((chunks + 255) / 256, 4 * sm_count()));
-    count_launch();
-    split_b_kernel<NS><<<blocks, 256, 0, s>>>(p.B, p.sbk, p.sbn, p.K, p.N, planes, k_pad, n_pad);
-    cudaError_t e = cudaGetLastError();
-    if (e != cudaSuccess) {
-      note_cuda_error(e, "noalloc split_b");
-      return HML_STATUS_CUDA_ERROR;
-    }
-  }
-  CUtensorMap ta, tb;
-  memset(&ta, 0, sizeof ta);
-  memset(&tb, 0, sizeof tb);
-  bool ok;
-  if (AK)
-    ok = tensor_map_2d(&ta, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, p.A, p.K, p.M, p.sam * 4, kBK, kBM,
-                       CU_TENSOR_MAP_SWIZZLE_128B);
-  else
-    ok = tensor_map_2d(&ta, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, p.A, p.M, p.K, p.sak * 4, kBM, kBK,
-                       CU_TENSOR_MAP_SWIZZLE_NONE);
-  if (ok)
-    ok = tensor_map_2d(&tb, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, planes, k_pad,
-                       static_cast<uint64_t>(NS) * n_pad, static_cast<uint64_t>(k_pad) * 2, kBK, BN,
-                       CU_TENSOR_MAP_SWIZZLE_64B);
-  if (!ok) return HML_STATUS_CUDA_ERROR;
-  TcArgs args;
-  args.p = p;
-  args.split = c.split_k;
-  const int kchunks = k_pad / kChunkK;
-  args.kc = ((kchunks + c.split_k - 1) / c.split_k) * kChunkK;
-  TcPlan plan;
-  if (!tc_plan(BN, NS, c.stages, &plan)) return HML_STATUS_INVALID_VALUE;
-  args.sa = plan.sa;
-  args.so = plan.so;
-  args.n_pad = n_pad;
-  args.err = nullptr;
-  const size_t smem = tc_plan_bytes(BN, NS, plan);
-  auto kern = tc_kernel<BN, NS, AK>;
-  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       static_cast<int>(smem));
-  if (e == cudaSuccess && c.split_k > 8)
-    e = cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
-  if (e != cudaSuccess) {
-    note_cuda_error(e, "noalloc tc attributes");
-    return HML_STATUS_CUDA_ERROR;
-  }
-  const int64_t tiles_m = (static_cast<int64_t>(p.M) + kBM - 1) / kBM;
-  const int64_t tiles_n = n_pad / BN;
-  if (tiles_m * c.split_k > 0x7fffffff || tiles_n > 65535) return HML_STATUS_NOT_SUPPORTED;
-  dim3 grid(static_cast<unsigned>(tiles_m * c.split_k), static_cast<unsigned>(tiles_n));
-  e = launch_k(kern, grid, dim3(kThreads), smem, s, c.split_k, ta, tb, args);
-  note_cuda_error(e, "noalloc tc launch");
-  return cuda_status(e);
+  hml_status st = split_b<NS>(p, planes, k_pad, n_pad, s);
+  if (st != HML_STATUS_SUCCESS) return st;
+  return launch_tc_planes<BN, NS, AK>(p, c, planes, k_pad, n_pad, nullptr, s);
 }
 
 template <int NS>

@@ -36,7 +36,7 @@ def check_tol(algo, got, D, absD, K, what=""):
     return e
 
 
-def run_tc(M, N, K, algo, bn, split=1, stages=3, order=0, ta=0, tb=0, alpha=1.0, beta=0.0,
+def run_tc(M, N, K, algo, bn, split=1, stages=4, order=0, ta=0, tb=0, alpha=1.0, beta=0.0,
            dist=dg.UNIFORM, seed=5, offset=0):
     import torch
     A = dg.matrix(K if ta else M, M if ta else K, seed, 0, dist, order="C")
@@ -71,7 +71,7 @@ def test_tc_cluster_split_k(cuda, algo, split):
         check_tol(algo, got, D, absD, K, what=f"split {split} K {K}")
 
 
-@pytest.mark.parametrize("stages", [2, 3, 4, 6])
+@pytest.mark.parametrize("stages", [2, 4, 6, 8])
 def test_tc_ring_depths(cuda, stages):
     for algo, bn in ((X3, 128), (X6, 64)):
         cfg = SgemmConfig(algo, 128, bn, 1, stages, VAR[bn])
@@ -82,7 +82,7 @@ def test_tc_ring_depths(cuda, stages):
 
 
 def test_tc_rejects_unaligned_a(cuda):
-    cfg = SgemmConfig(X6, 128, 16, 1, 3, 0)
+    cfg = SgemmConfig(X6, 128, 16, 1, 4, 0)
     # lda = 301 floats is not a multiple of 16 bytes: TMA cannot address A
     assert hml.config_check(0, 0, 0, 300, 16, 64, 301, 64, 300, cfg) == 2
 
@@ -96,7 +96,7 @@ def test_tc_beta_zero_does_not_read_c(cuda):
     hml.fill_random(B, 9, 1)
     C = torch.full((M * N,), float("nan"), device="cuda")
     hml.sgemm_ex(0, 0, 0, M, N, K, 1.0, A, M, B, K, 0.0, C, M,
-                 config=SgemmConfig(X6, 128, 64, 1, 3, 2))
+                 config=SgemmConfig(X6, 128, 64, 1, 4, 2))
     assert torch.isfinite(C).all()
 
 

@@ -51,7 +51,7 @@ def _both(algo, bn, M, N, K, seed, alpha=1.5, beta=-0.5):
     point and through hml_sgemm_ex_config; returns both results."""
     import torch
     A, B, C0 = _problem(M, N, K, seed)
-    cfg = SgemmConfig(algo, 128, bn, 1, 3, VAR[bn])
+    cfg = SgemmConfig(algo, 128, bn, 1, 4, VAR[bn])
     stream = torch.cuda.current_stream().cuda_stream
     c_ref = C0.clone()
     st = lib.hml_sgemm_ex_config(0, 0, 0, M, N, K, alpha, A.data_ptr(), M, B.data_ptr(), K, beta,
@@ -79,7 +79,7 @@ def test_noalloc_rejects_problems_beyond_the_scratch(cuda):
     import torch
     M, N, K = 256, 128, 8192  # BF16X6: 3 x 128 x 8192 x 2 B = 6 MiB > 4 MiB
     A, B, C0 = _problem(M, N, K, 13)
-    cfg = SgemmConfig(hml.ALGO_BF16X6, 128, 128, 1, 3, VAR[128])
+    cfg = SgemmConfig(hml.ALGO_BF16X6, 128, 128, 1, 4, VAR[128])
     st = _noalloc(0, 0, 0, M, N, K, 1.0, A.data_ptr(), M, B.data_ptr(), K, 0.0, C0.data_ptr(), M,
                   ctypes.byref(cfg), torch.cuda.current_stream().cuda_stream)
     assert st == 1  # HML_STATUS_INVALID_VALUE
