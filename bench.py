@@ -521,6 +521,11 @@ def run_ours(args):
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": dict(config_desc(args.workload),
                            parallelism=f"independent per-GPU problems x{world}",
+                           selection=("the library's automatic choice: the B200 tuned table "
+                                      "shipped as data/tuned_b200.txt (autotuner-measured), "
+                                      "else the learned predictor" if algo is None else
+                                      f"forced family {args.algo}: the library's heuristic "
+                                      "configuration of that family"),
                            **({"rows_override": args.rows} if args.rows else {}),
                            **({"only_n": args.only_n} if args.only_n else {})),
             "roofline": roof, "cpu_baseline": cpu, "e2e": e2e,

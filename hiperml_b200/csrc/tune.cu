@@ -16,6 +16,8 @@
 //   # device <name> sms <n>
 //   akc bkc M N K : algo tile_m tile_n split_k stages variant time_us
 // (akc/bkc: whether A / B are K-contiguous in the canonical long-M form).
+#include <dlfcn.h>
+
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
@@ -50,6 +52,7 @@ struct Rec {
 std::mutex g_mu;
 std::map<Key, Rec> g_table;
 int g_math_mode = HML_MATH_FP32;
+bool g_default_tried = false;  // the shipped table was loaded or ruled out
 
 Key key_of(const GemmProblem &p) {
   return Key{p.a_kcontig() ? 1 : 0, p.b_kcontig() ? 1 : 0, p.M, p.N, p.K};
@@ -61,7 +64,42 @@ bool allowed(int algo) { return algo != HML_ALGO_BF16X3 || g_math_mode == HML_MA
 
 int math_mode() { return g_math_mode; }
 
+hml_status tune_load(const char *path, int *records);
+
+namespace {
+// The table shipped beside the library (data/tuned_b200.txt next to
+// libhml_b200.so): the autotuner's measured best configurations on the B200
+// for the library's reference workloads, in the role of the reference's
+// per-GPU .cfg files.  It is loaded on the first selection when no table was
+// loaded, measured or cleared before; HML_TUNED=<path> names another file,
+// HML_TUNED=none disables it.
+void load_default_table() {
+  {
+    std::lock_guard<std::mutex> lk(g_mu);
+    if (g_default_tried) return;
+    g_default_tried = true;
+    if (!g_table.empty()) return;
+  }
+  std::string path;
+  const char *env = getenv("HML_TUNED");
+  if (env && *env) {
+    if (strcmp(env, "none") == 0) return;
+    path = env;
+  } else {
+    Dl_info info;
+    if (!dladdr(reinterpret_cast<void *>(&load_default_table), &info) || !info.dli_fname) return;
+    path = info.dli_fname;
+    const size_t slash = path.rfind('/');
+    path = (slash == std::string::npos ? std::string(".") : path.substr(0, slash)) +
+           "/data/tuned_b200.txt";
+  }
+  int n = 0;
+  tune_load(path.c_str(), &n);  // a missing file leaves the table empty
+}
+}  // namespace
+
 bool tuned_lookup(const GemmProblem &p, hml_sgemm_config *c) {
+  load_default_table();
   std::lock_guard<std::mutex> lk(g_mu);
   if (g_table.empty()) return false;
   const Key k = key_of(p);
@@ -132,6 +170,7 @@ hml_status tune_load(const char *path, int *records) {
   fclose(f);
   if (!header) return HML_STATUS_CONFIG_ERROR;
   std::lock_guard<std::mutex> lk(g_mu);
+  g_default_tried = true;  // an explicit table replaces the shipped one
   for (auto &kv : t) g_table[kv.first] = kv.second;
   if (records) *records = n;
   return HML_STATUS_SUCCESS;
@@ -297,6 +336,7 @@ hml_status autotune(hml_order order, hml_op ta, hml_op tb, int M, int N, int K,
 hml_status tune_clear() {
   std::lock_guard<std::mutex> lk(g_mu);
   g_table.clear();
+  g_default_tried = true;  // cleared means empty: the shipped table stays out
   return HML_STATUS_SUCCESS;
 }
 

@@ -13,6 +13,13 @@ is an ``.npz`` file with
     device   str
 
 Usage (on the GPU):  python -m hiperml_b200.tuning_data OUT.npz --count 5000
+
+It also writes the B200 tuned table shipped beside the library
+(``data/tuned_b200.txt``, the counterpart of the reference's per-GPU .cfg
+files): the autotuner's measured best configuration, among the FP32-accurate
+families, for each of the library's reference workload shapes:
+
+    python -m hiperml_b200.tuning_data --table hiperml_b200/data/tuned_b200.txt
 """
 from __future__ import annotations
 
@@ -82,6 +89,26 @@ def measure(shapes: np.ndarray, reps: int = 3, deadline: float | None = None,
     return times
 
 
+# The reference workloads' SGEMM shapes (M, N, K, transA, transB), column-major:
+# the skinny 4096 x 16 x 4096 case, the M=65536, K=4096 precision sweep and the
+# square 8192^3 case.
+TABLE_SHAPES = ((4096, 16, 4096, 0, 0), (65536, 8, 4096, 0, 0), (65536, 32, 4096, 0, 0),
+                (65536, 64, 4096, 0, 0), (65536, 128, 4096, 0, 0), (8192, 8192, 8192, 0, 0))
+
+
+def make_table(path, shapes=TABLE_SHAPES, reps: int = 5) -> None:
+    """Autotunes each shape over the FP32-accurate families (SIMT, BF16X6) and
+    saves the resulting tuned table."""
+    from . import api
+    api.tune_clear()
+    fams = (1 << api.ALGO_SIMT) | (1 << api.ALGO_BF16X6)
+    for (M, N, K, ta, tb) in shapes:
+        ents = api.autotune(api.COL_MAJOR, ta, tb, M, N, K, families=fams, reps=reps)
+        best = min(((t, c) for c, t, st in ents if st == 0 and t > 0), key=lambda e: e[0])
+        print(f"M={M} N={N} K={K} ta={ta} tb={tb}: {best[1]} {best[0]:.1f} us", flush=True)
+    api.tune_save(str(path))
+
+
 def save(path, shapes, times, cfgs, device):
     np.savez_compressed(path, shapes=shapes, times_us=times.astype(np.float32), configs=cfgs,
                         device=np.asarray(device))
@@ -94,7 +121,9 @@ def load(path):
 
 def main(argv=None):
     ap = argparse.ArgumentParser()
-    ap.add_argument("out")
+    ap.add_argument("out", nargs="?")
+    ap.add_argument("--table", default=None,
+                    help="write the tuned table of the reference workload shapes to this file")
     ap.add_argument("--count", type=int, default=5000)
     ap.add_argument("--seed", type=int, default=5)
     ap.add_argument("--reps", type=int, default=3)
@@ -106,6 +135,11 @@ def main(argv=None):
                     help="existing dataset: its shapes are re-measured for --families only "
                          "and its other columns kept")
     args = ap.parse_args(argv)
+    if args.table:
+        make_table(args.table)
+        return 0
+    if not args.out:
+        ap.error("OUT.npz is required")
     import torch
     base = load(args.merge) if args.merge else None
     shapes = base["shapes"] if base is not None else sample_shapes(args.count, args.seed)

@@ -79,8 +79,12 @@ const char *hml_version(void);
 
 /* C = alpha * op(A) * op(B) + beta * C on device pointers.  op(A) is M x K,
  * op(B) is K x N, C is M x N.  The configuration comes from the tuned table
- * (hml_tune_load / hml_autotune_sgemm), else the learned predictor, else the
- * built-in heuristic.  The predictor is the one loaded by hml_predictor_load
+ * (hml_tune_load / hml_autotune_sgemm; without either, the first selection
+ * loads the B200 table shipped as data/tuned_b200.txt beside the library,
+ * HML_TUNED=<file> names another, HML_TUNED=none disables it; an entry also
+ * serves shapes within about 2x of it in every dimension), else the learned
+ * predictor, else the built-in heuristic.  The predictor is the one loaded by
+ * hml_predictor_load
  * or trained by hml_predictor_train; without either, the first selection
  * loads the network shipped as data/predictor_b200.txt beside the library
  * (environment: HML_PREDICTOR=<file> names another, HML_PREDICTOR=none

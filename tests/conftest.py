@@ -6,9 +6,11 @@ import pytest
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 # Selection tests check the built-in heuristic; the shipped predictor network
-# (loaded by the library on first use unless HML_PREDICTOR says otherwise) is
-# exercised by its own tests, which load it explicitly.
+# and tuned table (loaded by the library on first use unless HML_PREDICTOR /
+# HML_TUNED say otherwise) are exercised by their own tests, which load them
+# explicitly or in a child process with the variable unset.
 os.environ.setdefault("HML_PREDICTOR", "none")
+os.environ.setdefault("HML_TUNED", "none")
 if ROOT not in sys.path:
     sys.path.insert(0, ROOT)
 

@@ -82,3 +82,29 @@ def test_math_mode_controls_automatic_choice():
         hml.set_math_mode(hml.MATH_FP32)
     with pytest.raises(hml.HmlError):
         hml.set_math_mode(7)
+
+
+SHIPPED = __import__("os").path.join(__import__("os").path.dirname(hml.__file__), "data",
+                                     "tuned_b200.txt")
+
+
+def test_shipped_table_parses_and_covers_the_reference_workloads():
+    """The B200 tuned table shipped beside the library loads into this build's
+    configuration space and holds an entry for every reference workload."""
+    import os
+
+    from hiperml_b200 import tuning_data as td
+    if not os.path.exists(SHIPPED):
+        pytest.skip("no shipped table")
+    hml.tune_clear()
+    try:
+        assert hml.tune_load(SHIPPED) == len(td.TABLE_SHAPES)
+        keys = set()
+        for line in open(SHIPPED):
+            if line.startswith("#"):
+                continue
+            akc, bkc, M, N, K = (int(x) for x in line.split(":")[0].split())
+            keys.add((M, N, K))
+        assert {(M, N, K) for (M, N, K, _ta, _tb) in td.TABLE_SHAPES} <= keys
+    finally:
+        hml.tune_clear()

@@ -74,3 +74,43 @@ def test_autotune_family_mask_and_bad_arguments(cuda):
     with pytest.raises(hml.HmlError):
         hml.autotune(0, 0, 0, -1, 20, 512)
     hml.tune_clear()
+
+
+def _select_child(env_tuned, shape):
+    """hml.select in a fresh process (HML_TUNED as given, unset for None)."""
+    import os
+    import subprocess
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    M, N, K = shape
+    code = ("import hiperml_b200 as h; "
+            f"c = h.select(0, 0, 0, {M}, {N}, {K}); "
+            "print(' '.join(map(str, c.as_tuple())), h.lib.hml_tune_size())")
+    env = dict(os.environ)
+    env.pop("HML_TUNED", None)
+    if env_tuned is not None:
+        env["HML_TUNED"] = env_tuned
+    out = subprocess.run([sys.executable, "-c", code], env=env, cwd=root, capture_output=True,
+                         text=True, timeout=300, check=True).stdout.split()
+    return tuple(int(x) for x in out[:6]), int(out[6])
+
+
+def test_shipped_table_is_the_default_selection(cuda):
+    """Without HML_TUNED the first selection loads data/tuned_b200.txt, and a
+    reference workload shape gets the table's measured configuration;
+    HML_TUNED=none leaves the table out."""
+    import os
+    path = os.path.join(os.path.dirname(hml.__file__), "data", "tuned_b200.txt")
+    if not os.path.exists(path):
+        pytest.skip("no shipped table")
+    want = {}
+    for line in open(path):
+        if not line.startswith("#"):
+            key, cfg = line.split(":")
+            akc, bkc, M, N, K = (int(x) for x in key.split())
+            want[(M, N, K)] = tuple(int(x) for x in cfg.split()[:6])
+    shape = (65536, 32, 4096)
+    got, size = _select_child(None, shape)
+    assert size == len(want) and got == want[shape]
+    _, size = _select_child("none", shape)
+    assert size == 0
