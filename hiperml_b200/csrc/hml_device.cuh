@@ -59,26 +59,33 @@ __device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
   asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
 }
 
+// One try_wait with a suspend-time hint: the thread is parked until the
+// phase completes or about `kSuspendNs` pass, instead of returning at once
+// and re-polling (a polling warp takes issue slots from the warps doing the
+// work).
+constexpr uint32_t kSuspendNs = 1000000u;  // 1 ms
+
 __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
   uint32_t ok;
   asm volatile(
       "{\n\t.reg .pred p;\n\t"
-      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
       "selp.u32 %0, 1, 0, p;\n\t}"
       : "=r"(ok)
-      : "r"(smem_u32(bar)), "r"(parity)
+      : "r"(smem_u32(bar)), "r"(parity), "r"(kSuspendNs)
       : "memory");
   return ok != 0;
 }
 
 // Waits for the phase with the given parity to complete, for at most
-// kWaitLimitNs.  Returns false (and records `code`) when the limit expires.
+// kWaitLimitNs (plus one suspend slice).  Returns false (and records `code`)
+// when the limit expires.
 __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, int *err, int code) {
   if (mbar_try_wait(bar, parity)) return true;
   const uint64_t t0 = globaltimer_ns();
-  for (uint32_t it = 0;; ++it) {
+  for (;;) {
     if (mbar_try_wait(bar, parity)) return true;
-    if ((it & 63u) == 63u && globaltimer_ns() - t0 > kWaitLimitNs) {
+    if (globaltimer_ns() - t0 > kWaitLimitNs) {
       set_device_error(err, code);
       return false;
     }
