@@ -11,6 +11,6 @@ from .api import (  # noqa: F401
     config_check, configs, device_error, error_fp64, fill_random, hmlSgemm, hmlSgemmBasic,
     hmlSgemmKernelConfig, hmlSgemv, hmlSgemvBasic, hmlSgemvKernelConfig, select, select_algo, sgemm,
     sgemm_ex, sgemv_ex, autotune, tune_save, tune_load, tune_clear, set_math_mode, MATH_FP32,
-    MATH_FAST, BatchPlan, gemm_descs, sgemm_batched)
+    MATH_FAST, BatchPlan, gemm_descs, sgemm_batched, batch_problem_config)
 
 __version__ = lib.hml_version().decode()

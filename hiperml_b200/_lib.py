@@ -112,6 +112,8 @@ _SIGS = {
                                     ctypes.POINTER(ctypes.c_double)]),
     "hml_batch_plan_destroy": (c_int, [c_void_p]),
     "hml_sgemm_batched": (c_int, [c_int, ctypes.POINTER(GemmDesc), c_int, c_void_p]),
+    "hml_batch_problem_config": (c_int, [c_int, ctypes.POINTER(GemmDesc),
+                                         ctypes.POINTER(SgemmConfig)]),
     "hml_predictor_train": (c_int, [c_int, c_void_p, c_void_p, c_int, ctypes.POINTER(SgemmConfig),
                                     c_int, ctypes.POINTER(PredictorOptions), c_void_p]),
     "hml_predictor_loss_grad": (c_int, [c_void_p, c_int, c_void_p, c_void_p, c_void_p, c_int,

@@ -312,6 +312,15 @@ class BatchPlan:
             pass
 
 
+def batch_problem_config(order, problem) -> SgemmConfig:
+    """``hml_batch_problem_config``: the configuration a batch runs this
+    problem (one descriptor tuple, as for ``BatchPlan``) with."""
+    descs = gemm_descs([problem])
+    c = SgemmConfig()
+    check(lib.hml_batch_problem_config(order, descs, ctypes.byref(c)), "hml_batch_problem_config")
+    return c
+
+
 def sgemm_batched(order, problems, stream=None):
     """``hml_sgemm_batched``: one-shot batch, stream ordered."""
     descs = gemm_descs(problems)

@@ -22,8 +22,15 @@
 //     counter, which makes the launch replayable from a CUDA graph
 //     (hml_batch_plan_graph_launch captures it once and replays the graph).
 //
-// Each tile's result equals, bit for bit, the single-problem SIMT kernel's
-// result for the same tile shape with split_k = 1.
+// Problems the tensor cores can take (N > 8, A addressable by TMA, a real
+// product) go to the split-BF16 part of the plan instead (sgemm_tc.cu,
+// tc_batch_*): one B-splitting launch and one persistent launch per tile
+// width class, whose CTAs work through host-balanced item lists.  Both parts
+// are captured in the plan's graph.
+//
+// Each tile's result equals, bit for bit, the single-problem kernel's result
+// for the configuration hml_batch_problem_config reports (the SIMT tile, or
+// BF16X6 with the class's tile width, split_k = 1).
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
@@ -251,6 +258,7 @@ struct BatchPlan {
   double flops = 0.0, bytes = 0.0;
   void *dev = nullptr;  // [queue 256 B][problems][items]
   BatchArgs args = {};
+  TcBatch *tc = nullptr;  // the split-BF16 part
   cudaStream_t capture_stream = nullptr;
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
@@ -260,7 +268,7 @@ namespace {
 
 hml_status build_host(hml_order order, const hml_gemm_desc *descs, int count,
                       std::vector<BatchProblem> *probs, std::vector<BatchItem> *items,
-                      double *flops, double *bytes) {
+                      std::vector<GemmProblem> *tc_probs, double *flops, double *bytes) {
   if (count < 0 || (count > 0 && !descs)) return HML_STATUS_INVALID_VALUE;
   std::vector<double> cost;
   *flops = 0.0;
@@ -278,6 +286,13 @@ hml_status build_host(hml_order order, const hml_gemm_desc *descs, int count,
       return st;
     }
     if (g.M == 0 || g.N == 0) continue;
+    if (tc_probs && tc_batch_eligible(g)) {
+      tc_probs->push_back(g);
+      *flops += 2.0 * g.M * g.N * static_cast<double>(g.K);
+      *bytes += 4.0 * (static_cast<double>(g.M) * g.K + static_cast<double>(g.K) * g.N +
+                       static_cast<double>(g.M) * g.N * (g.beta != 0.0f ? 2 : 1));
+      continue;
+    }
     BatchProblem b;
     memset(&b, 0, sizeof b);
     b.A = g.A; b.B = g.B; b.C = g.C;
@@ -368,13 +383,21 @@ hml_status batch_plan_create(hml_order order, const hml_gemm_desc *descs, int co
   *out = nullptr;
   std::vector<BatchProblem> probs;
   std::vector<BatchItem> items;
+  std::vector<GemmProblem> tc_probs;
   double flops, bytes;
-  hml_status st = build_host(order, descs, count, &probs, &items, &flops, &bytes);
+  hml_status st = build_host(order, descs, count, &probs, &items, &tc_probs, &flops, &bytes);
   if (st != HML_STATUS_SUCCESS) return st;
   st = kernel_attributes();
   if (st != HML_STATUS_SUCCESS) return st;
+  TcBatch *tc = nullptr;
+  st = tc_batch_create(tc_probs.data(), static_cast<int>(tc_probs.size()), nullptr, &tc);
+  if (st != HML_STATUS_SUCCESS) return st;
   BatchPlan *pl = new (std::nothrow) BatchPlan;
-  if (!pl) return HML_STATUS_ALLOC_FAILED;
+  if (!pl) {
+    tc_batch_destroy(tc);
+    return HML_STATUS_ALLOC_FAILED;
+  }
+  pl->tc = tc;
   cudaGetDevice(&pl->device);
   pl->count = count;
   pl->nitems = static_cast<int>(items.size());
@@ -386,6 +409,7 @@ hml_status batch_plan_create(hml_order order, const hml_gemm_desc *descs, int co
   cudaError_t e = cudaMalloc(&pl->dev, total);
   if (e != cudaSuccess) {
     note_cuda_error(e, "batch plan allocation");
+    tc_batch_destroy(pl->tc);
     delete pl;
     return HML_STATUS_ALLOC_FAILED;
   }
@@ -400,6 +424,7 @@ hml_status batch_plan_create(hml_order order, const hml_gemm_desc *descs, int co
   if (e != cudaSuccess) {
     note_cuda_error(e, "batch plan upload");
     cudaFree(pl->dev);
+    tc_batch_destroy(pl->tc);
     delete pl;
     return HML_STATUS_CUDA_ERROR;
   }
@@ -411,28 +436,38 @@ hml_status batch_plan_create(hml_order order, const hml_gemm_desc *descs, int co
   return HML_STATUS_SUCCESS;
 }
 
+// The plan's launches: the SIMT queue, then the split-BF16 part.
+hml_status launch_plan(BatchPlan *pl, cudaStream_t s) {
+  if (pl->nitems > 0) {
+    count_launch();
+    const cudaError_t e = launch_batched(pl->args, pl->ctas, s);
+    note_cuda_error(e, "batched launch");
+    if (e != cudaSuccess) return HML_STATUS_CUDA_ERROR;
+  }
+  return tc_batch_launch(pl->tc, s);
+}
+
+bool plan_empty(const BatchPlan *pl) { return pl->nitems == 0 && tc_batch_items(pl->tc) == 0; }
+
 hml_status batch_plan_run(BatchPlan *pl, cudaStream_t s) {
   if (!pl) return HML_STATUS_INVALID_VALUE;
-  if (pl->nitems == 0) return HML_STATUS_SUCCESS;
-  count_launch();
-  const cudaError_t e = launch_batched(pl->args, pl->ctas, s);
-  note_cuda_error(e, "batched launch");
-  return cuda_status(e);
+  if (plan_empty(pl)) return HML_STATUS_SUCCESS;
+  return launch_plan(pl, s);
 }
 
 hml_status batch_plan_graph_launch(BatchPlan *pl, cudaStream_t s) {
   if (!pl) return HML_STATUS_INVALID_VALUE;
-  if (pl->nitems == 0) return HML_STATUS_SUCCESS;
+  if (plan_empty(pl)) return HML_STATUS_SUCCESS;
   cudaError_t e = cudaSuccess;
   if (!pl->exec) {
-    // capture the single persistent launch once on a private stream
+    // capture the plan's launches once on a private stream
     e = cudaStreamCreateWithFlags(&pl->capture_stream, cudaStreamNonBlocking);
     if (e == cudaSuccess)
       e = cudaStreamBeginCapture(pl->capture_stream, cudaStreamCaptureModeThreadLocal);
     if (e == cudaSuccess) {
-      const cudaError_t el = launch_batched(pl->args, pl->ctas, pl->capture_stream);
+      const hml_status sl = launch_plan(pl, pl->capture_stream);
       e = cudaStreamEndCapture(pl->capture_stream, &pl->graph);
-      if (e == cudaSuccess) e = el;
+      if (e == cudaSuccess && sl != HML_STATUS_SUCCESS) e = cudaErrorLaunchFailure;
     }
     if (e == cudaSuccess) e = cudaGraphInstantiate(&pl->exec, pl->graph, 0);
     if (e != cudaSuccess) {
@@ -455,6 +490,7 @@ void batch_plan_destroy(BatchPlan *pl) {
   if (pl->graph) cudaGraphDestroy(pl->graph);
   if (pl->capture_stream) cudaStreamDestroy(pl->capture_stream);
   if (pl->dev) cudaFree(pl->dev);
+  tc_batch_destroy(pl->tc);
   delete pl;
 }
 
@@ -462,9 +498,20 @@ void batch_plan_destroy(BatchPlan *pl) {
 hml_status sgemm_batched(hml_order order, const hml_gemm_desc *descs, int count, cudaStream_t s) {
   std::vector<BatchProblem> probs;
   std::vector<BatchItem> items;
+  std::vector<GemmProblem> tc_probs;
   double flops, bytes;
-  hml_status st = build_host(order, descs, count, &probs, &items, &flops, &bytes);
-  if (st != HML_STATUS_SUCCESS || items.empty()) return st;
+  hml_status st = build_host(order, descs, count, &probs, &items, &tc_probs, &flops, &bytes);
+  if (st != HML_STATUS_SUCCESS) return st;
+  if (!tc_probs.empty()) {
+    // the split-BF16 part in stream-ordered memory, released after its launches
+    TcBatch *tc = nullptr;
+    st = tc_batch_create(tc_probs.data(), static_cast<int>(tc_probs.size()), s, &tc);
+    if (st != HML_STATUS_SUCCESS) return st;
+    st = tc_batch_launch(tc, s);
+    tc_batch_destroy(tc);
+    if (st != HML_STATUS_SUCCESS) return st;
+  }
+  if (items.empty()) return HML_STATUS_SUCCESS;
   st = kernel_attributes();
   if (st != HML_STATUS_SUCCESS) return st;
   size_t op, oi;
@@ -538,8 +585,9 @@ hml_status hml_batch_plan_graph_launch(hml_batch_plan plan, void *stream) {
 hml_status hml_batch_plan_info(hml_batch_plan plan, int *tiles, int *ctas, double *flops,
                                double *bytes) {
   if (!plan) return HML_STATUS_INVALID_VALUE;
-  if (tiles) *tiles = plan->impl->nitems;
-  if (ctas) *ctas = plan->impl->ctas;
+  if (tiles) *tiles = plan->impl->nitems + hml::tc_batch_items(plan->impl->tc);
+  if (ctas) *ctas = std::max(plan->impl->nitems > 0 ? plan->impl->ctas : 0,
+                             hml::tc_batch_ctas(plan->impl->tc));
   if (flops) *flops = plan->impl->flops;
   if (bytes) *bytes = plan->impl->bytes;
   return HML_STATUS_SUCCESS;
@@ -555,6 +603,25 @@ hml_status hml_batch_plan_destroy(hml_batch_plan plan) {
 hml_status hml_sgemm_batched(hml_order order, const hml_gemm_desc *descs, int count,
                              void *stream) {
   return hml::sgemm_batched(order, descs, count, static_cast<cudaStream_t>(stream));
+}
+
+hml_status hml_batch_problem_config(hml_order order, const hml_gemm_desc *desc,
+                                    hml_sgemm_config *config) {
+  using namespace hml;
+  if (!desc || !config) return HML_STATUS_INVALID_VALUE;
+  GemmProblem g;
+  hml_status st = gemm_from_blas(order, static_cast<hml_op>(desc->transA),
+                                 static_cast<hml_op>(desc->transB), desc->M, desc->N, desc->K,
+                                 desc->alpha, desc->A, desc->lda, desc->B, desc->ldb, desc->beta,
+                                 desc->C, desc->ldc, &g);
+  if (st != HML_STATUS_SUCCESS) return st;
+  if (g.M > 0 && g.N > 0 && tc_batch_eligible(g)) {
+    *config = tc_batch_config(g);
+    return HML_STATUS_SUCCESS;
+  }
+  const int slot = slot_for(g.N);
+  *config = hml_sgemm_config{HML_ALGO_SIMT, 128, kSlotN[slot], 1, 3, kSlotVariant[slot]};
+  return HML_STATUS_SUCCESS;
 }
 
 }  // extern "C"

@@ -59,6 +59,21 @@ hml_status launch_tc(const GemmProblem &p, const hml_sgemm_config &c, cudaStream
 hml_status check_simt(const GemmProblem &p, const hml_sgemm_config &c);
 hml_status check_tc(const GemmProblem &p, const hml_sgemm_config &c);
 
+// The split-BF16 part of a batched plan (sgemm_tc.cu): problems that
+// tc_batch_eligible accepts run as persistent tensor-core launches, one per
+// tile-width class, after one launch that splits every B into BF16 planes.
+// With `stream_ordered` the device memory is allocated and freed on that
+// stream.
+struct TcBatch;
+bool tc_batch_eligible(const GemmProblem &p);
+hml_status tc_batch_create(const GemmProblem *probs, int count, cudaStream_t stream_ordered,
+                           TcBatch **out);
+hml_status tc_batch_launch(const TcBatch *b, cudaStream_t s);
+void tc_batch_destroy(TcBatch *b);
+hml_sgemm_config tc_batch_config(const GemmProblem &p);
+int tc_batch_items(const TcBatch *b);
+int tc_batch_ctas(const TcBatch *b);
+
 // Per-device resources.
 int *device_error_word();  // nullptr on failure
 hml_status workspace(size_t bytes, cudaStream_t s, void **ptr);

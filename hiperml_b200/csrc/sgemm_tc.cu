@@ -44,6 +44,9 @@
 #include <algorithm>
 #include <cstring>
 #include <mutex>
+#include <new>
+#include <utility>
+#include <vector>
 
 #include "hml_device.cuh"
 #include "hml_internal.h"
@@ -782,6 +785,659 @@ hml_status launch_tc(const GemmProblem &p, const hml_sgemm_config &c, cudaStream
   if (st != HML_STATUS_SUCCESS) return st;
   return c.algo == HML_ALGO_BF16X3 ? run_tc_ns<2>(p, c, s) : run_tc_ns<3>(p, c, s);
 }
+
+}  // namespace hml
+
+// ------------------------------------------- batched split-BF16 (persistent)
+//
+// The batched plan (batched.cu) hands the problems it routes to the tensor
+// cores to tc_batch_create.  Each tile width class (BN = 32, 64, 128) gets one
+// persistent launch of tc_batch_kernel with one CTA per SM; every CTA works
+// through its own list of (problem, 128-row tile, BN-column tile) items,
+// assigned on the host longest-first to the least-loaded CTA, so CTAs never
+// share state and never wait for each other.  The pipeline inside a CTA is
+// the single-problem kernel's (TMA warps, converter groups, MMA issuers with
+// one TMEM accumulator each, drain warps) walking the 64-deep chunks of its
+// items in order; the TMA descriptors of every problem sit in device memory.
+// A tile's arithmetic is the single-problem kernel's with split_k = 1, so
+// each result equals hml_sgemm_ex_config's for the same tile width, bit for
+// bit.
+namespace hml {
+namespace {
+
+struct TcBatchProblem {
+  float *C;
+  int64_t scm, scn;
+  int M, N;
+  float alpha, beta;
+  int akc;    // 1: A is K-contiguous (128 x 32 boxes, 128-byte swizzle)
+  int cpt;    // 64-deep chunks of K (K padded to 64)
+  int n_pad;  // rows of one B plane
+  int pad_;
+};
+
+struct TcBatchItem {
+  int prob, tm, tn, pad_;
+};
+
+struct TcBatchArgs {
+  const CUtensorMap *tmA;       // [problems], 64-byte aligned
+  const CUtensorMap *tmB;       // [problems]
+  const TcBatchProblem *probs;  // [problems]
+  const TcBatchItem *items;     // this class's items, grouped by CTA
+  const int2 *cta;              // [grid]: first item of the CTA, its number of chunks
+  int sa, so;
+  int *err;
+};
+
+// Walks the chunks of a CTA's item list in order.  next() is called before
+// every chunk but the first, so it never reads past the CTA's last item.
+struct ItemCursor {
+  TcBatchItem it;
+  const TcBatchProblem *pr;
+  int item, c;
+  __device__ __forceinline__ void start(const TcBatchArgs &a, int i0) {
+    item = i0;
+    c = 0;
+    it = a.items[item];
+    pr = a.probs + it.prob;
+  }
+  __device__ __forceinline__ void next(const TcBatchArgs &a) {
+    if (++c == pr->cpt) {
+      c = 0;
+      ++item;
+      it = a.items[item];
+      pr = a.probs + it.prob;
+    }
+  }
+};
+
+// Drain warpgroups of the batched kernel: 32 columns each (its drain also
+// finishes C tiles, so it keeps fewer running sums per thread).
+__host__ __device__ constexpr int tcb_drain_groups(int bn) { return bn >= 32 ? bn / 32 : 1; }
+__host__ __device__ constexpr int tcb_warps(int bn, int ns) {
+  return tc_conv_warp0(bn, ns) + 4 * tc_groups() + 4 * tcb_drain_groups(bn);
+}
+
+template <int BN, int NS>
+__global__ void __launch_bounds__(tcb_warps(BN, NS) * 32, 1) tc_batch_kernel(TcBatchArgs args) {
+  constexpr int G = tc_groups();
+  constexpr int D = tcb_drain_groups(BN);
+  constexpr int DC = BN / D;
+  constexpr int NI = tc_issuers(BN, NS);
+  constexpr int kConvWarp0 = tc_conv_warp0(BN, NS), kDrainWarp0 = kConvWarp0 + 4 * G;
+  constexpr int A32_BYTES = static_cast<int>(tc_a_bytes());
+  constexpr int BPL_BYTES = BN * kBK * 2;
+  constexpr int BSLOT = NS * BPL_BYTES;
+  constexpr int SC = tc_stage_cols(NS);
+  constexpr uint32_t IDESC = idesc_bf16(BN);
+  constexpr int P = kChunkK / kBK;
+  static_assert(G == P, "converter group g converts block g of every chunk");
+
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t *smem = reinterpret_cast<uint8_t *>(
+      (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~static_cast<uintptr_t>(1023));
+  const int SA = args.sa, SO = args.so;
+  uint8_t *aring = smem;
+  uint8_t *bring = aring + SA * A32_BYTES;
+  uint64_t *afull = reinterpret_cast<uint64_t *>(bring + SO * BSLOT);
+  uint64_t *aempty = afull + SA;
+  uint64_t *opfull = aempty + SA;
+  uint64_t *opempty = opfull + SO;
+  uint64_t *accfull = opempty + SO;
+  uint64_t *accempty = accfull + NI;
+  uint64_t *mmadone = accempty + NI;
+  uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(mmadone + 1);
+
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int2 work = args.cta[blockIdx.x];
+  const int i0 = work.x, nch = work.y, nblk = nch * P;
+  const uint32_t tmem_cols = tc_tmem_alloc_cols(BN, NS, SO);
+
+  if (tid == 0) {
+    for (int s = 0; s < SA; ++s) {
+      mbar_init(&afull[s], 1);
+      mbar_init(&aempty[s], 4);
+    }
+    for (int o = 0; o < SO; ++o) {
+      mbar_init(&opfull[o], 4 + 1);
+      mbar_init(&opempty[o], 1);
+    }
+    for (int b = 0; b < NI; ++b) {
+      mbar_init(&accfull[b], 1);
+      mbar_init(&accempty[b], 4 * D);
+    }
+    mbar_init(mmadone, NI);
+    fence_mbar_init();
+  }
+  if (warp == 2) tmem_alloc(tmem_slot, tmem_cols);
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tmem_slot;
+  const uint32_t tacc = tmem;
+  const uint32_t tA = tmem + NI * BN;
+
+  if (warp == 0) {
+    // -------------------------------------------------------- TMA, A
+    if (lane == 0 && nch > 0) {
+      ItemCursor cur;
+      cur.start(args, i0);
+      for (int blk = 0; blk < nblk; ++blk) {
+        if (blk > 0 && blk % P == 0) cur.next(args);
+        const CUtensorMap *tm = args.tmA + cur.it.prob;
+        const int m0 = cur.it.tm * kBM;
+        const int k0 = (cur.c * P + blk % P) * kBK;
+        const int s = blk % SA;
+        if (!mbar_wait(&aempty[s], ((blk / SA) & 1) ^ 1, args.err, kDevErrEmptyBarrier)) break;
+        mbar_arrive_expect_tx(&afull[s], A32_BYTES);
+        // k beyond K (the last chunk of a problem) reads TMA's zero fill
+        if (cur.pr->akc)
+          tma_load_2d(aring + s * A32_BYTES, tm, &afull[s], k0, m0);
+        else
+          tma_load_2d(aring + s * A32_BYTES, tm, &afull[s], m0, k0);
+      }
+    }
+  } else if (warp == 1) {
+    // -------------------------------------------------------- TMA, B
+    if (lane == 0 && nch > 0) {
+      ItemCursor cur;
+      cur.start(args, i0);
+      for (int blk = 0; blk < nblk; ++blk) {
+        if (blk > 0 && blk % P == 0) cur.next(args);
+        const CUtensorMap *tm = args.tmB + cur.it.prob;
+        const int n0 = cur.it.tn * BN;
+        const int k0 = (cur.c * P + blk % P) * kBK;
+        const int np = cur.pr->n_pad;
+        const int o = blk % SO;
+        if (!mbar_wait(&opempty[o], ((blk / SO) & 1) ^ 1, args.err, kDevErrEmptyBarrier)) break;
+        uint8_t *dst = bring + o * BSLOT;
+        mbar_arrive_expect_tx(&opfull[o], BSLOT);
+#pragma unroll
+        for (int i = 0; i < NS; ++i)
+          tma_load_2d(dst + i * BPL_BYTES, tm, &opfull[o], k0, i * np + n0);
+      }
+    }
+  } else if (warp >= 2 && warp < 2 + NI) {
+    // ---------------------------------------------------------- MMA
+    if (lane == 0) {
+      const int b = warp - 2;
+      const uint32_t dacc = tacc + static_cast<uint32_t>(b * BN);
+      bool ok = true;
+      for (int j = b; j < nch && ok; j += NI) {
+        if (!mbar_wait(&accempty[b], ((j / NI) & 1) ^ 1, args.err, kDevErrEmptyBarrier)) {
+          ok = false;
+          break;
+        }
+        for (int kb = 0; kb < P; ++kb) {
+          const int blk = j * P + kb;
+          const int o = blk % SO;
+          if (!mbar_wait(&opfull[o], (blk / SO) & 1, args.err, kDevErrFullBarrier)) {
+            ok = false;
+            break;
+          }
+          tc_fence_after();
+          const uint32_t astage = tA + static_cast<uint32_t>(o * SC);
+          const uint64_t b_desc = sw64_desc(smem_u32(bring + o * BSLOT));
+#pragma unroll
+          for (int kk = 0; kk < kBK / 16; ++kk) {
+#pragma unroll
+            for (int i = 0; i < NS; ++i)
+#pragma unroll
+              for (int jj = 0; jj < NS - i; ++jj) {
+                const uint32_t at = astage + static_cast<uint32_t>(i * 16 + kk * 8);
+                const uint64_t bd =
+                    b_desc + static_cast<uint64_t>((jj * BPL_BYTES + kk * 32) >> 4);
+                const uint32_t acc = (kb > 0 || kk > 0 || i > 0 || jj > 0) ? 1u : 0u;
+                mma_bf16_ts(dacc, at, bd, IDESC, acc);
+              }
+          }
+          mma_commit(&opempty[o]);
+        }
+        if (ok) mma_commit(&accfull[b]);
+      }
+      mma_commit(mmadone);
+    }
+  } else if (warp >= kConvWarp0 && warp < kDrainWarp0) {
+    // ------------------------------------------ converters (G groups)
+    // group g converts block g of every chunk (G == P)
+    const int g = (warp - kConvWarp0) >> 2;
+    const int m = tid & (kBM - 1);
+    const uint32_t lanes = static_cast<uint32_t>((warp & 3) * 32) << 16;
+    ItemCursor cur;
+    if (nch > 0) cur.start(args, i0);
+    for (int j = 0; j < nch; ++j) {
+      if (j > 0) cur.next(args);
+      const int blk = j * P + g;
+      const int s = blk % SA, o = blk % SO;
+      bool w = mbar_wait(&afull[s], (blk / SA) & 1, args.err, kDevErrFullBarrier);
+      if (!__all_sync(0xffffffffu, w)) break;
+      const float *a32 = reinterpret_cast<const float *>(aring + s * A32_BYTES);
+      float x[32];
+      if (cur.pr->akc) {
+        // row m holds 32 floats in 128 bytes, 128-byte swizzle
+#pragma unroll
+        for (int c = 0; c < 8; ++c) {
+          const float4 v = *reinterpret_cast<const float4 *>(a32 + m * 32 + ((c ^ (m & 7)) * 4));
+          x[4 * c + 0] = v.x; x[4 * c + 1] = v.y; x[4 * c + 2] = v.z; x[4 * c + 3] = v.w;
+        }
+      } else {
+#pragma unroll
+        for (int k = 0; k < 32; ++k) x[k] = a32[k * kBM + m];
+      }
+      uint32_t wv[16];
+      split_plane32<NS == 1>(x, wv);
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&aempty[s]);
+      w = mbar_wait(&opempty[o], ((blk / SO) & 1) ^ 1, args.err, kDevErrEmptyBarrier);
+      if (!__all_sync(0xffffffffu, w)) break;
+      tc_fence_after();
+      const uint32_t dst = tA + lanes + static_cast<uint32_t>(o * SC);
+      tmem_st16(dst, wv);
+      split_plane32<NS == 2>(x, wv);
+      tmem_st16(dst + 16u, wv);
+      if constexpr (NS == 3) {
+        split_plane32<true>(x, wv);
+        tmem_st16(dst + 32u, wv);
+      }
+      tmem_wait_st();
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&opfull[o]);
+    }
+  } else if (warp >= kDrainWarp0) {
+    // ------------------------------------------ drain (D groups)
+    const int d = (warp - kDrainWarp0) >> 2;
+    const int m = tid & (kBM - 1);
+    const uint32_t lanes = static_cast<uint32_t>((warp & 3) * 32) << 16;
+    float sums[DC];
+#pragma unroll
+    for (int i = 0; i < DC; ++i) sums[i] = 0.0f;
+    ItemCursor cur;
+    if (nch > 0) cur.start(args, i0);
+    for (int j = 0; j < nch; ++j) {
+      if (j > 0) cur.next(args);
+      const int b = j % NI;
+      const bool w = mbar_wait(&accfull[b], (j / NI) & 1, args.err, kDevErrMmaBarrier);
+      if (!__all_sync(0xffffffffu, w)) break;
+      tc_fence_after();
+      const uint32_t src = tacc + lanes + static_cast<uint32_t>(b * BN + d * DC);
+      if constexpr (DC >= 16) {
+#pragma unroll
+        for (int c = 0; c < DC; c += 16) {
+          uint32_t r0[16];
+          tmem_ld16(src + c, r0);
+          tmem_wait_ld();
+#pragma unroll
+          for (int i = 0; i < 16; ++i) sums[c + i] += __uint_as_float(r0[i]);
+        }
+      } else {
+        static_assert(DC % 8 == 0, "drain width");
+        uint32_t r0[8];
+        tmem_ld8(src, r0);
+        tmem_wait_ld();
+#pragma unroll
+        for (int i = 0; i < 8; ++i) sums[i] += __uint_as_float(r0[i]);
+      }
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&accempty[b]);
+      if (cur.c == cur.pr->cpt - 1) {
+        // the item's last chunk: C tile (row m, columns d*DC ..) and reset
+        const TcBatchProblem &pr = *cur.pr;
+        const int64_t gm = static_cast<int64_t>(cur.it.tm) * kBM + m;
+        const int nb = cur.it.tn * BN + d * DC;
+        if (gm < pr.M) {
+#pragma unroll
+          for (int i = 0; i < DC; ++i) {
+            if (nb + i < pr.N) {
+              float *cp = pr.C + gm * pr.scm + static_cast<int64_t>(nb + i) * pr.scn;
+              *cp = axpby(pr.alpha, sums[i], pr.beta, cp);
+            }
+          }
+        }
+#pragma unroll
+        for (int i = 0; i < DC; ++i) sums[i] = 0.0f;
+      }
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 2) {
+    bool w = true;
+    if (lane == 0) w = mbar_wait(mmadone, 0, args.err, kDevErrMmaBarrier);
+    __syncwarp();
+    (void)w;
+    tc_fence_after();
+    tmem_dealloc(tmem, tmem_cols);
+  }
+}
+
+// B of every routed problem -> its BF16 planes, one launch: blockIdx.y is the
+// problem, the x blocks stride over its (n, 8-deep k) chunks.
+struct TcSplitDesc {
+  const float *B;
+  int64_t sbk, sbn;
+  int K, N, k_pad, n_pad;
+  __nv_bfloat16 *planes;
+};
+
+template <int NS>
+__global__ void split_b_batch_kernel(const TcSplitDesc *descs) {
+  const TcSplitDesc d = descs[blockIdx.y];
+  const int64_t chunks = static_cast<int64_t>(d.n_pad) * (d.k_pad / 8);
+  for (int64_t c = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; c < chunks;
+       c += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int n = static_cast<int>(c / (d.k_pad / 8));
+    const int k0 = static_cast<int>(c % (d.k_pad / 8)) * 8;
+    float x[8];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      const int k = k0 + j;
+      x[j] = (n < d.N && k < d.K)
+                 ? d.B[static_cast<int64_t>(k) * d.sbk + static_cast<int64_t>(n) * d.sbn]
+                 : 0.0f;
+    }
+    uint4 v[NS];
+    pack8<NS>(x, v);
+#pragma unroll
+    for (int i = 0; i < NS; ++i)
+      *reinterpret_cast<uint4 *>(d.planes + (static_cast<int64_t>(i) * d.n_pad + n) * d.k_pad +
+                                 k0) = v[i];
+  }
+}
+
+constexpr int kBatchTcNS = 3;                     // BF16X6: FP32-level accuracy
+constexpr int kBatchTcBN[] = {32, 64, 128};       // tile width classes
+
+int batch_tc_class(int N) { return N <= 32 ? 0 : N <= 64 ? 1 : 2; }
+
+}  // namespace
+
+// Host side of the batched split-BF16 part of a plan.
+struct TcBatch {
+  int nprob = 0;
+  int items = 0;
+  int ctas = 0;                   // the widest class launch
+  void *dev = nullptr;            // one device allocation holding everything below
+  cudaStream_t owner = nullptr;   // stream of a stream-ordered allocation, if any
+  const TcSplitDesc *splits = nullptr;
+  int split_blocks = 1;
+  struct Class {
+    int grid = 0;
+    size_t smem = 0;
+    TcBatchArgs args = {};
+  } cls[3];
+};
+
+// Problems the batched plan can run on the tensor cores: A addressable by TMA
+// (16-byte aligned base, leading dimension a multiple of 16 bytes), a real
+// product (K > 0, alpha != 0) and N > 8 (at N <= 8 the FP32 SIMT tile is
+// faster).
+bool tc_batch_eligible(const GemmProblem &p) {
+  if (p.N <= 8 || p.M < 1 || p.K < 1 || p.alpha == 0.0f) return false;
+  const int64_t sa = p.a_kcontig() ? p.sam : p.sak;
+  if ((reinterpret_cast<uintptr_t>(p.A) & 15u) != 0 || (sa * 4) % 16 != 0) return false;
+  if (p.a_kcontig() ? p.sak != 1 : p.sam != 1) return false;
+  return true;
+}
+
+namespace {
+
+size_t up256(size_t b) { return (b + 255) & ~static_cast<size_t>(255); }
+
+template <int BN>
+hml_status tc_batch_class_setup(TcBatch::Class &c) {
+  TcPlan plan;
+  int sa = 8;
+  while (sa >= 2 && !tc_plan(BN, kBatchTcNS, sa, &plan)) sa -= 2;
+  if (sa < 2) return HML_STATUS_NOT_SUPPORTED;
+  c.args.sa = plan.sa;
+  c.args.so = plan.so;
+  c.smem = tc_plan_bytes(BN, kBatchTcNS, plan);
+  const cudaError_t e = cudaFuncSetAttribute(tc_batch_kernel<BN, kBatchTcNS>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             static_cast<int>(c.smem));
+  if (e != cudaSuccess) {
+    note_cuda_error(e, "tc batch attributes");
+    return HML_STATUS_CUDA_ERROR;
+  }
+  return HML_STATUS_SUCCESS;
+}
+
+}  // namespace
+
+hml_status tc_batch_create(const GemmProblem *probs, int count, cudaStream_t stream_ordered,
+                           TcBatch **out) {
+  *out = nullptr;
+  if (count <= 0) return HML_STATUS_SUCCESS;
+  if (count > 65535) return HML_STATUS_NOT_SUPPORTED;  // grid.y of the split launch
+  const int sms = sm_count();
+  // per problem: class, padded sizes, planes
+  std::vector<int> cls(count), k_pad(count), n_pad(count);
+  std::vector<size_t> plane_off(count);
+  size_t planes_bytes = 0;
+  std::vector<std::vector<std::pair<int, TcBatchItem>>> items(3);  // (cost, item)
+  int64_t max_chunks = 1;
+  for (int i = 0; i < count; ++i) {
+    const GemmProblem &p = probs[i];
+    cls[i] = batch_tc_class(p.N);
+    const int bn = kBatchTcBN[cls[i]];
+    k_pad[i] = ((p.K + kChunkK - 1) / kChunkK) * kChunkK;
+    n_pad[i] = ((p.N + bn - 1) / bn) * bn;
+    plane_off[i] = planes_bytes;
+    planes_bytes += up256(static_cast<size_t>(kBatchTcNS) * n_pad[i] * k_pad[i] * 2);
+    max_chunks = std::max<int64_t>(max_chunks, static_cast<int64_t>(n_pad[i]) * (k_pad[i] / 8));
+    const int64_t tm = (static_cast<int64_t>(p.M) + kBM - 1) / kBM, tn = n_pad[i] / bn;
+    if (tm > 0x7fffffff) return HML_STATUS_NOT_SUPPORTED;
+    for (int64_t x = 0; x < tm; ++x)
+      for (int64_t y = 0; y < tn; ++y)
+        items[cls[i]].push_back({k_pad[i] / kChunkK, TcBatchItem{i, static_cast<int>(x),
+                                                                 static_cast<int>(y), 0}});
+  }
+  // longest-processing-time assignment per class: items longest first, each
+  // to the CTA with the least work so far; then grouped by CTA
+  std::vector<TcBatchItem> cls_items[3];
+  std::vector<int2> cls_cta[3];
+  size_t total_items = 0;
+  for (int c = 0; c < 3; ++c) {
+    auto &v = items[c];
+    if (v.empty()) continue;
+    std::stable_sort(v.begin(), v.end(),
+                     [](const std::pair<int, TcBatchItem> &a, const std::pair<int, TcBatchItem> &b) {
+                       return a.first > b.first;
+                     });
+    const int grid = static_cast<int>(std::min<size_t>(v.size(), static_cast<size_t>(sms)));
+    std::vector<std::vector<TcBatchItem>> per(grid);
+    std::vector<int64_t> load(grid, 0);
+    // (load, cta) min-heap
+    std::vector<std::pair<int64_t, int>> heap;
+    for (int g = 0; g < grid; ++g) heap.push_back({0, g});
+    auto cmp = [](const std::pair<int64_t, int> &a, const std::pair<int64_t, int> &b) {
+      return a.first != b.first ? a.first > b.first : a.second > b.second;
+    };
+    std::make_heap(heap.begin(), heap.end(), cmp);
+    for (const auto &e : v) {
+      std::pop_heap(heap.begin(), heap.end(), cmp);
+      auto &top = heap.back();
+      per[top.second].push_back(e.second);
+      top.first += e.first;
+      load[top.second] = top.first;
+      std::push_heap(heap.begin(), heap.end(), cmp);
+    }
+    for (int g = 0; g < grid; ++g) {
+      const int first = static_cast<int>(cls_items[c].size());
+      int64_t chunks = 0;
+      for (const auto &it : per[g]) {
+        cls_items[c].push_back(it);
+        chunks += k_pad[it.prob] / kChunkK;
+      }
+      if (chunks > 0x7fffffff / kChunkK) return HML_STATUS_NOT_SUPPORTED;
+      cls_cta[c].push_back(make_int2(first, static_cast<int>(chunks)));
+    }
+    total_items += v.size();
+  }
+  // device layout: tensor maps | problems | split descriptors | per class
+  // items and CTA table | planes
+  const size_t o_tmA = 0, o_tmB = up256(count * sizeof(CUtensorMap));
+  const size_t o_prob = o_tmB + up256(count * sizeof(CUtensorMap));
+  const size_t o_split = o_prob + up256(count * sizeof(TcBatchProblem));
+  size_t o = o_split + up256(count * sizeof(TcSplitDesc));
+  size_t o_items[3], o_cta[3];
+  for (int c = 0; c < 3; ++c) {
+    o_items[c] = o;
+    o += up256(cls_items[c].size() * sizeof(TcBatchItem));
+    o_cta[c] = o;
+    o += up256(cls_cta[c].size() * sizeof(int2));
+  }
+  const size_t o_planes = o;
+  const size_t total = o_planes + planes_bytes;
+
+  TcBatch *b = new (std::nothrow) TcBatch;
+  if (!b) return HML_STATUS_ALLOC_FAILED;
+  cudaError_t e = stream_ordered ? cudaMallocAsync(&b->dev, total, stream_ordered)
+                                 : cudaMalloc(&b->dev, total);
+  if (e != cudaSuccess) {
+    note_cuda_error(e, "tc batch allocation");
+    delete b;
+    return HML_STATUS_ALLOC_FAILED;
+  }
+  b->owner = stream_ordered;
+  uint8_t *base = static_cast<uint8_t *>(b->dev);
+  // host images
+  std::vector<CUtensorMap> tmA(count), tmB(count);
+  std::vector<TcBatchProblem> hp(count);
+  std::vector<TcSplitDesc> hs(count);
+  bool ok = true;
+  for (int i = 0; i < count && ok; ++i) {
+    const GemmProblem &p = probs[i];
+    const int bn = kBatchTcBN[cls[i]];
+    auto *planes = reinterpret_cast<__nv_bfloat16 *>(base + o_planes + plane_off[i]);
+    memset(&tmA[i], 0, sizeof(CUtensorMap));
+    memset(&tmB[i], 0, sizeof(CUtensorMap));
+    if (p.a_kcontig())
+      ok = tensor_map_2d(&tmA[i], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, p.A, p.K, p.M, p.sam * 4, kBK,
+                         kBM, CU_TENSOR_MAP_SWIZZLE_128B);
+    else
+      ok = tensor_map_2d(&tmA[i], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, p.A, p.M, p.K, p.sak * 4, kBM,
+                         kBK, CU_TENSOR_MAP_SWIZZLE_NONE);
+    if (ok)
+      ok = tensor_map_2d(&tmB[i], CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, planes, k_pad[i],
+                         static_cast<uint64_t>(kBatchTcNS) * n_pad[i],
+                         static_cast<uint64_t>(k_pad[i]) * 2, kBK, bn, CU_TENSOR_MAP_SWIZZLE_64B);
+    TcBatchProblem &q = hp[i];
+    memset(&q, 0, sizeof q);
+    q.C = p.C;
+    q.scm = p.scm;
+    q.scn = p.scn;
+    q.M = p.M;
+    q.N = p.N;
+    q.alpha = p.alpha;
+    q.beta = p.beta;
+    q.akc = p.a_kcontig() ? 1 : 0;
+    q.cpt = k_pad[i] / kChunkK;
+    q.n_pad = n_pad[i];
+    hs[i] = TcSplitDesc{p.B, p.sbk, p.sbn, p.K, p.N, k_pad[i], n_pad[i], planes};
+  }
+  auto upload = [&](size_t off, const void *src, size_t bytes) {
+    if (e != cudaSuccess || bytes == 0) return;
+    e = stream_ordered ? cudaMemcpyAsync(base + off, src, bytes, cudaMemcpyHostToDevice,
+                                         stream_ordered)
+                       : cudaMemcpy(base + off, src, bytes, cudaMemcpyHostToDevice);
+  };
+  if (ok) {
+    upload(o_tmA, tmA.data(), count * sizeof(CUtensorMap));
+    upload(o_tmB, tmB.data(), count * sizeof(CUtensorMap));
+    upload(o_prob, hp.data(), count * sizeof(TcBatchProblem));
+    upload(o_split, hs.data(), count * sizeof(TcSplitDesc));
+    for (int c = 0; c < 3; ++c) {
+      upload(o_items[c], cls_items[c].data(), cls_items[c].size() * sizeof(TcBatchItem));
+      upload(o_cta[c], cls_cta[c].data(), cls_cta[c].size() * sizeof(int2));
+    }
+    // pageable sources: a synchronous copy has consumed them on return; the
+    // stream-ordered ones have been staged by the driver before returning
+  }
+  hml_status st = ok ? cuda_status(e) : HML_STATUS_CUDA_ERROR;
+  for (int c = 0; c < 3 && st == HML_STATUS_SUCCESS; ++c) {
+    TcBatch::Class &k = b->cls[c];
+    k.grid = static_cast<int>(cls_cta[c].size());
+    if (k.grid == 0) continue;
+    st = c == 0   ? tc_batch_class_setup<32>(k)
+         : c == 1 ? tc_batch_class_setup<64>(k)
+                  : tc_batch_class_setup<128>(k);
+    k.args.tmA = reinterpret_cast<const CUtensorMap *>(base + o_tmA);
+    k.args.tmB = reinterpret_cast<const CUtensorMap *>(base + o_tmB);
+    k.args.probs = reinterpret_cast<const TcBatchProblem *>(base + o_prob);
+    k.args.items = reinterpret_cast<const TcBatchItem *>(base + o_items[c]);
+    k.args.cta = reinterpret_cast<const int2 *>(base + o_cta[c]);
+    k.args.err = device_error_word();
+    b->ctas = std::max(b->ctas, k.grid);
+  }
+  if (st != HML_STATUS_SUCCESS) {
+    if (e != cudaSuccess) note_cuda_error(e, "tc batch upload");
+    tc_batch_destroy(b);
+    return st;
+  }
+  b->nprob = count;
+  b->items = static_cast<int>(total_items);
+  b->splits = reinterpret_cast<const TcSplitDesc *>(base + o_split);
+  b->split_blocks = static_cast<int>(std::min<int64_t>((max_chunks + 255) / 256, 64));
+  *out = b;
+  return HML_STATUS_SUCCESS;
+}
+
+hml_status tc_batch_launch(const TcBatch *b, cudaStream_t s) {
+  if (!b || b->nprob == 0) return HML_STATUS_SUCCESS;
+  count_launch();
+  split_b_batch_kernel<kBatchTcNS>
+      <<<dim3(static_cast<unsigned>(b->split_blocks), static_cast<unsigned>(b->nprob)), 256, 0,
+         s>>>(b->splits);
+  cudaError_t e = cudaGetLastError();
+  for (int c = 0; c < 3 && e == cudaSuccess; ++c) {
+    const TcBatch::Class &k = b->cls[c];
+    if (k.grid == 0) continue;
+    count_launch();
+    if (c == 0)
+      tc_batch_kernel<32, kBatchTcNS>
+          <<<k.grid, tcb_warps(32, kBatchTcNS) * 32, k.smem, s>>>(k.args);
+    else if (c == 1)
+      tc_batch_kernel<64, kBatchTcNS>
+          <<<k.grid, tcb_warps(64, kBatchTcNS) * 32, k.smem, s>>>(k.args);
+    else
+      tc_batch_kernel<128, kBatchTcNS>
+          <<<k.grid, tcb_warps(128, kBatchTcNS) * 32, k.smem, s>>>(k.args);
+    e = cudaGetLastError();
+  }
+  note_cuda_error(e, "tc batch launch");
+  return cuda_status(e);
+}
+
+void tc_batch_destroy(TcBatch *b) {
+  if (!b) return;
+  if (b->dev) {
+    if (b->owner)
+      cudaFreeAsync(b->dev, b->owner);
+    else
+      cudaFree(b->dev);
+  }
+  delete b;
+}
+
+// The configuration under which a batched plan runs an eligible problem:
+// its tile width class and the A-ring depth the class launch uses; the
+// single-problem kernel with this configuration computes the same bits.
+hml_sgemm_config tc_batch_config(const GemmProblem &p) {
+  const int bn = kBatchTcBN[batch_tc_class(p.N)];
+  int sa = 8;
+  TcPlan plan;
+  while (sa > 2 && !tc_plan(bn, kBatchTcNS, sa, &plan)) sa -= 2;
+  int var = 0;
+  while (var + 1 < kNumTcShapes && kTcShapes[var].bn != bn) ++var;
+  return hml_sgemm_config{HML_ALGO_BF16X6, kBM, bn, 1, sa, var};
+}
+
+int tc_batch_items(const TcBatch *b) { return b ? b->items : 0; }
+int tc_batch_ctas(const TcBatch *b) { return b ? b->ctas : 0; }
 
 }  // namespace hml
 

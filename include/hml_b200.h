@@ -270,16 +270,20 @@ typedef struct hml_batch_plan_s *hml_batch_plan;
 
 /* Builds a plan for a batch: validates every problem, cuts all of them into
  * tile work items ordered longest first, and uploads the items to the
- * device.  The reference has no batched form: its callers loop over
+ * device.  Problems with N > 8 (in the long-M form) whose A TMA can address
+ * (16-byte aligned base, leading dimension a multiple of 4 floats) run as
+ * split-BF16 (BF16X6) tensor-core tiles, the others as FP32 SIMT tiles.  The reference has no batched form: its callers loop over
  * hmlSgemm, one launch and one synchronisation per problem
  * (src/hml_sgemm.cu:120-211).  The descriptors are copied; the matrices they
  * point to are read when the plan runs. */
 hml_status hml_batch_plan_create(hml_order order, const hml_gemm_desc *descs,
                                  int count, hml_batch_plan *plan);
 
-/* Runs every problem of the plan in ONE persistent kernel launch whose CTAs
- * take tiles from a device work queue.  Stream ordered; capturable.  One
- * plan runs on one stream at a time. */
+/* Runs every problem of the plan: the SIMT tiles in ONE persistent kernel
+ * launch whose CTAs take tiles from a device work queue, the tensor-core
+ * tiles in one B-splitting launch and one persistent launch per tile width
+ * (32, 64, 128 columns) whose CTAs work through host-balanced item lists.
+ * Stream ordered; capturable.  One plan runs on one stream at a time. */
 hml_status hml_batch_plan_run(hml_batch_plan plan, void *stream);
 
 /* Same, through a CUDA graph holding the launch: the first call captures
@@ -294,9 +298,15 @@ hml_status hml_batch_plan_info(hml_batch_plan plan, int *tiles, int *ctas,
                                double *flops, double *bytes);
 hml_status hml_batch_plan_destroy(hml_batch_plan plan);
 
-/* One-shot batch: plan, one launch and release, all stream ordered. */
+/* One-shot batch: plan, its launches and release, all stream ordered. */
 hml_status hml_sgemm_batched(hml_order order, const hml_gemm_desc *descs,
                              int count, void *stream);
+
+/* The configuration under which a batch runs this problem (an FP32 SIMT tile
+ * or BF16X6 with the tile width class); hml_sgemm_ex_config with it computes
+ * the same bits.  No counterpart in the reference, which has no batches. */
+hml_status hml_batch_problem_config(hml_order order, const hml_gemm_desc *desc,
+                                    hml_sgemm_config *config);
 
 /* ---------------------------------------------------------------- SGEMV */
 

@@ -1,9 +1,11 @@
-"""Batched SGEMM: many uneven problems in one persistent launch (GPU).
+"""Batched SGEMM: many uneven problems in persistent launches (GPU).
 
 Every problem of a batch is checked two ways: bit for bit against the
-single-problem FP32 SIMT kernel run with the same tile shape and split_k = 1
-(the batched kernel shares its tile arithmetic), and against the FP64 oracle
-within the classical FP32 bound gamma_{K+2} (|alpha||A||B| + |beta||C|)."""
+single-problem kernel run with the configuration the batch reports for it
+(hml_batch_problem_config: the FP32 SIMT tile, or BF16X6 tensor-core tiles
+for N > 8 with split_k = 1; the batched kernels share the tile arithmetic),
+and against the FP64 oracle within the classical FP32 bound
+gamma_{K+2} (|alpha||A||B| + |beta||C|)."""
 import numpy as np
 import pytest
 
@@ -14,17 +16,6 @@ from hiperml_b200._lib import SgemmConfig, lib
 from tests.gpu_util import assert_within_fp32_bound
 
 pytestmark = pytest.mark.gpu
-
-# batched tile slots: canonical N up to 8, 16, 32, 64, 128 (and wider)
-_SLOTS = ((8, 1, 8), (16, 0, 16), (32, 2, 32), (64, 7, 64), (1 << 30, 8, 128))
-
-
-def slot_config(M, N):
-    nc = min(M, N)  # the canonical form has the long dimension as M
-    for top, var, bn in _SLOTS:
-        if nc <= top:
-            return SgemmConfig(hml.ALGO_SIMT, 128, bn, 1, 3, var)
-
 
 class Problem:
     """One problem with its own device buffers (storage order, ld padding and
@@ -72,13 +63,13 @@ class Problem:
         return h[:self.M * self.ldc].reshape(self.M, self.ldc)[:, :self.N].copy()
 
     def single(self):
-        """The single-problem SIMT kernel with this problem's batched tile."""
+        """The single-problem kernel with this problem's batched configuration."""
         import torch
         keep = self.Cb.clone()
         self.reset()
         hml.sgemm_ex(self.order, self.ta, self.tb, self.M, self.N, self.K, self.alpha, self.Ap,
                      self.lda, self.Bp, self.ldb, self.beta, self.Cp, self.ldc,
-                     config=slot_config(self.M, self.N))
+                     config=hml.batch_problem_config(self.order, self.desc()))
         torch.cuda.synchronize()
         out = self.result()
         self.Cb.copy_(keep)
