@@ -114,6 +114,10 @@ std::vector<hml_sgemm_config> build_space() {
     for (int var = 0; var < tc_num_shapes(); ++var) {
       int bm, bn;
       tc_shape(var, &bm, &bn);
+      // CTA-pair tiles are explicit configurations only: correct (bitwise
+      // equal to the 128-row tile) but measured slower on B200, the
+      // per-block handshakes between the two CTAs costing about 1 us
+      if (bm != 128) continue;
       for (int split : {1, 2, 4, 8, 16})
         for (int stages : {2, 4, 6, 8}) {  // A-ring depths: multiples of the converter groups
           if (!tc_config_fits(bn, algo == HML_ALGO_BF16X3 ? 2 : 3, stages)) continue;

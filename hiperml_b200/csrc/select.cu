@@ -43,13 +43,13 @@ hml_sgemm_config heuristic_config(const GemmProblem &p, int algo) {
   hml_sgemm_config c = {};
   if (algo == HML_ALGO_BF16X3 || algo == HML_ALGO_BF16X6) {
     int best = -1;
+    // the narrowest single-CTA (128-row) tile that holds N
     for (int v = 0; v < tc_num_shapes(); ++v) {
       int bm, bn;
       tc_shape(v, &bm, &bn);
-      if (bn >= p.N || v == tc_num_shapes() - 1) {
-        best = v;
-        break;
-      }
+      if (bm != 128) continue;
+      best = v;
+      if (bn >= p.N) break;
     }
     if (best >= 0) {
       int bm, bn;

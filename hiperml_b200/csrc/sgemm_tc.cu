@@ -59,10 +59,14 @@ constexpr int kBK = 32;       // K per block (one 64-byte BF16 swizzle row)
 constexpr int kChunkK = 64;   // K accumulated in TMEM before an FP32 drain
 constexpr int kTmemCols = 512;
 
+// Tile shapes: 128-row tiles on one CTA, and 256-row tiles on a CTA pair
+// (tcgen05.mma.cta_group::2: one MMA spans both SMs of a cluster pair, each
+// SM holding its 128 rows of A and C in its TMEM and half of B).
 struct TcShape {
-  int bn;
+  int bm, bn;
 };
-constexpr TcShape kTcShapes[] = {{16}, {32}, {64}, {128}};
+constexpr TcShape kTcShapes[] = {{128, 16}, {128, 32}, {128, 64}, {128, 128},
+                                 {256, 32}, {256, 64}, {256, 128}};
 constexpr int kNumTcShapes = sizeof(kTcShapes) / sizeof(kTcShapes[0]);
 
 // Warp roles of one CTA:
@@ -145,6 +149,54 @@ __device__ __forceinline__ void mma_bf16_ts(uint32_t dtmem, uint32_t atmem, uint
       : "memory");
 }
 
+// The same on a CTA pair: issued by the pair's leader (cluster rank 0); A rows
+// 0..127 come from the leader's TMEM and 128..255 from the peer's (same
+// address), B columns 0..N/2-1 from the leader's shared memory and N/2..N-1
+// from the peer's (same address), and D rows likewise from each TMEM.
+__device__ __forceinline__ void mma_bf16_ts_pair(uint32_t dtmem, uint32_t atmem, uint64_t bdesc,
+                                                 uint32_t idesc, uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::2.kind::f16 [%0], [%1], %2, %3, p;\n\t}" ::"r"(dtmem),
+      "r"(atmem), "l"(bdesc), "r"(idesc), "r"(accumulate)
+      : "memory");
+}
+
+// Arrives on the mbarrier at this offset in both CTAs of the pair when the
+// pair's MMAs issued so far by this thread have completed.
+__device__ __forceinline__ void mma_commit_pair(uint64_t *bar) {
+  asm volatile(
+      "tcgen05.commit.cta_group::2.mbarrier::arrive::one.shared::cluster.multicast::cluster.b64 "
+      "[%0], %1;" ::"r"(smem_u32(bar)),
+      "h"(static_cast<uint16_t>(3))
+      : "memory");
+}
+
+__device__ __forceinline__ void tmem_alloc_pair(uint32_t *dst_smem, uint32_t ncols) {
+  asm volatile("tcgen05.alloc.cta_group::2.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                   smem_u32(dst_smem)),
+               "r"(ncols)
+               : "memory");
+  asm volatile("tcgen05.relinquish_alloc_permit.cta_group::2.sync.aligned;" ::: "memory");
+}
+
+__device__ __forceinline__ void tmem_dealloc_pair(uint32_t taddr, uint32_t ncols) {
+  asm volatile("tcgen05.dealloc.cta_group::2.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(ncols)
+               : "memory");
+}
+
+// Arrive on the mbarrier at the same offset in cluster rank 0 (release at
+// cluster scope: this thread's earlier writes, TMEM included after a
+// tcgen05.fence::before_thread_sync, are visible to a waiter there).
+__device__ __forceinline__ void mbar_arrive_rank0(uint64_t *bar) {
+  asm volatile(
+      "{\n\t.reg .b32 ra;\n\t"
+      "mapa.shared::cluster.u32 ra, %0, 0;\n\t"
+      "mbarrier.arrive.release.cluster.shared::cluster.b64 _, [ra];\n\t}" ::"r"(smem_u32(bar))
+      : "memory");
+}
+
 __device__ __forceinline__ void mma_commit(uint64_t *bar) {
   asm volatile(
       "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
@@ -199,10 +251,11 @@ __device__ __forceinline__ uint64_t sw64_desc(uint32_t saddr) {
          (static_cast<uint64_t>(4) << 61);
 }
 
-// Instruction descriptor: BF16 x BF16 -> F32, both K-major, M = 128, N = bn.
-__host__ __device__ constexpr uint32_t idesc_bf16(int bn) {
+// Instruction descriptor: BF16 x BF16 -> F32, both K-major, M = bm (128, or
+// 256 on a CTA pair), N = bn.
+__host__ __device__ constexpr uint32_t idesc_bf16(int bn, int bm = kBM) {
   return (1u << 4) | (1u << 7) | (1u << 10) | (static_cast<uint32_t>(bn >> 3) << 17) |
-         (static_cast<uint32_t>(kBM >> 4) << 24);
+         (static_cast<uint32_t>(bm >> 4) << 24);
 }
 
 // Split eight floats into NS BF16 planes, t0 = bf16(x), t1 = bf16(x - t0),
@@ -332,10 +385,17 @@ __host__ __device__ constexpr uint32_t tc_tmem_alloc_cols(int bn, int ns, int so
   return tc_pow2_cols(tc_issuers(bn, ns) * bn + so * tc_stage_cols(ns));
 }
 
-template <int BN, int NS, bool AK>
+// PAIR: the CTA is one of a cluster pair running 256-row tiles with
+// tcgen05.mma.cta_group::2.  Both CTAs load and convert their own 128 rows of
+// A and their own half of B (BN/2 rows of each plane) and drain their own
+// rows of C; only the leader (rank 0) issues MMAs, for both.  The peer's
+// converters, B loader and drain warps arrive on the leader's barriers
+// (remote arrives); the leader's commits arrive on both CTAs' barriers.
+template <int BN, int NS, bool AK, bool PAIR>
 __global__ void __launch_bounds__(tc_warps(BN, NS) * 32, 1)
     tc_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
               TcArgs args) {
+  static_assert(!PAIR || BN >= 32, "a CTA pair holds BN/2 >= 16 rows of B each");
   constexpr int G = tc_groups();
   constexpr int D = tc_drain_groups(BN);
   constexpr int DC = BN / D;                                 // columns per drain thread
@@ -343,10 +403,11 @@ __global__ void __launch_bounds__(tc_warps(BN, NS) * 32, 1)
   constexpr int kThreads = tc_warps(BN, NS) * 32;
   constexpr int kConvWarp0 = tc_conv_warp0(BN, NS), kDrainWarp0 = kConvWarp0 + 4 * G;
   constexpr int A32_BYTES = static_cast<int>(tc_a_bytes());  // FP32 A slot (16 KB)
-  constexpr int BPL_BYTES = BN * kBK * 2;                    // one B plane tile
+  constexpr int BROWS = PAIR ? BN / 2 : BN;                 // B rows of a plane in this CTA
+  constexpr int BPL_BYTES = BROWS * kBK * 2;                 // one B plane tile
   constexpr int BSLOT = NS * BPL_BYTES;                      // one B slot
   constexpr int SC = tc_stage_cols(NS);                      // TMEM columns of an A stage
-  constexpr uint32_t IDESC = idesc_bf16(BN);
+  constexpr uint32_t IDESC = idesc_bf16(BN, PAIR ? 2 * kBM : kBM);
   constexpr int P = kChunkK / kBK;                           // blocks per TMEM chunk
 
   extern __shared__ uint8_t smem_raw[];
@@ -369,6 +430,8 @@ __global__ void __launch_bounds__(tc_warps(BN, NS) * 32, 1)
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int split = args.split;
   const int rank = split > 1 ? static_cast<int>(cluster_ctarank()) : 0;
+  const int prank = PAIR ? static_cast<int>(cluster_ctarank()) : 0;  // 0 or 1 in a pair
+  const bool leader = prank == 0;
   const int64_t m0 = static_cast<int64_t>(blockIdx.x / split) * kBM;
   const int n0 = blockIdx.y * BN;
   const int kbeg = rank * args.kc;
@@ -383,20 +446,30 @@ __global__ void __launch_bounds__(tc_warps(BN, NS) * 32, 1)
       mbar_init(&aempty[s], 4);
     }
     for (int o = 0; o < SO; ++o) {
-      mbar_init(&opfull[o], 4 + 1);  // the converter group's warps + the B loader
+      // the converter group's warps + the B loader (both CTAs' on a pair's
+      // leader; on the peer, only its B loader's own TMA completion)
+      mbar_init(&opfull[o], PAIR ? (leader ? 2 * (4 + 1) : 1) : 4 + 1);
       mbar_init(&opempty[o], 1);
     }
     for (int b = 0; b < NI; ++b) {
       mbar_init(&accfull[b], 1);
-      mbar_init(&accempty[b], 4 * D);
+      mbar_init(&accempty[b], PAIR ? 2 * 4 * D : 4 * D);
     }
     mbar_init(mmadone, NI);  // one commit per MMA issuer
     *bad_flag = 0;
     fence_mbar_init();
   }
-  if (warp == 2) tmem_alloc(tmem_slot, tmem_cols);
+  if (warp == 2) {
+    if (PAIR)
+      tmem_alloc_pair(tmem_slot, tmem_cols);
+    else
+      tmem_alloc(tmem_slot, tmem_cols);
+  }
   tc_fence_before();
-  __syncthreads();
+  if (PAIR)
+    cluster_sync();  // both CTAs' barriers are initialised before any remote arrive
+  else
+    __syncthreads();
   tc_fence_after();
   const uint32_t tmem = *tmem_slot;
   const uint32_t tacc = tmem;           // accumulator b: columns b*BN .. +BN-1
@@ -436,7 +509,8 @@ __global__ void __launch_bounds__(tc_warps(BN, NS) * 32, 1)
         mbar_arrive_expect_tx(&opfull[o], BSLOT);
 #pragma unroll
         for (int i = 0; i < NS; ++i)
-          tma_load_2d(dst + i * BPL_BYTES, &tmB, &opfull[o], k0, i * args.n_pad + n0);
+          tma_load_2d(dst + i * BPL_BYTES, &tmB, &opfull[o], k0,
+                      i * args.n_pad + n0 + prank * BROWS);
       }
     }
   } else if (warp >= 2 && warp < 2 + NI) {
@@ -444,12 +518,16 @@ __global__ void __launch_bounds__(tc_warps(BN, NS) * 32, 1)
     // NI issuing threads, one per accumulator: issuer b takes the chunks
     // q = b, b+NI, ...  A commit tracks only the MMAs of the thread that
     // issues it.
-    if (lane == 0) {
+    if (lane == 0 && leader) {
       const int b = warp - 2;
       const uint32_t dacc = tacc + static_cast<uint32_t>(b * BN);
       bool ok = true;
       for (int q = b; q < nchunks && ok; q += NI) {
-        if (!mbar_wait(&accempty[b], ((q / NI) & 1) ^ 1, args.err, kDevErrEmptyBarrier)) {
+        const bool w = PAIR ? mbar_wait_cluster(&accempty[b], ((q / NI) & 1) ^ 1, args.err,
+                                                kDevErrEmptyBarrier)
+                            : mbar_wait(&accempty[b], ((q / NI) & 1) ^ 1, args.err,
+                                        kDevErrEmptyBarrier);
+        if (!w) {
           ok = false;
           break;
         }
@@ -457,7 +535,10 @@ __global__ void __launch_bounds__(tc_warps(BN, NS) * 32, 1)
         for (int kb = q * P; kb < kb1; ++kb) {
           const int o = kb % SO;
           const bool first = kb == q * P;
-          if (!mbar_wait(&opfull[o], (kb / SO) & 1, args.err, kDevErrFullBarrier)) {
+          const bool w = PAIR ? mbar_wait_cluster(&opfull[o], (kb / SO) & 1, args.err,
+                                                  kDevErrFullBarrier)
+                              : mbar_wait(&opfull[o], (kb / SO) & 1, args.err, kDevErrFullBarrier);
+          if (!w) {
             ok = false;
             break;
           }
@@ -476,15 +557,42 @@ __global__ void __launch_bounds__(tc_warps(BN, NS) * 32, 1)
                 const uint64_t bd =
                     b_desc + static_cast<uint64_t>((j * BPL_BYTES + kk * 32) >> 4);
                 const uint32_t acc = (!first || kk > 0 || i > 0 || j > 0) ? 1u : 0u;
-                mma_bf16_ts(dacc, at, bd, IDESC, acc);
+                if (PAIR)
+                  mma_bf16_ts_pair(dacc, at, bd, IDESC, acc);
+                else
+                  mma_bf16_ts(dacc, at, bd, IDESC, acc);
               }
           }
-          mma_commit(&opempty[o]);
+          if (PAIR)
+            mma_commit_pair(&opempty[o]);
+          else
+            mma_commit(&opempty[o]);
         }
-        if (ok) mma_commit(&accfull[b]);
+        if (ok) {
+          if (PAIR)
+            mma_commit_pair(&accfull[b]);
+          else
+            mma_commit(&accfull[b]);
+        }
       }
       if (!ok) *bad_flag = 1;
-      mma_commit(mmadone);  // tracks every MMA this thread issued
+      // tracks every MMA this thread issued
+      if (PAIR)
+        mma_commit_pair(mmadone);
+      else
+        mma_commit(mmadone);
+    } else if (PAIR && !leader && warp == 3 && lane == 0) {
+      // the peer's B relay: each time a B slot of this CTA has landed (its
+      // own opfull completes on the TMA bytes), arrive on the leader's.  In
+      // a thread of its own so the B loader keeps several loads in flight.
+      for (int kb = 0; kb < nkb; ++kb) {
+        const int o = kb % SO;
+        if (!mbar_wait(&opfull[o], (kb / SO) & 1, args.err, kDevErrFullBarrier)) {
+          *bad_flag = 1;
+          break;
+        }
+        mbar_arrive_rank0(&opfull[o]);
+      }
     }
   } else if (warp >= kConvWarp0 && warp < kDrainWarp0) {
     // ------------------------------------------ converters (G groups)
@@ -537,7 +645,12 @@ __global__ void __launch_bounds__(tc_warps(BN, NS) * 32, 1)
       tmem_wait_st();
       tc_fence_before();
       __syncwarp();
-      if (lane == 0) mbar_arrive(&opfull[o]);
+      if (lane == 0) {
+        if (PAIR && !leader)
+          mbar_arrive_rank0(&opfull[o]);
+        else
+          mbar_arrive(&opfull[o]);
+      }
     }
   } else if (warp >= kDrainWarp0) {
     // ------------------------------------------ drain (D groups)
@@ -574,7 +687,12 @@ __global__ void __launch_bounds__(tc_warps(BN, NS) * 32, 1)
       }
       tc_fence_before();
       __syncwarp();
-      if (lane == 0) mbar_arrive(&accempty[b]);
+      if (lane == 0) {
+        if (PAIR && !leader)
+          mbar_arrive_rank0(&accempty[b]);
+        else
+          mbar_arrive(&accempty[b]);
+      }
     }
     // ---------------------------------------------------- epilogue
     // (the running sums stay in this branch's registers; the barrier is the
@@ -633,14 +751,22 @@ __global__ void __launch_bounds__(tc_warps(BN, NS) * 32, 1)
   tc_fence_before();
   __syncthreads();
   if (warp == 2) {
-    // the TMEM is freed only once every issued MMA has completed
+    // the TMEM is freed only once every issued MMA has completed (on a pair,
+    // the leader's commits arrive on both CTAs' mmadone)
     bool w = true;
     if (lane == 0) w = mbar_wait(mmadone, 0, args.err, kDevErrMmaBarrier);
     __syncwarp();
     (void)w;
     tc_fence_after();
-    tmem_dealloc(tmem, tmem_cols);
   }
+  if (PAIR) cluster_sync();  // neither CTA leaves while the other may arrive on it
+  if (warp == 2) {
+    if (PAIR)
+      tmem_dealloc_pair(tmem, tmem_cols);
+    else
+      tmem_dealloc(tmem, tmem_cols);
+  }
+  if (PAIR) cluster_sync();
 }
 
 }  // namespace
@@ -657,6 +783,9 @@ template <int BN, int NS, bool AK>
 hml_status launch_tc_planes(const GemmProblem &p, const hml_sgemm_config &c,
                             const __nv_bfloat16 *planes, int k_pad, int n_pad, int *err,
                             cudaStream_t s) {
+  // a 256-row configuration runs on CTA pairs (clusters of two)
+  const bool pair = c.tile_m == 2 * kBM;
+  if (pair && (BN < 32 || c.split_k != 1)) return HML_STATUS_INVALID_VALUE;
   CUtensorMap ta, tb;
   memset(&ta, 0, sizeof ta);
   memset(&tb, 0, sizeof tb);
@@ -669,8 +798,8 @@ hml_status launch_tc_planes(const GemmProblem &p, const hml_sgemm_config &c,
                        CU_TENSOR_MAP_SWIZZLE_NONE);
   if (ok)
     ok = tensor_map_2d(&tb, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, planes, k_pad,
-                       static_cast<uint64_t>(NS) * n_pad, static_cast<uint64_t>(k_pad) * 2, kBK, BN,
-                       CU_TENSOR_MAP_SWIZZLE_64B);
+                       static_cast<uint64_t>(NS) * n_pad, static_cast<uint64_t>(k_pad) * 2, kBK,
+                       pair ? BN / 2 : BN, CU_TENSOR_MAP_SWIZZLE_64B);
   if (!ok) return HML_STATUS_CUDA_ERROR;
   TcArgs args;
   args.p = p;
@@ -684,7 +813,10 @@ hml_status launch_tc_planes(const GemmProblem &p, const hml_sgemm_config &c,
   args.n_pad = n_pad;
   args.err = err;
   const size_t smem = tc_plan_bytes(BN, NS, plan);
-  auto kern = tc_kernel<BN, NS, AK>;
+  void (*kern)(CUtensorMap, CUtensorMap, TcArgs) = tc_kernel<BN, NS, AK, false>;
+  if constexpr (BN >= 32) {
+    if (pair) kern = tc_kernel<BN, NS, AK, true>;
+  }
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        static_cast<int>(smem));
   if (e == cudaSuccess && c.split_k > 8)
@@ -693,11 +825,13 @@ hml_status launch_tc_planes(const GemmProblem &p, const hml_sgemm_config &c,
     note_cuda_error(e, "tc attributes");
     return HML_STATUS_CUDA_ERROR;
   }
-  const int64_t tiles_m = (static_cast<int64_t>(p.M) + kBM - 1) / kBM;
+  int64_t tiles_m = (static_cast<int64_t>(p.M) + kBM - 1) / kBM;
+  if (pair) tiles_m = (tiles_m + 1) / 2 * 2;  // whole pairs; rows past M are not stored
   const int64_t tiles_n = n_pad / BN;
   if (tiles_m * c.split_k > 0x7fffffff || tiles_n > 65535) return HML_STATUS_NOT_SUPPORTED;
   dim3 grid(static_cast<unsigned>(tiles_m * c.split_k), static_cast<unsigned>(tiles_n));
-  e = launch_k(kern, grid, dim3(tc_warps(BN, NS) * 32), smem, s, c.split_k, ta, tb, args);
+  e = launch_k(kern, grid, dim3(tc_warps(BN, NS) * 32), smem, s, pair ? 2 : c.split_k, ta, tb,
+               args);
   note_cuda_error(e, "tc launch");
   return cuda_status(e);
 }
@@ -755,14 +889,17 @@ bool aligned16(const void *ptr) { return (reinterpret_cast<uintptr_t>(ptr) & 15u
 
 int tc_num_shapes() { return kNumTcShapes; }
 void tc_shape(int v, int *bm, int *bn) {
-  *bm = kBM;
+  *bm = kTcShapes[v].bm;
   *bn = kTcShapes[v].bn;
 }
 
 hml_status check_tc(const GemmProblem &p, const hml_sgemm_config &c) {
   if (c.algo != HML_ALGO_BF16X3 && c.algo != HML_ALGO_BF16X6) return HML_STATUS_INVALID_VALUE;
   if (c.variant < 0 || c.variant >= kNumTcShapes) return HML_STATUS_INVALID_VALUE;
-  if (c.tile_m != kBM || c.tile_n != kTcShapes[c.variant].bn) return HML_STATUS_INVALID_VALUE;
+  if (c.tile_m != kTcShapes[c.variant].bm || c.tile_n != kTcShapes[c.variant].bn)
+    return HML_STATUS_INVALID_VALUE;
+  // a CTA pair is one cluster: no cluster split-K on top of it
+  if (c.tile_m == 2 * kBM && c.split_k != 1) return HML_STATUS_INVALID_VALUE;
   if (c.split_k < 1 || c.split_k > 16 || (c.split_k & (c.split_k - 1)) != 0)
     return HML_STATUS_INVALID_VALUE;
   if (c.stages < 2 || c.stages > 8) return HML_STATUS_INVALID_VALUE;
