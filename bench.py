@@ -678,12 +678,15 @@ def run_batched(args):
     dom_s = per_launch_ms * 1e-3
     roof = {"bound": "hbm", "achieved": alg_bytes / dom_s / 1e9, "peak": pk["hbm_gbs"],
             "unit": "GB/s", "frac": alg_bytes / dom_s / 1e9 / pk["hbm_gbs"],
-            "traffic": traffic_table().get("batched"), "kernel": "batched_kernel",
+            "traffic": traffic_table().get("batched"),
+            "kernel": "batch plan (tc_batch_kernel<32|64|128> + batched_kernel + split_b_batch_kernel)",
             "alg_bytes_per_launch": alg_bytes, "alg_flops_per_launch": step_flops,
             "ms_per_launch": per_launch_ms, "peak_source": pk["source"],
             "simt_fp32_tflops": step_flops / dom_s / 1e12,
             "simt_fp32_peak_nominal": 148 * 128 * 2 * 1.965e-3,
-            "note": "mixed batch: HBM-bound (small N) and FP32-bound (large N) tiles"}
+            "note": ("one graph launch of the whole plan: BF16X6 tensor-core tiles for N > 8 "
+                     "(tc_batch_kernel<128,3> dominates) and FP32 SIMT tiles for N <= 8; "
+                     "achieved = the plan's algorithmic bytes over its event-timed duration")}
 
     cpu = None
     if not args.no_cpu_baseline and rank == 0 and world == 1:
