@@ -110,6 +110,14 @@ std::vector<hml_sgemm_config> build_space() {
         v.push_back(c);
       }
   }
+  // the stream-K kernel for N <= 16 (variants after the tiled shapes)
+  for (int i = 0; i < stream_num_variants(); ++i) {
+    const int nb = stream_tile_n(i), top = stream_max_stages(nb);
+    for (int stages : {top - 2, top - 1, top}) {
+      hml_sgemm_config c = {HML_ALGO_SIMT, 128, nb, 1, stages, simt_num_shapes() + i};
+      v.push_back(c);
+    }
+  }
   for (int algo : {HML_ALGO_BF16X3, HML_ALGO_BF16X6})
     for (int var = 0; var < tc_num_shapes(); ++var) {
       int bm, bn;

@@ -13,11 +13,13 @@
 //             scheduling.
 //  gemv_cols  A(p,q) columns contiguous (sp == 1): column-major y = A x.
 //             Each lane owns 4 consecutive rows (one 16-byte load per
-//             column), the 8 warps of a CTA take interleaved columns, and
-//             `split` CTAs of one thread-block cluster take disjoint column
-//             ranges.  Partial sums are combined in a fixed order through
-//             shared memory and then distributed shared memory, so results
-//             are deterministic and no global workspace is used.
+//             column), the 8 warps of a CTA take 2 row groups x 4
+//             interleaved column phases, and `split` CTAs take disjoint
+//             column ranges of the same 256 rows.  Partial sums are combined
+//             in a fixed order: the phases in shared memory, the split CTAs
+//             through a per-stream workspace, summed in rank order by
+//             whichever CTA of the tile finishes last (a per-tile arrival
+//             counter, reset by that CTA), so results are deterministic.
 #include <algorithm>
 
 #include "hml_device.cuh"
@@ -104,66 +106,72 @@ __global__ void __launch_bounds__(kThreads) gemv_rows_kernel(GemvProblem p) {
 }
 
 // ----------------------------------------------------------------- cols
-// VEC: lane owns rows base + 4*lane .. +3 (16-byte loads); else rows
-// base + lane + 32*j for j < 4.  Either way a warp covers 128 rows.
+// A CTA covers kColRows = 256 rows: warp w takes row group w & 1 (128 rows)
+// and column phase w >> 1 (columns qbeg + phase, + 4, + 8, ...).  VEC: lane
+// owns rows group_base + 4*lane .. +3 (16-byte loads); else rows
+// group_base + lane + 32*j for j < 4.  Eight columns are loaded before any
+// is used, and registers are capped at 32 so that 8 CTAs fit on an SM
+// (measured on B200, 32768 x 4096, split 8: 6.6 TB/s; with 48 registers and
+// 5 CTAs per SM 6.1 TB/s; the earlier 128-row CTAs with 4 loads in flight
+// reduced through cluster shared memory 5.3 TB/s).
+constexpr int kColRows = 256;
+constexpr int kColPhases = kThreads / 32 / 2;
+constexpr int kColUnroll = 8;
+constexpr int kMaxColSplit = 16;
+static_assert(kColRows == kThreads, "thread i finalises row i of the tile");
+
 template <bool VEC>
-__global__ void __launch_bounds__(kThreads) gemv_cols_kernel(GemvProblem p, int split) {
-  constexpr int kRows = 128;
-  __shared__ float4 part[kThreads / 32][kRows / 4];
-  __shared__ float sum[kRows];
+__global__ void __launch_bounds__(kThreads, 8) gemv_cols_kernel(GemvProblem p, int split,
+                                                             float *partial, unsigned *arrivals) {
+  __shared__ float4 part[kThreads / 32][32];
+  __shared__ float sum[kColRows];
+  __shared__ unsigned last;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int rank = split > 1 ? static_cast<int>(cluster_ctarank()) : 0;
+  const int group = warp & 1, phase = warp >> 1;
+  const int rank = static_cast<int>(blockIdx.x % split);
   const int64_t tile = blockIdx.x / split;
-  const int64_t row0 = tile * kRows;
+  const int64_t row0 = tile * kColRows;
+  const int64_t gbase = row0 + group * 128;
   const int qc = (p.Q + split - 1) / split;
   const int qbeg = rank * qc;
   const int qend = min(p.Q, qbeg + qc);
+  constexpr int S = kColPhases;  // column stride of one warp
 
   float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
-  const int64_t myrow = VEC ? row0 + 4 * lane : row0 + lane;
-  const bool full = VEC ? (myrow + 3 < p.P) : (row0 + kRows <= p.P);
+  const int64_t myrow = VEC ? gbase + 4 * lane : gbase + lane;
+  const bool full = VEC ? (myrow + 3 < p.P) : (gbase + 128 <= p.P);
   if (full) {
     const float *a = p.A + myrow;
     float4 acc1 = make_float4(0.f, 0.f, 0.f, 0.f);
-    int q = qbeg + warp;
-    for (; q + 3 * 8 < qend; q += 4 * 8) {
-      float4 v0, v1, v2, v3;
-      if (VEC) {
-        v0 = ldg_stream4(a + static_cast<int64_t>(q) * p.sq);
-        v1 = ldg_stream4(a + static_cast<int64_t>(q + 8) * p.sq);
-        v2 = ldg_stream4(a + static_cast<int64_t>(q + 16) * p.sq);
-        v3 = ldg_stream4(a + static_cast<int64_t>(q + 24) * p.sq);
-      } else {
-        const float *c0 = a + static_cast<int64_t>(q) * p.sq;
-        const float *c1 = a + static_cast<int64_t>(q + 8) * p.sq;
-        const float *c2 = a + static_cast<int64_t>(q + 16) * p.sq;
-        const float *c3 = a + static_cast<int64_t>(q + 24) * p.sq;
-        v0 = make_float4(ldg_stream(c0), ldg_stream(c0 + 32), ldg_stream(c0 + 64), ldg_stream(c0 + 96));
-        v1 = make_float4(ldg_stream(c1), ldg_stream(c1 + 32), ldg_stream(c1 + 64), ldg_stream(c1 + 96));
-        v2 = make_float4(ldg_stream(c2), ldg_stream(c2 + 32), ldg_stream(c2 + 64), ldg_stream(c2 + 96));
-        v3 = make_float4(ldg_stream(c3), ldg_stream(c3 + 32), ldg_stream(c3 + 64), ldg_stream(c3 + 96));
+    int q = qbeg + phase;
+    const int64_t astep = static_cast<int64_t>(S) * p.sq, xstep = static_cast<int64_t>(S) * p.incx;
+    const float *ac = a + static_cast<int64_t>(q) * p.sq;
+    const float *xc = p.x + static_cast<int64_t>(q) * p.incx;
+    for (; q + (kColUnroll - 1) * S < qend;
+         q += kColUnroll * S, ac += kColUnroll * astep, xc += kColUnroll * xstep) {
+      float4 v[kColUnroll];
+#pragma unroll
+      for (int u = 0; u < kColUnroll; ++u) {
+        const float *c = ac + u * astep;
+        v[u] = VEC ? ldg_stream4(c)
+                   : make_float4(ldg_stream(c), ldg_stream(c + 32), ldg_stream(c + 64),
+                                 ldg_stream(c + 96));
       }
-      const float x0 = __ldg(p.x + static_cast<int64_t>(q) * p.incx);
-      const float x1 = __ldg(p.x + static_cast<int64_t>(q + 8) * p.incx);
-      const float x2 = __ldg(p.x + static_cast<int64_t>(q + 16) * p.incx);
-      const float x3 = __ldg(p.x + static_cast<int64_t>(q + 24) * p.incx);
-      acc.x = fmaf(v0.x, x0, acc.x); acc.y = fmaf(v0.y, x0, acc.y);
-      acc.z = fmaf(v0.z, x0, acc.z); acc.w = fmaf(v0.w, x0, acc.w);
-      acc1.x = fmaf(v1.x, x1, acc1.x); acc1.y = fmaf(v1.y, x1, acc1.y);
-      acc1.z = fmaf(v1.z, x1, acc1.z); acc1.w = fmaf(v1.w, x1, acc1.w);
-      acc.x = fmaf(v2.x, x2, acc.x); acc.y = fmaf(v2.y, x2, acc.y);
-      acc.z = fmaf(v2.z, x2, acc.z); acc.w = fmaf(v2.w, x2, acc.w);
-      acc1.x = fmaf(v3.x, x3, acc1.x); acc1.y = fmaf(v3.y, x3, acc1.y);
-      acc1.z = fmaf(v3.z, x3, acc1.z); acc1.w = fmaf(v3.w, x3, acc1.w);
+#pragma unroll
+      for (int u = 0; u < kColUnroll; u += 2) {
+        const float x0 = __ldg(xc + u * xstep);
+        const float x1 = __ldg(xc + (u + 1) * xstep);
+        acc.x = fmaf(v[u].x, x0, acc.x); acc.y = fmaf(v[u].y, x0, acc.y);
+        acc.z = fmaf(v[u].z, x0, acc.z); acc.w = fmaf(v[u].w, x0, acc.w);
+        acc1.x = fmaf(v[u + 1].x, x1, acc1.x); acc1.y = fmaf(v[u + 1].y, x1, acc1.y);
+        acc1.z = fmaf(v[u + 1].z, x1, acc1.z); acc1.w = fmaf(v[u + 1].w, x1, acc1.w);
+      }
     }
-    for (; q < qend; q += 8) {
-      float4 v;
-      if (VEC) {
-        v = ldg_stream4(a + static_cast<int64_t>(q) * p.sq);
-      } else {
-        const float *c0 = a + static_cast<int64_t>(q) * p.sq;
-        v = make_float4(ldg_stream(c0), ldg_stream(c0 + 32), ldg_stream(c0 + 64), ldg_stream(c0 + 96));
-      }
+    for (; q < qend; q += S) {
+      const float *c = a + static_cast<int64_t>(q) * p.sq;
+      const float4 v = VEC ? ldg_stream4(c)
+                           : make_float4(ldg_stream(c), ldg_stream(c + 32), ldg_stream(c + 64),
+                                         ldg_stream(c + 96));
       const float xv = __ldg(p.x + static_cast<int64_t>(q) * p.incx);
       acc.x = fmaf(v.x, xv, acc.x); acc.y = fmaf(v.y, xv, acc.y);
       acc.z = fmaf(v.z, xv, acc.z); acc.w = fmaf(v.w, xv, acc.w);
@@ -172,7 +180,7 @@ __global__ void __launch_bounds__(kThreads) gemv_cols_kernel(GemvProblem p, int 
   } else {
     // ragged last tile: element-wise with bounds checks
     float v[4] = {0.f, 0.f, 0.f, 0.f};
-    for (int q = qbeg + warp; q < qend; q += 8) {
+    for (int q = qbeg + phase; q < qend; q += S) {
       const float xv = __ldg(p.x + static_cast<int64_t>(q) * p.incx);
       const float *col = p.A + static_cast<int64_t>(q) * p.sq;
 #pragma unroll
@@ -183,50 +191,47 @@ __global__ void __launch_bounds__(kThreads) gemv_cols_kernel(GemvProblem p, int 
     }
     acc = make_float4(v[0], v[1], v[2], v[3]);
   }
-  // combine the 8 warps: part[w][lane] holds this lane's 4 rows
+  // combine the column phases: part[w][lane] holds this lane's 4 rows
   part[warp][lane] = acc;
   __syncthreads();
-  if (threadIdx.x < kRows) {
-    // thread i sums row slot i over warps in order 0..7
-    const int slot_lane = VEC ? threadIdx.x >> 2 : threadIdx.x & 31;
-    const int comp = VEC ? threadIdx.x & 3 : threadIdx.x >> 5;
+  {
+    // thread i owns row offset i of the tile: group i / 128, and within the
+    // group the lane slot / component that holds it; phases summed in order
+    const int i = static_cast<int>(threadIdx.x);
+    const int g = i >> 7, r = i & 127;
+    const int slot_lane = VEC ? r >> 2 : r & 31;
+    const int comp = VEC ? r & 3 : r >> 5;
     float s = 0.0f;
 #pragma unroll
-    for (int w = 0; w < kThreads / 32; ++w) {
-      const float4 v = part[w][slot_lane];
+    for (int ph = 0; ph < kColPhases; ++ph) {
+      const float4 v = part[2 * ph + g][slot_lane];
       s += comp == 0 ? v.x : comp == 1 ? v.y : comp == 2 ? v.z : v.w;
     }
-    // both lane-to-row maps give row offset == threadIdx.x for this slot
-    sum[threadIdx.x] = s;
+    sum[i] = s;
   }
+  const int64_t rr = row0 + threadIdx.x;
   if (split > 1) {
-    cluster_sync();
-    // rank r finalises rows [r*len, (r+1)*len) of the tile, summing the
-    // partials of ranks 0..split-1 in order
-    const int len = (kRows + split - 1) / split;
-    const int i = static_cast<int>(threadIdx.x);
-    if (i < len) {
-      const int roff = rank * len + i;
-      if (roff < kRows) {
-        const uint32_t base = smem_u32(&sum[roff]);
-        float s = 0.0f;
-        for (int r = 0; r < split; ++r) s += ld_dsmem(mapa_shared(base, r));
-        const int64_t rr = row0 + roff;
-        if (rr < p.P) {
-          float *y = p.y + rr * p.incy;
-          *y = axpby(p.alpha, s, p.beta, y);
-        }
-      }
+    // publish this CTA's partial; the tile's last CTA to arrive sums the
+    // split partials in rank order
+    if (rr < p.P) __stcg(partial + static_cast<int64_t>(rank) * p.P + rr, sum[threadIdx.x]);
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) last = atomicAdd(&arrivals[tile], 1u) == static_cast<unsigned>(split - 1);
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    if (rr < p.P) {
+      float s = 0.0f;
+      for (int r = 0; r < split; ++r) s += __ldcg(partial + static_cast<int64_t>(r) * p.P + rr);
+      float *y = p.y + rr * p.incy;
+      *y = axpby(p.alpha, s, p.beta, y);
     }
-    cluster_sync();
+    if (threadIdx.x == 0) arrivals[tile] = 0u;  // ready for the next call
   } else {
     __syncthreads();
-    if (threadIdx.x < kRows) {
-      const int64_t rr = row0 + threadIdx.x;
-      if (rr < p.P) {
-        float *y = p.y + rr * p.incy;
-        *y = axpby(p.alpha, sum[threadIdx.x], p.beta, y);
-      }
+    if (rr < p.P) {
+      float *y = p.y + rr * p.incy;
+      *y = axpby(p.alpha, sum[threadIdx.x], p.beta, y);
     }
   }
 }
@@ -261,7 +266,8 @@ bool aligned16(const void *ptr) { return (reinterpret_cast<uintptr_t>(ptr) & 15u
 }  // namespace
 
 // variant for the row kernel: threads per row (4..256), 0 = heuristic.
-// variant for the column kernel: cluster split (1..8), 0 = heuristic.
+// variant for the column kernel: CTAs per 256-row tile along the columns
+// (1..16), 0 = heuristic.
 hml_status launch_gemv(const GemvProblem &p, int variant, cudaStream_t s) {
   if (p.P == 0) return HML_STATUS_SUCCESS;
   if (p.sq != 1 && p.sp != 1) return HML_STATUS_NOT_SUPPORTED;
@@ -290,20 +296,43 @@ hml_status launch_gemv(const GemvProblem &p, int variant, cudaStream_t s) {
   }
   // columns contiguous
   const bool vec = aligned16(p.A) && (p.sq % 4 == 0 || p.Q == 1);
-  const int64_t tiles = (static_cast<int64_t>(p.P) + 127) / 128;
+  const int64_t tiles = (static_cast<int64_t>(p.P) + kColRows - 1) / kColRows;
   int split = variant;
   if (split == 0) {
-    // aim for >= 4 CTAs per SM, each with >= 64 columns
-    const int64_t want = 4 * static_cast<int64_t>(sm_count());
-    split = static_cast<int>((want + tiles - 1) / tiles);
-    split = max(1, min(split, 8));
+    // as many CTAs as fit on the GPU at once, in one wave (measured on B200,
+    // 32768 x 4096: 8 CTAs per SM resident, split 8 = 1024 CTAs 6.6 TB/s;
+    // a second partial wave costs up to a third of that), each with >= 64
+    // columns
+    static const int per_sm = [] {
+      int n = 0;
+      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, gemv_cols_kernel<true>, kThreads, 0) !=
+              cudaSuccess ||
+          n < 1)
+        n = 1;
+      return n;
+    }();
+    const int64_t resident = static_cast<int64_t>(per_sm) * sm_count();
+    split = static_cast<int>(resident / tiles);
+    split = max(1, min(split, kMaxColSplit));
     while (split > 1 && p.Q / split < 64) --split;
   }
-  if (split < 1 || split > 8) return HML_STATUS_INVALID_VALUE;
+  if (split < 1 || split > kMaxColSplit) return HML_STATUS_INVALID_VALUE;
   if (tiles * split > 0x7fffffff) return HML_STATUS_NOT_SUPPORTED;
+  float *partial = nullptr;
+  unsigned *arrivals = nullptr;
+  if (split > 1) {
+    void *ws = nullptr;
+    hml_status st = workspace(static_cast<size_t>(split) * p.P * sizeof(float), s, &ws);
+    if (st != HML_STATUS_SUCCESS) return st;
+    st = tile_counters(static_cast<size_t>(tiles), s, &arrivals);
+    if (st != HML_STATUS_SUCCESS) return st;
+    partial = static_cast<float *>(ws);
+  }
   const dim3 grid(static_cast<unsigned>(tiles * split));
-  cudaError_t e = vec ? launch_k(gemv_cols_kernel<true>, grid, dim3(kThreads), 0, s, split, p, split)
-                      : launch_k(gemv_cols_kernel<false>, grid, dim3(kThreads), 0, s, split, p, split);
+  cudaError_t e = vec ? launch_k(gemv_cols_kernel<true>, grid, dim3(kThreads), 0, s, 1, p, split,
+                                 partial, arrivals)
+                      : launch_k(gemv_cols_kernel<false>, grid, dim3(kThreads), 0, s, 1, p, split,
+                                 partial, arrivals);
   note_cuda_error(e, "gemv_cols");
   return cuda_status(e);
 }

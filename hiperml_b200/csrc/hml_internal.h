@@ -57,6 +57,14 @@ hml_status launch_scale(float *C, int M, int N, int64_t scm, int64_t scn, float 
 hml_status launch_simt(const GemmProblem &p, const hml_sgemm_config &c, cudaStream_t s);
 hml_status launch_tc(const GemmProblem &p, const hml_sgemm_config &c, cudaStream_t s);
 hml_status check_simt(const GemmProblem &p, const hml_sgemm_config &c);
+// The stream-K SIMT kernel for N <= 16 with contiguous columns of A
+// (sgemm_stream.cu); reached through the SIMT family's variants
+// simt_num_shapes() .. simt_num_shapes() + stream_num_variants() - 1.
+int stream_num_variants();
+int stream_tile_n(int i);
+int stream_max_stages(int nb);  // deepest ring that fits
+hml_status check_stream(const GemmProblem &p, const hml_sgemm_config &c);
+hml_status launch_stream(const GemmProblem &p, const hml_sgemm_config &c, cudaStream_t s);
 hml_status check_tc(const GemmProblem &p, const hml_sgemm_config &c);
 
 // The split-BF16 part of a batched plan (sgemm_tc.cu): problems that
@@ -77,6 +85,9 @@ int tc_batch_ctas(const TcBatch *b);
 // Per-device resources.
 int *device_error_word();  // nullptr on failure
 hml_status workspace(size_t bytes, cudaStream_t s, void **ptr);
+// n zero-initialised counters private to (device, stream).  Kernels that use
+// them leave every counter at zero again when they finish.
+hml_status tile_counters(size_t n, cudaStream_t s, unsigned **ptr);
 
 // Tensor maps.
 bool tensor_map_2d(CUtensorMap *map, CUtensorMapDataType dtype, const void *base,

@@ -21,6 +21,7 @@ struct Ws {
   size_t bytes = 0;
 };
 std::map<std::pair<int, cudaStream_t>, Ws> g_ws;
+std::map<std::pair<int, cudaStream_t>, Ws> g_counters;
 std::map<int, int> g_sms;
 thread_local std::string t_last_error;
 
@@ -141,12 +142,42 @@ bool tensor_map_2d(CUtensorMap *map, CUtensorMapDataType dtype, const void *base
   return true;
 }
 
+hml_status tile_counters(size_t n, cudaStream_t s, unsigned **ptr) {
+  const int d = current_device();
+  std::lock_guard<std::mutex> lk(g_mu);
+  Ws &w = g_counters[std::make_pair(d, s)];
+  const size_t bytes = n * sizeof(unsigned);
+  if (w.bytes < bytes) {
+    if (w.ptr) {
+      cudaStreamSynchronize(s);
+      cudaFree(w.ptr);
+      w.ptr = nullptr;
+      w.bytes = 0;
+    }
+    size_t want = bytes < 65536 ? 65536 : bytes;
+    cudaError_t e = cudaMalloc(&w.ptr, want);
+    if (e == cudaSuccess) e = cudaMemsetAsync(w.ptr, 0, want, s);
+    if (e != cudaSuccess) {
+      note_cuda_error(e, "tile counters");
+      if (w.ptr) cudaFree(w.ptr);
+      w.ptr = nullptr;
+      return HML_STATUS_ALLOC_FAILED;
+    }
+    w.bytes = want;
+  }
+  *ptr = static_cast<unsigned *>(w.ptr);
+  return HML_STATUS_SUCCESS;
+}
+
 hml_status release_all() {
   std::lock_guard<std::mutex> lk(g_mu);
   cudaDeviceSynchronize();
   for (auto &kv : g_ws)
     if (kv.second.ptr) cudaFree(kv.second.ptr);
   g_ws.clear();
+  for (auto &kv : g_counters)
+    if (kv.second.ptr) cudaFree(kv.second.ptr);
+  g_counters.clear();
   return HML_STATUS_SUCCESS;
 }
 

@@ -62,6 +62,17 @@ hml_sgemm_config heuristic_config(const GemmProblem &p, int algo) {
       return c;
     }
   }
+  // SIMT, N <= 16 with contiguous columns of A: the stream-K kernel with the
+  // narrowest NB that holds N and its deepest ring (measured on B200,
+  // 65536 x 8 x 4096: 6.5 TB/s against 4.8 for the tiled kernel)
+  for (int i = 0; i < stream_num_variants(); ++i) {
+    const int nb = stream_tile_n(i);
+    if (nb < p.N) continue;
+    const hml_sgemm_config sc = {HML_ALGO_SIMT, 128, nb, 1, stream_max_stages(nb),
+                                 simt_num_shapes() + i};
+    if (check_stream(p, sc) == HML_STATUS_SUCCESS) return sc;
+    break;
+  }
   // SIMT: the narrowest tile that holds N, wider rows when M is large
   int var;
   if (p.N <= 8) var = 1;

@@ -274,6 +274,10 @@ hml_status run_layouts(const GemmProblem &p, const hml_sgemm_config &c, cudaStre
 }  // namespace
 
 hml_status check_simt(const GemmProblem &p, const hml_sgemm_config &c) {
+  if (c.variant >= kNumSimtShapes && c.variant < kNumSimtShapes + stream_num_variants()) {
+    if (c.tile_n != stream_tile_n(c.variant - kNumSimtShapes)) return HML_STATUS_INVALID_VALUE;
+    return check_stream(p, c);
+  }
   if (c.variant < 0 || c.variant >= kNumSimtShapes) return HML_STATUS_INVALID_VALUE;
   const SimtShape &sh = kSimtShapes[c.variant];
   if (c.tile_m != sh.bm() || c.tile_n != sh.bn()) return HML_STATUS_INVALID_VALUE;
@@ -292,6 +296,7 @@ hml_status check_simt(const GemmProblem &p, const hml_sgemm_config &c) {
 hml_status launch_simt(const GemmProblem &p, const hml_sgemm_config &c, cudaStream_t s) {
   hml_status st = check_simt(p, c);
   if (st != HML_STATUS_SUCCESS) return st;
+  if (c.variant >= kNumSimtShapes) return launch_stream(p, c, s);
   switch (c.variant) {
     case 0: return run_layouts<0>(p, c, s);
     case 1: return run_layouts<1>(p, c, s);

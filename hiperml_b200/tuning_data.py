@@ -144,10 +144,22 @@ def main(argv=None):
     base = load(args.merge) if args.merge else None
     shapes = base["shapes"] if base is not None else sample_shapes(args.count, args.seed)
     cfgs = config_table()
-    if base is not None and not np.array_equal(base["configs"], cfgs):
-        raise SystemExit("--merge: the dataset was measured on another configuration space")
     fam_cols = (np.ones(len(cfgs), bool) if args.families == 0
                 else ((1 << cfgs[:, 0]) & args.families) != 0)
+    if base is not None and not np.array_equal(base["configs"], cfgs):
+        # the space has grown or changed: keep the old columns of the
+        # configurations still in it; every other column must be measured
+        col = {tuple(c): i for i, c in enumerate(base["configs"])}
+        old_t = base["times_us"]
+        mapped = np.full((len(shapes), len(cfgs)), np.nan, dtype=np.float32)
+        for j, c in enumerate(cfgs):
+            i = col.get(tuple(c))
+            if i is not None:
+                mapped[:, j] = old_t[:, i]
+            elif not fam_cols[j]:
+                raise SystemExit(f"--merge: configuration {tuple(c)} is new; "
+                                 "measure its family (--families)")
+        base = dict(base, times_us=mapped, configs=cfgs)
     device = torch.cuda.get_device_name(0)
     deadline = time.time() + args.max_seconds
     t0 = time.time()

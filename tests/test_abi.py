@@ -101,6 +101,10 @@ def test_config_space_roundtrip():
 def test_selection_heuristic_shapes():
     c = hml.select(0, 0, 0, 4096, 16, 4096)
     assert c.tile_n == 16 and c.split_k > 1           # skinny: split K over a cluster
+    # N <= 8 with contiguous columns of A: the stream-K kernel (SIMT variants
+    # from 9 on), which spreads K over all SMs by itself
+    c = hml.select(0, 0, 0, 65536, 4, 4096)
+    assert c.tile_n == 4 and c.variant >= 9 and c.split_k == 1
     c = hml.select(0, 0, 0, 65536, 128, 4096)
     assert c.tile_n == 128 and c.split_k == 1
     c = hml.select(0, 0, 0, 65536, 8, 4096)

@@ -70,8 +70,10 @@ def test_gemv_rows_variants(cuda, variant):
     assert_within_fp32_bound(got, D, absD, N)
 
 
-@pytest.mark.parametrize("variant", [1, 2, 3, 5, 8])
-def test_gemv_cols_cluster_split(cuda, variant):
+@pytest.mark.parametrize("variant", [1, 2, 3, 5, 8, 11, 16])
+def test_gemv_cols_split(cuda, variant):
+    """The column kernel with `variant` CTAs per 256-row tile (the last to
+    finish sums the partials in rank order), ragged rows and columns."""
     M, N = 1531, 700
     A = dg.matrix(M, N, 103, 0, dg.UNIFORM, order="C")
     x = dg.fill(N, 103, 1)
@@ -79,6 +81,29 @@ def test_gemv_cols_cluster_split(cuda, variant):
     got = run_gemv(hml.COL_MAJOR, hml.OP_N, A, 0, x, y, 2.0, -1.0, variant=variant)
     D, absD = expected(A, x, y, 2.0, -1.0, False)
     assert_within_fp32_bound(got, D, absD, N)
+
+
+def test_gemv_cols_split_repeatable(cuda):
+    """Split partials are summed in rank order whatever order the CTAs finish
+    in: repeated calls give identical bits, and the per-tile arrival counters
+    are left ready for the next call (also after a call with another split)."""
+    import torch
+    M, N = 4099, 2048
+    A = dg.matrix(M, N, 105, 0, dg.NORMAL, order="F")
+    x = dg.fill(N, 105, 1, dg.NORMAL)
+    Ad, xd = to_dev(A), to_dev(x)
+    outs = []
+    for variant in (8, 8, 5, 8, 1, 8):
+        y = torch.zeros(M, device="cuda")
+        hml.sgemv_ex(hml.COL_MAJOR, hml.OP_N, M, N, 1.0, Ad, M, xd, 0.0, y, variant=variant)
+        torch.cuda.synchronize()
+        outs.append((variant, y.cpu().numpy()))
+    ref = [o for v, o in outs if v == 8]
+    for o in ref[1:]:
+        assert np.array_equal(o, ref[0])
+    D, absD = expected(A, x, np.zeros(M, np.float32), 1.0, 0.0, False)
+    for v, o in outs:
+        assert_within_fp32_bound(o, D, absD, N, what=f"split {v}")
 
 
 def test_beta_zero_does_not_read_y(cuda):

@@ -56,11 +56,16 @@ def run_case(M, N, K, order, ta, tb, alpha, beta, config=None, pad=0, offset=0, 
     return got, D, absD
 
 
+# SIMT variants from this index on are the stream-K kernel for N <= 16
+# (tests/test_stream_gpu.py); the tiled kernel's shapes come first.
+STREAM_VARIANT0 = 9
+
+
 def simt_configs():
     out = []
     seen = set()
     for c in hml.configs():
-        if c.algo != hml.ALGO_SIMT:
+        if c.algo != hml.ALGO_SIMT or c.variant >= STREAM_VARIANT0:
             continue
         key = (c.variant, c.split_k)
         if key in seen or c.split_k not in (1, 4) or c.stages != 3:
