@@ -299,10 +299,10 @@ hml_status launch_gemv(const GemvProblem &p, int variant, cudaStream_t s) {
   const int64_t tiles = (static_cast<int64_t>(p.P) + kColRows - 1) / kColRows;
   int split = variant;
   if (split == 0) {
-    // as many CTAs as fit on the GPU at once, in one wave (measured on B200,
-    // 32768 x 4096: 8 CTAs per SM resident, split 8 = 1024 CTAs 6.6 TB/s;
-    // a second partial wave costs up to a third of that), each with >= 64
-    // columns
+    // about 7/8 of the CTAs that fit on the GPU at once, in one wave
+    // (measured on B200, 32768 x 4096, 8 CTAs per SM resident: split 8 =
+    // 1024 CTAs 6.6 TB/s, split 9 = 1152 CTAs 5.9 TB/s, split 10 (a second
+    // wave) 5.3 TB/s), each with >= 64 columns
     static const int per_sm = [] {
       int n = 0;
       if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, gemv_cols_kernel<true>, kThreads, 0) !=
@@ -311,7 +311,7 @@ hml_status launch_gemv(const GemvProblem &p, int variant, cudaStream_t s) {
         n = 1;
       return n;
     }();
-    const int64_t resident = static_cast<int64_t>(per_sm) * sm_count();
+    const int64_t resident = static_cast<int64_t>(per_sm) * sm_count() * 7 / 8;
     split = static_cast<int>(resident / tiles);
     split = max(1, min(split, kMaxColSplit));
     while (split > 1 && p.Q / split < 64) --split;

@@ -31,9 +31,10 @@
 //     results on B200 in testing (cause not found), so it is not.
 //
 // Measured on B200 (M = 65536, K = 4096, column-major A, 4 stages): N = 8
-// with K-contiguous B 214 us (5.0 TB/s of A) and N-contiguous B 186 us
-// (5.8 TB/s), against 220 us for the tiled SIMT kernel; N = 4 168 us
-// (6.4 TB/s).  Reading B through the L1 cache (LDG broadcasts) instead of
+// with K-contiguous B 194 us (5.6 TB/s of A) and N-contiguous B 180 us
+// (6.0 TB/s), against 220 us for the tiled SIMT kernel; N = 4 169 us
+// (6.3 TB/s).  The packed FMAs took N = 8 from 214 to 194 us: the kernel
+// is bound by instruction issue as much as by HBM.  Reading B through the L1 cache (LDG broadcasts) instead of
 // staging it in shared memory capped the same structure at 5.0 TB/s with
 // either B.  For 8 < N <= 16 the 64 accumulators a thread cost the second
 // CTA on each SM, and the split-BF16 tensor-core kernel is faster there.
@@ -78,12 +79,26 @@ __device__ __forceinline__ int unit_owner(long long u, long long units, int ctas
   return static_cast<int>(((u + 1) * ctas - 1) / units);
 }
 
+// A lane's accumulators: rows j = 0..3 of its 4, columns of C in pairs
+// (acc[j][h] = columns 2h, 2h + 1), updated with sm_100's packed FP32 FMA
+// (fma.rn.f32x2): each half is rounded exactly as the scalar fma.rn, so the
+// sums are bitwise those of scalar FMAs in the same order, with half the
+// FMA instructions issued.
 template <int NB>
-__device__ __forceinline__ void zero_acc(float (&acc)[4][NB]) {
+__device__ __forceinline__ void zero_acc(float2 (&acc)[4][NB / 2]) {
 #pragma unroll
   for (int j = 0; j < 4; ++j)
 #pragma unroll
-    for (int n = 0; n < NB; ++n) acc[j][n] = 0.0f;
+    for (int h = 0; h < NB / 2; ++h) acc[j][h] = make_float2(0.0f, 0.0f);
+}
+
+// acc[j][*] += a.j * (b pairs), j = 0..3 for the four components of a
+template <int NB>
+__device__ __forceinline__ void fma_rows(float2 (&acc)[4][NB / 2], float4 a, int h, float2 b) {
+  acc[0][h] = __ffma2_rn(make_float2(a.x, a.x), b, acc[0][h]);
+  acc[1][h] = __ffma2_rn(make_float2(a.y, a.y), b, acc[1][h]);
+  acc[2][h] = __ffma2_rn(make_float2(a.z, a.z), b, acc[2][h]);
+  acc[3][h] = __ffma2_rn(make_float2(a.w, a.w), b, acc[3][h]);
 }
 
 // Returns only once every accumulator holds its value, i.e. once every
@@ -92,11 +107,11 @@ __device__ __forceinline__ void zero_acc(float (&acc)[4][NB]) {
 // compiler may otherwise sink the FMAs (and so the loads' completion) past
 // the release.
 template <int NB>
-__device__ __forceinline__ void loads_consumed(const float (&acc)[4][NB]) {
+__device__ __forceinline__ void loads_consumed(const float2 (&acc)[4][NB / 2]) {
 #pragma unroll
   for (int j = 0; j < 4; ++j)
 #pragma unroll
-    for (int n = 0; n < NB; ++n) asm volatile("" ::"f"(acc[j][n]));
+    for (int h = 0; h < NB / 2; ++h) asm volatile("" ::"f"(acc[j][h].x), "f"(acc[j][h].y));
 }
 
 __device__ __forceinline__ void consumers_sync() {
@@ -240,8 +255,8 @@ __global__ void __launch_bounds__(kSThreads, kSCtasPerSm)
   // -------------------------------------------------------------- consumers
   const int phase = warp;
   const int tid = static_cast<int>(threadIdx.x);  // 0..255
-  float acc[4][NB];
-  zero_acc(acc);
+  float2 acc[4][NB / 2];
+  zero_acc<NB>(acc);
   bool bad = false;  // after an expired wait: no more waits, same barriers
   int strip = strip0, kb = kb0;
   for (int it = 0; it < nunits; ++it) {
@@ -258,13 +273,9 @@ __global__ void __launch_bounds__(kSThreads, kSCtasPerSm)
         const int c = phase + j * kSPhases;
         const float4 v = *reinterpret_cast<const float4 *>(ta + c * kSRows + lane * 4);
 #pragma unroll
-        for (int n = 0; n < NB; ++n) {
-          const float b = tb[n * kSCols + c];
-          acc[0][n] = fmaf(v.x, b, acc[0][n]);
-          acc[1][n] = fmaf(v.y, b, acc[1][n]);
-          acc[2][n] = fmaf(v.z, b, acc[2][n]);
-          acc[3][n] = fmaf(v.w, b, acc[3][n]);
-        }
+        for (int h = 0; h < NB / 2; ++h)
+          fma_rows<NB>(acc, v, h,
+                       make_float2(tb[(2 * h) * kSCols + c], tb[(2 * h + 1) * kSCols + c]));
       }
     } else {
       // B box stored [k][n]: this warp's 4 consecutive columns, NB / 4
@@ -277,19 +288,13 @@ __global__ void __launch_bounds__(kSThreads, kSCtasPerSm)
 #pragma unroll
         for (int n4 = 0; n4 < NB; n4 += 4) {
           const float4 b4 = *reinterpret_cast<const float4 *>(tb + (c0 + q) * NB + n4);
-          const float bb[4] = {b4.x, b4.y, b4.z, b4.w};
-#pragma unroll
-          for (int r = 0; r < 4; ++r) {
-            acc[0][n4 + r] = fmaf(v.x, bb[r], acc[0][n4 + r]);
-            acc[1][n4 + r] = fmaf(v.y, bb[r], acc[1][n4 + r]);
-            acc[2][n4 + r] = fmaf(v.z, bb[r], acc[2][n4 + r]);
-            acc[3][n4 + r] = fmaf(v.w, bb[r], acc[3][n4 + r]);
-          }
+          fma_rows<NB>(acc, v, n4 / 2, make_float2(b4.x, b4.y));
+          fma_rows<NB>(acc, v, n4 / 2 + 1, make_float2(b4.z, b4.w));
         }
       }
     }
     // release the slot once every load from it has returned
-    loads_consumed(acc);
+    loads_consumed<NB>(acc);
     __syncwarp();
     if (lane == 0) mbar_arrive(&empty[s]);
 
@@ -305,10 +310,11 @@ __global__ void __launch_bounds__(kSThreads, kSCtasPerSm)
 #pragma unroll
       for (int n4 = 0; n4 < NB; n4 += 4)
         *reinterpret_cast<float4 *>(red + (phase * kSRows + lane * 4 + j) * NB + n4) =
-            make_float4(acc[j][n4], acc[j][n4 + 1], acc[j][n4 + 2], acc[j][n4 + 3]);
+            make_float4(acc[j][n4 / 2].x, acc[j][n4 / 2].y, acc[j][n4 / 2 + 1].x,
+                        acc[j][n4 / 2 + 1].y);
     consumers_sync();
     finish_strip<NB>(args, cur, cta, ctas, strip0, tid, red, &s_last);
-    zero_acc(acc);
+    zero_acc<NB>(acc);
   }
 }
 
