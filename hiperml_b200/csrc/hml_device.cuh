@@ -120,6 +120,19 @@ __device__ __forceinline__ bool mbar_wait_cluster(uint64_t *bar, uint32_t parity
   }
 }
 
+// ------------------------------------------------- dependent launches
+// Lets the next kernel on the stream (launched as a programmatic dependent)
+// begin as soon as every CTA of this grid has executed this.
+__device__ __forceinline__ void allow_dependent_launch() {
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
+// Waits until the grid this one was launched after has completed and its
+// memory writes are visible (returns at once for a normal launch).
+__device__ __forceinline__ void wait_prior_grid() {
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+}
+
 // ------------------------------------------------------------------ TMA
 // 2-D tiled bulk tensor load, global -> this CTA's shared memory, completing
 // on `bar` with the tile's byte count.  No multicast.

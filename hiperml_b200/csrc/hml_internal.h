@@ -110,26 +110,42 @@ void count_launch(int n = 1);
 uint64_t launch_count();
 
 // Launch with an optional thread-block cluster along x.
+// `early`: programmatic dependent launch -- the kernel may start while the
+// previous kernel on the stream is still running (once all of that kernel's
+// CTAs have executed griddepcontrol.launch_dependents); the kernel must
+// execute griddepcontrol.wait before it reads anything that kernel writes.
 template <typename... KArgs, typename... Args>
-cudaError_t launch_k(void (*k)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t s,
-                     int cluster_x, Args... args) {
+cudaError_t launch_k_ex(void (*k)(KArgs...), dim3 grid, dim3 block, size_t smem,
+                        cudaStream_t s, int cluster_x, bool early, Args... args) {
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = grid;
   cfg.blockDim = block;
   cfg.dynamicSmemBytes = smem;
   cfg.stream = s;
-  cudaLaunchAttribute attr[1];
-  cfg.numAttrs = 0;
+  cudaLaunchAttribute attr[2];
+  int n = 0;
   if (cluster_x > 1) {
-    attr[0].id = cudaLaunchAttributeClusterDimension;
-    attr[0].val.clusterDim.x = cluster_x;
-    attr[0].val.clusterDim.y = 1;
-    attr[0].val.clusterDim.z = 1;
-    cfg.attrs = attr;
-    cfg.numAttrs = 1;
+    attr[n].id = cudaLaunchAttributeClusterDimension;
+    attr[n].val.clusterDim.x = cluster_x;
+    attr[n].val.clusterDim.y = 1;
+    attr[n].val.clusterDim.z = 1;
+    ++n;
   }
+  if (early) {
+    attr[n].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[n].val.programmaticStreamSerializationAllowed = 1;
+    ++n;
+  }
+  cfg.attrs = n ? attr : nullptr;
+  cfg.numAttrs = n;
   count_launch();
   return cudaLaunchKernelEx(&cfg, k, static_cast<KArgs>(args)...);
+}
+
+template <typename... KArgs, typename... Args>
+cudaError_t launch_k(void (*k)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t s,
+                     int cluster_x, Args... args) {
+  return launch_k_ex(k, grid, block, smem, s, cluster_x, false, args...);
 }
 
 }  // namespace hml

@@ -317,6 +317,9 @@ struct TcArgs {
 template <int NS>
 __global__ void split_b_kernel(const float *B, int64_t sbk, int64_t sbn, int K, int N,
                                __nv_bfloat16 *planes, int k_pad, int n_pad) {
+  // the tensor-core kernel that reads the planes is launched as a
+  // programmatic dependent: its set-up and A loads overlap this kernel
+  allow_dependent_launch();
   const int64_t chunks = static_cast<int64_t>(n_pad) * (k_pad / 8);
   for (int64_t c = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; c < chunks;
        c += static_cast<int64_t>(gridDim.x) * blockDim.x) {
@@ -498,6 +501,10 @@ __global__ void __launch_bounds__(tc_warps(BN, NS) * 32, 1)
     // -------------------------------------------------------- TMA, B
     if (lane == 0) {
       prefetch_tmap(&tmB);
+      // the B planes come from the kernel launched just before this one,
+      // which may still be running (programmatic dependent launch); nothing
+      // else this kernel reads depends on it
+      wait_prior_grid();
       for (int kb = 0; kb < nkb; ++kb) {
         const int o = kb % SO;
         if (!mbar_wait(&opempty[o], ((kb / SO) & 1) ^ 1, args.err, kDevErrEmptyBarrier)) {
@@ -830,8 +837,10 @@ hml_status launch_tc_planes(const GemmProblem &p, const hml_sgemm_config &c,
   const int64_t tiles_n = n_pad / BN;
   if (tiles_m * c.split_k > 0x7fffffff || tiles_n > 65535) return HML_STATUS_NOT_SUPPORTED;
   dim3 grid(static_cast<unsigned>(tiles_m * c.split_k), static_cast<unsigned>(tiles_n));
-  e = launch_k(kern, grid, dim3(tc_warps(BN, NS) * 32), smem, s, pair ? 2 : c.split_k, ta, tb,
-               args);
+  // launched right after split_b_kernel wrote the planes: a programmatic
+  // dependent whose B loader waits for it (wait_prior_grid)
+  e = launch_k_ex(kern, grid, dim3(tc_warps(BN, NS) * 32), smem, s, pair ? 2 : c.split_k, true,
+                  ta, tb, args);
   note_cuda_error(e, "tc launch");
   return cuda_status(e);
 }
