@@ -1007,6 +1007,7 @@ __host__ __device__ constexpr int tcb_warps(int bn, int ns) {
 
 template <int BN, int NS>
 __global__ void __launch_bounds__(tcb_warps(BN, NS) * 32, 1) tc_batch_kernel(TcBatchArgs args) {
+  allow_dependent_launch();  // the next tile kernel may take SMs this one leaves
   constexpr int G = tc_groups();
   constexpr int D = tcb_drain_groups(BN);
   constexpr int DC = BN / D;
@@ -1087,6 +1088,11 @@ __global__ void __launch_bounds__(tcb_warps(BN, NS) * 32, 1) tc_batch_kernel(TcB
   } else if (warp == 1) {
     // -------------------------------------------------------- TMA, B
     if (lane == 0 && nch > 0) {
+      // launched as a programmatic dependent of the previous kernel of the
+      // plan: the B planes are complete once that kernel is (the kernel
+      // before a tile kernel is the splitting kernel or another tile
+      // kernel, itself complete only after the splitting kernel)
+      wait_prior_grid();
       ItemCursor cur;
       cur.start(args, i0);
       for (int blk = 0; blk < nblk; ++blk) {
@@ -1270,6 +1276,7 @@ struct TcSplitDesc {
 
 template <int NS>
 __global__ void split_b_batch_kernel(const TcSplitDesc *descs) {
+  allow_dependent_launch();  // the tensor-core kernels wait for the planes
   const TcSplitDesc d = descs[blockIdx.y];
   const int64_t chunks = static_cast<int64_t>(d.n_pad) * (d.k_pad / 8);
   for (int64_t c = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; c < chunks;
@@ -1539,20 +1546,21 @@ hml_status tc_batch_launch(const TcBatch *b, cudaStream_t s) {
       <<<dim3(static_cast<unsigned>(b->split_blocks), static_cast<unsigned>(b->nprob)), 256, 0,
          s>>>(b->splits);
   cudaError_t e = cudaGetLastError();
+  // each tile kernel is a programmatic dependent of the kernel before it:
+  // its CTAs start on the SMs that kernel has finished with, and only its B
+  // loader waits for that kernel to complete
   for (int c = 0; c < 3 && e == cudaSuccess; ++c) {
     const TcBatch::Class &k = b->cls[c];
     if (k.grid == 0) continue;
-    count_launch();
     if (c == 0)
-      tc_batch_kernel<32, kBatchTcNS>
-          <<<k.grid, tcb_warps(32, kBatchTcNS) * 32, k.smem, s>>>(k.args);
+      e = launch_k_ex(tc_batch_kernel<32, kBatchTcNS>, dim3(k.grid),
+                      dim3(tcb_warps(32, kBatchTcNS) * 32), k.smem, s, 1, true, k.args);
     else if (c == 1)
-      tc_batch_kernel<64, kBatchTcNS>
-          <<<k.grid, tcb_warps(64, kBatchTcNS) * 32, k.smem, s>>>(k.args);
+      e = launch_k_ex(tc_batch_kernel<64, kBatchTcNS>, dim3(k.grid),
+                      dim3(tcb_warps(64, kBatchTcNS) * 32), k.smem, s, 1, true, k.args);
     else
-      tc_batch_kernel<128, kBatchTcNS>
-          <<<k.grid, tcb_warps(128, kBatchTcNS) * 32, k.smem, s>>>(k.args);
-    e = cudaGetLastError();
+      e = launch_k_ex(tc_batch_kernel<128, kBatchTcNS>, dim3(k.grid),
+                      dim3(tcb_warps(128, kBatchTcNS) * 32), k.smem, s, 1, true, k.args);
   }
   note_cuda_error(e, "tc batch launch");
   return cuda_status(e);
