@@ -49,7 +49,7 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="sweep",
                     choices=["sweep", "c1", "gemv_n", "gemv_t", "square", "batched"])
-    ap.add_argument("--algo", default="auto", choices=["auto", "simt", "bf16x3", "bf16x6"],
+    ap.add_argument("--algo", default="auto", choices=["auto", "simt", "bf16x3", "bf16x6", "tf32x3"],
                     help="force one algorithm family (default: the library's choice)")
     ap.add_argument("--rows", type=int, default=None,
                     help="sweep workload: M other than 65536 (small cases for profiler captures)")
@@ -347,7 +347,7 @@ def run_ours(args):
     stream = torch.cuda.current_stream()
 
     problems = workload_problems(args.workload, args.rows, args.only_n)
-    algo = {"auto": None, "simt": 1, "bf16x3": 2, "bf16x6": 3}[args.algo]
+    algo = {"auto": None, "simt": 1, "bf16x3": 2, "bf16x6": 3, "tf32x3": 4}[args.algo]
 
     # ---- device operands (one A shared by the sweep's GEMMs)
     bufs = []
@@ -442,7 +442,7 @@ def run_ours(args):
     alg_flops = flops_of(k, M, N, K)
     dom_s = per_kernel_ms[dom] * 1e-3
     dcfg = bufs[dom][7]
-    algo_names = {1: "simt", 2: "bf16x3", 3: "bf16x6"}
+    algo_names = {1: "simt", 2: "bf16x3", 3: "bf16x6", 4: "tf32x3"}
     key = f"{args.workload}:{k}:{M}x{N}x{K}:{algo_names.get(dcfg.algo, 'gemv') if dcfg else 'gemv'}"
     traffic = traffic_table().get(key)
     ai = alg_flops / alg_bytes
@@ -451,9 +451,11 @@ def run_ours(args):
             "traffic": traffic, "kernel": key, "alg_bytes_per_launch": alg_bytes,
             "alg_flops_per_launch": alg_flops, "ms_per_launch": per_kernel_ms[dom],
             "peak_source": pk["source"], "arith_intensity": ai}
-    if dcfg is not None and dcfg.algo in (2, 3):
+    if dcfg is not None and dcfg.algo in (2, 3, 4):
         ridge = pk["bf16_tflops_sustained"] * 1e12 / (pk["hbm_gbs"] * 1e9)
-        products = 3 if dcfg.algo == 2 else 6
+        # tensor work in BF16-product units: a TF32 product runs at half the
+        # BF16 rate, so TF32X3's three count as six
+        products = {2: 3, 3: 6, 4: 6}[dcfg.algo]
         if ai * products > ridge:
             tc = alg_flops * products / dom_s / 1e12
             roof.update({"bound": "tensor", "achieved": tc, "peak": pk["bf16_tflops_sustained"],

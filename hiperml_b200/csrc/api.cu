@@ -118,6 +118,8 @@ std::vector<hml_sgemm_config> build_space() {
       v.push_back(c);
     }
   }
+  // (TF32X3 is an explicit configuration only: as accurate as BF16X6 and
+  // measured no faster -- slower up to N = 64, 2 % faster at N = 128)
   for (int algo : {HML_ALGO_BF16X3, HML_ALGO_BF16X6})
     for (int var = 0; var < tc_num_shapes(); ++var) {
       int bm, bn;
@@ -152,7 +154,8 @@ hml_status run(const GemmProblem &p, const hml_sgemm_config &c, cudaStream_t s) 
   switch (c.algo) {
     case HML_ALGO_SIMT: return launch_simt(p, c, s);
     case HML_ALGO_BF16X3:
-    case HML_ALGO_BF16X6: return launch_tc(p, c, s);
+    case HML_ALGO_BF16X6:
+    case HML_ALGO_TF32X3: return launch_tc(p, c, s);
     default: return HML_STATUS_INVALID_VALUE;
   }
 }
@@ -175,7 +178,8 @@ hml_status check_config(const GemmProblem &p, const hml_sgemm_config &c) {
   switch (c.algo) {
     case HML_ALGO_SIMT: return check_simt(p, c);
     case HML_ALGO_BF16X3:
-    case HML_ALGO_BF16X6: return check_tc(p, c);
+    case HML_ALGO_BF16X6:
+    case HML_ALGO_TF32X3: return check_tc(p, c);
     default: return HML_STATUS_INVALID_VALUE;
   }
 }
@@ -264,7 +268,8 @@ hml_status hml_sgemm_select_algo(hml_order order, hml_op transA, hml_op transB, 
                                  int K, int algo, hml_sgemm_config *config) {
   if (!config) return HML_STATUS_INVALID_VALUE;
   if (algo == HML_ALGO_AUTO) return hml_sgemm_select(order, transA, transB, M, N, K, config);
-  if (algo != HML_ALGO_SIMT && algo != HML_ALGO_BF16X3 && algo != HML_ALGO_BF16X6)
+  if (algo != HML_ALGO_SIMT && algo != HML_ALGO_BF16X3 && algo != HML_ALGO_BF16X6 &&
+      algo != HML_ALGO_TF32X3)
     return HML_STATUS_INVALID_VALUE;
   GemmProblem p;
   const bool cm = order == HML_COL_MAJOR;

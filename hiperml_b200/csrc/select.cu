@@ -19,6 +19,7 @@ void simt_shape(int v, int *bm, int *bn, int *wk);
 int tc_num_shapes();
 void tc_shape(int v, int *bm, int *bn);
 bool tc_config_fits(int bn, int ns, int stages);
+int tc_ns(int algo);
 
 namespace {
 
@@ -41,7 +42,7 @@ int choose_split(int64_t tiles, int K, int ctas_per_sm, int min_k) {
 
 hml_sgemm_config heuristic_config(const GemmProblem &p, int algo) {
   hml_sgemm_config c = {};
-  if (algo == HML_ALGO_BF16X3 || algo == HML_ALGO_BF16X6) {
+  if (algo == HML_ALGO_BF16X3 || algo == HML_ALGO_BF16X6 || algo == HML_ALGO_TF32X3) {
     int best = -1;
     // the narrowest single-CTA (128-row) tile that holds N
     for (int v = 0; v < tc_num_shapes(); ++v) {
@@ -57,7 +58,7 @@ hml_sgemm_config heuristic_config(const GemmProblem &p, int algo) {
       const int64_t tiles = ((p.M + bm - 1) / bm) * static_cast<int64_t>((p.N + bn - 1) / bn);
       int stages = 2;
       for (int st : {4, 6, 8})
-        if (tc_config_fits(bn, algo == HML_ALGO_BF16X3 ? 2 : 3, st)) stages = st;
+        if (tc_config_fits(bn, tc_ns(algo), st)) stages = st;
       c = {algo, bm, bn, choose_split(tiles, p.K, 1, 256), stages, best};
       return c;
     }

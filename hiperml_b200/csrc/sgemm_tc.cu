@@ -258,6 +258,40 @@ __host__ __device__ constexpr uint32_t idesc_bf16(int bn, int bm = kBM) {
          (static_cast<uint32_t>(bm >> 4) << 24);
 }
 
+// The same for TF32 x TF32 -> F32 (kind::tf32; A and B format code 2).
+__host__ __device__ constexpr uint32_t idesc_tf32(int bn, int bm = kBM) {
+  return (1u << 4) | (2u << 7) | (2u << 10) | (static_cast<uint32_t>(bn >> 3) << 17) |
+         (static_cast<uint32_t>(bm >> 4) << 24);
+}
+
+// Shared-memory matrix descriptor: K-major, 128-byte swizzle (rows of 128 B =
+// 32 TF32), 8-row atoms 1024 B apart (stride byte offset), version 1.
+__device__ __forceinline__ uint64_t sw128_desc(uint32_t saddr) {
+  return static_cast<uint64_t>((saddr >> 4) & 0x3FFFu) | (static_cast<uint64_t>(1) << 16) |
+         (static_cast<uint64_t>(1024 >> 4) << 32) | (static_cast<uint64_t>(1) << 46) |
+         (static_cast<uint64_t>(2) << 61);
+}
+
+// D (TMEM) (+)= A (TMEM, 128 lanes x 8 TF32 in 8 columns) * B (shared
+// memory descriptor, 8 TF32 deep), kind::tf32 with an FP32 accumulator.
+__device__ __forceinline__ void mma_tf32_ts(uint32_t dtmem, uint32_t atmem, uint64_t bdesc,
+                                            uint32_t idesc, uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::tf32 [%0], [%1], %2, %3, p;\n\t}" ::"r"(dtmem),
+      "r"(atmem), "l"(bdesc), "r"(idesc), "r"(accumulate)
+      : "memory");
+}
+
+// x rounded to TF32 (11 significant bits, nearest, ties away), in a 32-bit
+// container whose low 13 bits are zero.
+__device__ __forceinline__ uint32_t tf32_rna(float x) {
+  uint32_t r;
+  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+  return r;
+}
+
 // Split eight floats into NS BF16 planes, t0 = bf16(x), t1 = bf16(x - t0),
 // ... (each residual is exact in FP32), packed two per 32-bit word with
 // cvt.rn.bf16x2.f32 (the lower k in the low half, as in memory order).
@@ -313,10 +347,12 @@ struct TcArgs {
 };
 
 // ------------------------------------------------------------ B planes
-// planes[p][n][k] (k contiguous, zero padded to n_pad x k_pad).
+// planes[p][n][k] (k contiguous, zero padded to n_pad x k_pad): NS BF16
+// planes, or for NS = 4 two 32-bit TF32 planes, hi = TF32(x) and
+// lo = TF32(x - hi).
 template <int NS>
 __global__ void split_b_kernel(const float *B, int64_t sbk, int64_t sbn, int K, int N,
-                               __nv_bfloat16 *planes, int k_pad, int n_pad) {
+                               void *planes_out, int k_pad, int n_pad) {
   // the tensor-core kernel that reads the planes is launched as a
   // programmatic dependent: its set-up and A loads overlap this kernel
   allow_dependent_launch();
@@ -333,12 +369,29 @@ __global__ void split_b_kernel(const float *B, int64_t sbk, int64_t sbn, int K, 
                  ? B[static_cast<int64_t>(k) * sbk + static_cast<int64_t>(n) * sbn]
                  : 0.0f;
     }
-    uint4 v[NS];
-    pack8<NS>(x, v);
+    if constexpr (NS == 4) {
+      uint32_t *planes = static_cast<uint32_t *>(planes_out);
+      uint32_t h[8], l[8];
 #pragma unroll
-    for (int i = 0; i < NS; ++i)
-      *reinterpret_cast<uint4 *>(planes + (static_cast<int64_t>(i) * n_pad + n) * k_pad + k0) =
-          v[i];
+      for (int j = 0; j < 8; ++j) {
+        h[j] = tf32_rna(x[j]);
+        l[j] = tf32_rna(x[j] - __uint_as_float(h[j]));
+      }
+      uint32_t *ph = planes + static_cast<int64_t>(n) * k_pad + k0;
+      uint32_t *pl = planes + (static_cast<int64_t>(n_pad) + n) * k_pad + k0;
+      reinterpret_cast<uint4 *>(ph)[0] = make_uint4(h[0], h[1], h[2], h[3]);
+      reinterpret_cast<uint4 *>(ph)[1] = make_uint4(h[4], h[5], h[6], h[7]);
+      reinterpret_cast<uint4 *>(pl)[0] = make_uint4(l[0], l[1], l[2], l[3]);
+      reinterpret_cast<uint4 *>(pl)[1] = make_uint4(l[4], l[5], l[6], l[7]);
+    } else {
+      __nv_bfloat16 *planes = static_cast<__nv_bfloat16 *>(planes_out);
+      uint4 v[NS];
+      pack8<NS>(x, v);
+#pragma unroll
+      for (int i = 0; i < NS; ++i)
+        *reinterpret_cast<uint4 *>(planes + (static_cast<int64_t>(i) * n_pad + n) * k_pad + k0) =
+            v[i];
+    }
   }
 }
 
@@ -399,6 +452,13 @@ __global__ void __launch_bounds__(tc_warps(BN, NS) * 32, 1)
     tc_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
               TcArgs args) {
   static_assert(!PAIR || BN >= 32, "a CTA pair holds BN/2 >= 16 rows of B each");
+  // NS = 4 is the TF32 form: 2 planes of 32-bit TF32 (hi, lo), the TMEM and
+  // shared-memory footprint of 4 BF16 planes
+  constexpr bool TF = NS == 4;
+  static_assert(!(PAIR && TF), "CTA pairs run the BF16 forms only");
+  constexpr int PL = TF ? 2 : NS;                            // planes
+  constexpr int PLC = TF ? kBK : kBK / 2;                    // TMEM columns of a plane
+  constexpr int KMMA = TF ? 8 : 16;                          // K of one MMA
   constexpr int G = tc_groups();
   constexpr int D = tc_drain_groups(BN);
   constexpr int DC = BN / D;                                 // columns per drain thread
@@ -407,10 +467,11 @@ __global__ void __launch_bounds__(tc_warps(BN, NS) * 32, 1)
   constexpr int kConvWarp0 = tc_conv_warp0(BN, NS), kDrainWarp0 = kConvWarp0 + 4 * G;
   constexpr int A32_BYTES = static_cast<int>(tc_a_bytes());  // FP32 A slot (16 KB)
   constexpr int BROWS = PAIR ? BN / 2 : BN;                 // B rows of a plane in this CTA
-  constexpr int BPL_BYTES = BROWS * kBK * 2;                 // one B plane tile
-  constexpr int BSLOT = NS * BPL_BYTES;                      // one B slot
+  constexpr int BPL_BYTES = BROWS * kBK * (TF ? 4 : 2);      // one B plane tile
+  constexpr int BSLOT = PL * BPL_BYTES;                      // one B slot
   constexpr int SC = tc_stage_cols(NS);                      // TMEM columns of an A stage
-  constexpr uint32_t IDESC = idesc_bf16(BN, PAIR ? 2 * kBM : kBM);
+  static_assert(SC == PL * PLC, "stage columns");
+  constexpr uint32_t IDESC = TF ? idesc_tf32(BN) : idesc_bf16(BN, PAIR ? 2 * kBM : kBM);
   constexpr int P = kChunkK / kBK;                           // blocks per TMEM chunk
 
   extern __shared__ uint8_t smem_raw[];
@@ -515,7 +576,7 @@ __global__ void __launch_bounds__(tc_warps(BN, NS) * 32, 1)
         const int k0 = kbeg + kb * kBK;
         mbar_arrive_expect_tx(&opfull[o], BSLOT);
 #pragma unroll
-        for (int i = 0; i < NS; ++i)
+        for (int i = 0; i < PL; ++i)
           tma_load_2d(dst + i * BPL_BYTES, &tmB, &opfull[o], k0,
                       i * args.n_pad + n0 + prank * BROWS);
       }
@@ -551,20 +612,24 @@ __global__ void __launch_bounds__(tc_warps(BN, NS) * 32, 1)
           }
           tc_fence_after();
           const uint32_t astage = tA + static_cast<uint32_t>(o * SC);
-          const uint64_t b_desc = sw64_desc(smem_u32(bring + o * BSLOT));
+          const uint64_t b_desc = TF ? sw128_desc(smem_u32(bring + o * BSLOT))
+                                     : sw64_desc(smem_u32(bring + o * BSLOT));
 #pragma unroll
-          for (int kk = 0; kk < kBK / 16; ++kk) {
+          for (int kk = 0; kk < kBK / KMMA; ++kk) {
 #pragma unroll
-            for (int i = 0; i < NS; ++i)
+            for (int i = 0; i < PL; ++i)
 #pragma unroll
-              for (int j = 0; j < NS - i; ++j) {
-                // A plane i: 16 columns per plane, 8 per 16-deep step;
-                // descriptor start addresses count 16-byte units
-                const uint32_t at = astage + static_cast<uint32_t>(i * 16 + kk * 8);
+              for (int j = 0; j < PL - i; ++j) {
+                // A plane i: PLC columns per plane, 8 per MMA step (16 BF16
+                // or 8 TF32 deep); B: 32 bytes per step; descriptor start
+                // addresses count 16-byte units
+                const uint32_t at = astage + static_cast<uint32_t>(i * PLC + kk * 8);
                 const uint64_t bd =
                     b_desc + static_cast<uint64_t>((j * BPL_BYTES + kk * 32) >> 4);
                 const uint32_t acc = (!first || kk > 0 || i > 0 || j > 0) ? 1u : 0u;
-                if (PAIR)
+                if constexpr (TF)
+                  mma_tf32_ts(dacc, at, bd, IDESC, acc);
+                else if (PAIR)
                   mma_bf16_ts_pair(dacc, at, bd, IDESC, acc);
                 else
                   mma_bf16_ts(dacc, at, bd, IDESC, acc);
@@ -631,7 +696,15 @@ __global__ void __launch_bounds__(tc_warps(BN, NS) * 32, 1)
       // __syncwarp alone does not wait for the other lanes' shared-memory
       // loads to return
       uint32_t wv[16];
-      split_plane32<NS == 1>(x, wv);
+      if constexpr (TF) {
+        // hi of the first 16 values; the other 16 only need to have arrived
+#pragma unroll
+        for (int k = 0; k < 16; ++k) wv[k] = tf32_rna(x[k]);
+#pragma unroll
+        for (int k = 16; k < 32; ++k) asm volatile("" ::"f"(x[k]));
+      } else {
+        split_plane32<NS == 1>(x, wv);
+      }
       __syncwarp();
       if (lane == 0) mbar_arrive(&aempty[s]);
       // the A stage: wait until the MMAs that read it are done
@@ -642,12 +715,31 @@ __global__ void __launch_bounds__(tc_warps(BN, NS) * 32, 1)
       }
       tc_fence_after();
       const uint32_t dst = tA + lanes + static_cast<uint32_t>(o * SC);
-      tmem_st16(dst, wv);
-      split_plane32<NS == 2>(x, wv);
-      tmem_st16(dst + 16u, wv);
-      if constexpr (NS == 3) {
-        split_plane32<true>(x, wv);
+      if constexpr (TF) {
+        // one TF32 per column: plane hi in columns 0..31 (k), lo in 32..63;
+        // lo = TF32(x - hi), the residual being exact in FP32
+        tmem_st16(dst, wv);
+#pragma unroll
+        for (int k = 0; k < 16; ++k) x[k] -= __uint_as_float(wv[k]);
+#pragma unroll
+        for (int k = 0; k < 16; ++k) wv[k] = tf32_rna(x[16 + k]);
+        tmem_st16(dst + 16u, wv);
+#pragma unroll
+        for (int k = 0; k < 16; ++k) x[16 + k] -= __uint_as_float(wv[k]);
+#pragma unroll
+        for (int k = 0; k < 16; ++k) wv[k] = tf32_rna(x[k]);
         tmem_st16(dst + 32u, wv);
+#pragma unroll
+        for (int k = 0; k < 16; ++k) wv[k] = tf32_rna(x[16 + k]);
+        tmem_st16(dst + 48u, wv);
+      } else {
+        tmem_st16(dst, wv);
+        split_plane32<NS == 2>(x, wv);
+        tmem_st16(dst + 16u, wv);
+        if constexpr (NS == 3) {
+          split_plane32<true>(x, wv);
+          tmem_st16(dst + 32u, wv);
+        }
       }
       tmem_wait_st();
       tc_fence_before();
@@ -792,7 +884,7 @@ hml_status launch_tc_planes(const GemmProblem &p, const hml_sgemm_config &c,
                             cudaStream_t s) {
   // a 256-row configuration runs on CTA pairs (clusters of two)
   const bool pair = c.tile_m == 2 * kBM;
-  if (pair && (BN < 32 || c.split_k != 1)) return HML_STATUS_INVALID_VALUE;
+  if (pair && (BN < 32 || c.split_k != 1 || NS == 4)) return HML_STATUS_INVALID_VALUE;
   CUtensorMap ta, tb;
   memset(&ta, 0, sizeof ta);
   memset(&tb, 0, sizeof tb);
@@ -803,10 +895,16 @@ hml_status launch_tc_planes(const GemmProblem &p, const hml_sgemm_config &c,
   else
     ok = tensor_map_2d(&ta, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, p.A, p.M, p.K, p.sak * 4, kBM, kBK,
                        CU_TENSOR_MAP_SWIZZLE_NONE);
-  if (ok)
-    ok = tensor_map_2d(&tb, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, planes, k_pad,
-                       static_cast<uint64_t>(NS) * n_pad, static_cast<uint64_t>(k_pad) * 2, kBK,
-                       pair ? BN / 2 : BN, CU_TENSOR_MAP_SWIZZLE_64B);
+  if (ok) {
+    if (NS == 4)  // two TF32 planes: rows of 32 x 4 bytes, 128-byte swizzle
+      ok = tensor_map_2d(&tb, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, planes, k_pad,
+                         static_cast<uint64_t>(2) * n_pad, static_cast<uint64_t>(k_pad) * 4, kBK,
+                         BN, CU_TENSOR_MAP_SWIZZLE_128B);
+    else
+      ok = tensor_map_2d(&tb, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, planes, k_pad,
+                         static_cast<uint64_t>(NS) * n_pad, static_cast<uint64_t>(k_pad) * 2, kBK,
+                         pair ? BN / 2 : BN, CU_TENSOR_MAP_SWIZZLE_64B);
+  }
   if (!ok) return HML_STATUS_CUDA_ERROR;
   TcArgs args;
   args.p = p;
@@ -821,7 +919,7 @@ hml_status launch_tc_planes(const GemmProblem &p, const hml_sgemm_config &c,
   args.err = err;
   const size_t smem = tc_plan_bytes(BN, NS, plan);
   void (*kern)(CUtensorMap, CUtensorMap, TcArgs) = tc_kernel<BN, NS, AK, false>;
-  if constexpr (BN >= 32) {
+  if constexpr (BN >= 32 && NS != 4) {
     if (pair) kern = tc_kernel<BN, NS, AK, true>;
   }
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -902,18 +1000,23 @@ void tc_shape(int v, int *bm, int *bn) {
   *bn = kTcShapes[v].bn;
 }
 
+// Planes of a split-precision family, in units of BF16 planes: TF32X3's two
+// 32-bit planes take the room of four (its kernels are instantiated NS = 4).
+int tc_ns(int algo) { return algo == HML_ALGO_BF16X3 ? 2 : algo == HML_ALGO_BF16X6 ? 3 : 4; }
+
 hml_status check_tc(const GemmProblem &p, const hml_sgemm_config &c) {
-  if (c.algo != HML_ALGO_BF16X3 && c.algo != HML_ALGO_BF16X6) return HML_STATUS_INVALID_VALUE;
+  if (c.algo != HML_ALGO_BF16X3 && c.algo != HML_ALGO_BF16X6 && c.algo != HML_ALGO_TF32X3)
+    return HML_STATUS_INVALID_VALUE;
   if (c.variant < 0 || c.variant >= kNumTcShapes) return HML_STATUS_INVALID_VALUE;
   if (c.tile_m != kTcShapes[c.variant].bm || c.tile_n != kTcShapes[c.variant].bn)
     return HML_STATUS_INVALID_VALUE;
   // a CTA pair is one cluster: no cluster split-K on top of it
-  if (c.tile_m == 2 * kBM && c.split_k != 1) return HML_STATUS_INVALID_VALUE;
+  if (c.tile_m == 2 * kBM && (c.split_k != 1 || c.algo == HML_ALGO_TF32X3))
+    return HML_STATUS_INVALID_VALUE;
   if (c.split_k < 1 || c.split_k > 16 || (c.split_k & (c.split_k - 1)) != 0)
     return HML_STATUS_INVALID_VALUE;
   if (c.stages < 2 || c.stages > 8) return HML_STATUS_INVALID_VALUE;
-  const int ns = c.algo == HML_ALGO_BF16X3 ? 2 : 3;
-  if (!tc_config_fits(c.tile_n, ns, c.stages)) return HML_STATUS_INVALID_VALUE;
+  if (!tc_config_fits(c.tile_n, tc_ns(c.algo), c.stages)) return HML_STATUS_INVALID_VALUE;
   // the A ring is reused for the split-K partial tile
   if (c.split_k > 1 &&
       static_cast<size_t>(kBM) * c.tile_n * 4 > static_cast<size_t>(c.stages) * tc_a_bytes())
@@ -929,7 +1032,11 @@ hml_status check_tc(const GemmProblem &p, const hml_sgemm_config &c) {
 hml_status launch_tc(const GemmProblem &p, const hml_sgemm_config &c, cudaStream_t s) {
   hml_status st = check_tc(p, c);
   if (st != HML_STATUS_SUCCESS) return st;
-  return c.algo == HML_ALGO_BF16X3 ? run_tc_ns<2>(p, c, s) : run_tc_ns<3>(p, c, s);
+  switch (c.algo) {
+    case HML_ALGO_BF16X3: return run_tc_ns<2>(p, c, s);
+    case HML_ALGO_BF16X6: return run_tc_ns<3>(p, c, s);
+    default: return run_tc_ns<4>(p, c, s);
+  }
 }
 
 }  // namespace hml

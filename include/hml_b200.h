@@ -51,7 +51,10 @@ typedef enum hml_algo {
   HML_ALGO_AUTO = 0,   /* tuned table, then predictor, then default        */
   HML_ALGO_SIMT = 1,   /* plain FP32 FMA on CUDA cores                     */
   HML_ALGO_BF16X3 = 2, /* tcgen05: hi/lo BF16 split, 3 products (hh,hl,lh) */
-  HML_ALGO_BF16X6 = 3  /* tcgen05: hi/mid/lo split, 6 products            */
+  HML_ALGO_BF16X6 = 3, /* tcgen05: hi/mid/lo split, 6 products            */
+  HML_ALGO_TF32X3 = 4  /* tcgen05 kind::tf32: hi/lo TF32 split, 3 products
+                          (FP32-level accuracy like BF16X6; explicit
+                          configurations only, 128-row tiles)           */
 } hml_algo;
 
 /* Accuracy policy of hml_sgemm_ex's automatic choice. */

@@ -1,9 +1,11 @@
-"""Split-BF16 tcgen05 SGEMM against the FP64 oracle and the reference
-fixtures (GPU).
+"""Split-precision tcgen05 SGEMM (BF16X3, BF16X6, TF32X3) against the FP64
+oracle and the reference fixtures (GPU).
 
 Tolerances (normwise = max|dC| / max|C64|, componentwise = max |dC| /
 (|alpha||A||B| + |beta||C|)):
-  BF16X6  normwise <= 2e-6 and componentwise <= 2 gamma_{K+2} (the FP32 bound)
+  BF16X6, TF32X3  normwise <= 2e-6 and componentwise <= 2 gamma_{K+2} (the
+          FP32 bound; TF32X3's hi + lo keep 22 significant bits of each
+          operand, the one product it drops, lo x lo, is below 2**-22)
   BF16X3  normwise <= 1e-5 and componentwise <= 2**-16 + 2 gamma_{K+2}
           (the two-term split keeps ~16 significant bits of each operand)
 """
@@ -21,14 +23,15 @@ from tests.test_sgemm_gpu import fetch, store
 pytestmark = pytest.mark.gpu
 META, ARR = load()
 
-X3, X6 = hml.ALGO_BF16X3, hml.ALGO_BF16X6
+X3, X6, TF = hml.ALGO_BF16X3, hml.ALGO_BF16X6, hml.ALGO_TF32X3
+FP32_LEVEL = (X6, TF)
 VAR = {16: 0, 32: 1, 64: 2, 128: 3}
 PAIR_VAR = {32: 4, 64: 5, 128: 6}  # 256-row tiles on a CTA pair
 
 
 def check_tol(algo, got, D, absD, K, what=""):
     e = oracle.rel_errors(got, D, absD)
-    if algo == X6:
+    if algo in FP32_LEVEL:
         assert e["normwise"] <= 2e-6, (what, e)
         assert e["compwise"] <= 2 * gamma(K + 2), (what, e)
     else:
@@ -55,7 +58,7 @@ def run_tc(M, N, K, algo, bn, split=1, stages=4, order=0, ta=0, tb=0, alpha=1.0,
     return got, D, absD
 
 
-@pytest.mark.parametrize("algo", [X3, X6])
+@pytest.mark.parametrize("algo", [X3, X6, TF])
 @pytest.mark.parametrize("bn", [16, 32, 64, 128])
 @pytest.mark.parametrize("layout", [(0, 0, 0), (0, 1, 0), (0, 0, 1), (1, 0, 0), (1, 1, 1)])
 def test_tc_tiles_and_layouts(cuda, algo, bn, layout):
@@ -65,7 +68,7 @@ def test_tc_tiles_and_layouts(cuda, algo, bn, layout):
         check_tol(algo, got, D, absD, K, what=f"{algo} {bn} {layout} {(M, N, K)}")
 
 
-@pytest.mark.parametrize("algo", [X3, X6])
+@pytest.mark.parametrize("algo", [X3, X6, TF])
 @pytest.mark.parametrize("split", [2, 4, 8, 16])
 def test_tc_cluster_split_k(cuda, algo, split):
     for K in (64, 1000, 4096):
@@ -75,7 +78,7 @@ def test_tc_cluster_split_k(cuda, algo, split):
 
 @pytest.mark.parametrize("stages", [2, 4, 6, 8])
 def test_tc_ring_depths(cuda, stages):
-    for algo, bn in ((X3, 128), (X6, 64)):
+    for algo, bn in ((X3, 128), (X6, 64), (TF, 32), (TF, 128)):
         cfg = SgemmConfig(algo, 128, bn, 1, stages, VAR[bn])
         if hml.config_check(0, 0, 0, 500, bn, 800, 500, 800, 500, cfg) != 0:
             continue
@@ -102,7 +105,7 @@ def test_tc_beta_zero_does_not_read_c(cuda):
     assert torch.isfinite(C).all()
 
 
-@pytest.mark.parametrize("algo", [X3, X6])
+@pytest.mark.parametrize("algo", [X3, X6, TF])
 @pytest.mark.parametrize("case", [c for c in META["sgemm"] if (c["K"] * 4) % 16 == 0],
                          ids=lambda c: c["name"])
 def test_tc_matches_reference_golden(cuda, algo, case):
@@ -130,7 +133,7 @@ def test_tc_matches_reference_golden(cuda, algo, case):
     assert np.all(np.abs(ref - D) <= 2 * gamma(K + 2) * absD + 1e-37)
 
 
-@pytest.mark.parametrize("algo", [X3, X6])
+@pytest.mark.parametrize("algo", [X3, X6, TF])
 def test_tc_c1_full_size_against_reference_golden(cuda, algo):
     import torch
     M, N, K = 4096, 16, 4096
@@ -147,11 +150,11 @@ def test_tc_c1_full_size_against_reference_golden(cuda, algo):
     D, absD = oracle.dgemm(An, Bn, with_abs=True)
     check_tol(algo, got, D, absD, K, what="C1")
     ref = ARR["cfg_sgemm_4096x16x4096"].astype(np.float64)
-    tol = 2e-6 if algo == X6 else 1e-5
+    tol = 2e-6 if algo in FP32_LEVEL else 1e-5
     assert np.max(np.abs(got - ref)) / np.max(np.abs(ref)) <= tol + 4 * 2.0 ** -24 * 64
 
 
-@pytest.mark.parametrize("algo", [X3, X6])
+@pytest.mark.parametrize("algo", [X3, X6, TF])
 @pytest.mark.parametrize("N", [8, 32, 64, 128])
 def test_tc_precision_sweep_full_size(cuda, algo, N):
     """M = 65536, K = 4096, uniform and log-uniform (1e-3..1e3) inputs,
@@ -167,7 +170,7 @@ def test_tc_precision_sweep_full_size(cuda, algo, N):
         hml.fill_random(B, 2, 1, dist)
         hml.sgemm_ex(0, 0, 0, M, N, K, 1.0, A, M, B, K, 0.0, C, M, config=cfg)
         err = hml.error_fp64(0, 0, 0, M, N, K, 1.0, A, M, B, K, 0.0, None, C, M)
-        if algo == X6:
+        if algo in FP32_LEVEL:
             assert err[0] <= 2e-6 and err[2] <= 2 * gamma(K + 2), err
         else:
             assert err[0] <= 1e-5, err
@@ -200,3 +203,13 @@ def test_tc_cta_pair_equals_single_cta(cuda, algo, bn, layout):
 def test_tc_cta_pair_rejects_split_k(cuda):
     cfg = SgemmConfig(X6, 256, 64, 2, 4, PAIR_VAR[64])
     assert hml.config_check(0, 0, 0, 512, 64, 256, 512, 256, 512, cfg) == 1
+
+
+def test_tf32x3_explicit_only_and_no_cta_pair(cuda):
+    """TF32X3 is an explicit configuration: outside the autotuner's space,
+    and single-CTA tiles only."""
+    assert all(c.algo != TF for c in hml.configs())
+    assert hml.config_check(0, 0, 0, 4096, 64, 4096, 4096, 4096, 4096,
+                            SgemmConfig(TF, 256, 64, 1, 4, PAIR_VAR[64])) == 1
+    assert hml.config_check(0, 0, 0, 4096, 64, 4096, 4096, 4096, 4096,
+                            SgemmConfig(TF, 128, 64, 1, 4, VAR[64])) == 0
