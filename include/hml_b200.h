@@ -223,7 +223,8 @@ typedef struct hml_predictor_options {
 /* Trains on n shapes (shapes: n x 5 int32 rows M, N, K, transA, transB in
  * `order` with 16-byte-rounded leading dimensions, the autotuner's layout)
  * and their measured times (times_us: n x n_configs, <= 0 where a
- * configuration was not measured; column j belongs to configs[j]).  The
+ * configuration was not measured; column j belongs to configuration j of
+ * hml_sgemm_get_config, the n_configs of the space).  The
  * trained network becomes the active predictor; loss_history (may be NULL)
  * receives the mean training loss of each epoch. */
 hml_status hml_predictor_train(hml_order order, const int32_t *shapes,
