@@ -110,7 +110,7 @@ std::vector<hml_sgemm_config> build_space() {
         v.push_back(c);
       }
   }
-  // the stream-K kernel for N <= 16 (variants after the tiled shapes)
+  // the stream-K kernel for N <= 8 (variants after the tiled shapes)
   for (int i = 0; i < stream_num_variants(); ++i) {
     const int nb = stream_tile_n(i), top = stream_max_stages(nb);
     for (int stages : {top - 2, top - 1, top}) {

@@ -57,7 +57,7 @@ hml_status launch_scale(float *C, int M, int N, int64_t scm, int64_t scn, float 
 hml_status launch_simt(const GemmProblem &p, const hml_sgemm_config &c, cudaStream_t s);
 hml_status launch_tc(const GemmProblem &p, const hml_sgemm_config &c, cudaStream_t s);
 hml_status check_simt(const GemmProblem &p, const hml_sgemm_config &c);
-// The stream-K SIMT kernel for N <= 16 with contiguous columns of A
+// The stream-K SIMT kernel for N <= 8 with contiguous columns of A
 // (sgemm_stream.cu); reached through the SIMT family's variants
 // simt_num_shapes() .. simt_num_shapes() + stream_num_variants() - 1.
 int stream_num_variants();

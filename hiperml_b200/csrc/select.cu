@@ -63,7 +63,7 @@ hml_sgemm_config heuristic_config(const GemmProblem &p, int algo) {
       return c;
     }
   }
-  // SIMT, N <= 16 with contiguous columns of A: the stream-K kernel with the
+  // SIMT, N <= 8 with contiguous columns of A: the stream-K kernel with the
   // narrowest NB that holds N and its deepest ring (measured on B200,
   // 65536 x 8 x 4096: 6.5 TB/s against 4.8 for the tiled kernel)
   for (int i = 0; i < stream_num_variants(); ++i) {

@@ -36,8 +36,9 @@
 // (6.3 TB/s).  The packed FMAs took N = 8 from 214 to 194 us: the kernel
 // is bound by instruction issue as much as by HBM.  Reading B through the L1
 // cache (LDG broadcasts) instead of staging it in shared memory capped the
-// same structure at 5.0 TB/s with either B.  For 8 < N <= 16 the 64 accumulators a thread cost the second
-// CTA on each SM, and the split-BF16 tensor-core kernel is faster there.
+// same structure at 5.0 TB/s with either B.  For 8 < N <= 16 the 64
+// accumulators a thread cost the second CTA on each SM, and the split-BF16
+// tensor-core kernel is faster there.
 #include <algorithm>
 #include <cstring>
 

@@ -75,7 +75,10 @@ typedef struct hml_sgemm_config {
                       each taking a slice of K; partial tiles are summed
                       in rank order through distributed shared memory     */
   int32_t stages;  /* shared-memory pipeline depth                        */
-  int32_t variant; /* per-algorithm micro-tile selector                   */
+  int32_t variant; /* per-algorithm micro-tile selector (SIMT: 0-8 the
+                      tiled kernel's micro-tiles, 9-10 the stream-K
+                      kernel for N <= 4 / 8 with contiguous columns of A;
+                      split-BF16/TF32: the tile shape)                  */
 } hml_sgemm_config;
 
 const char *hml_status_string(hml_status status);

@@ -56,7 +56,7 @@ def run_case(M, N, K, order, ta, tb, alpha, beta, config=None, pad=0, offset=0, 
     return got, D, absD
 
 
-# SIMT variants from this index on are the stream-K kernel for N <= 16
+# SIMT variants from this index on are the stream-K kernel for N <= 8
 # (tests/test_stream_gpu.py); the tiled kernel's shapes come first.
 STREAM_VARIANT0 = 9
 
