@@ -9,17 +9,18 @@
 //
 // Structure of one CTA (2 per SM):
 //   * warp 8, one lane: TMA of each unit's A box (128 x 32 FP32, column
-//     after column) and of the matching 32 rows of B (K-contiguous or
-//     N-contiguous, as stored) into a ring of `stages` shared-memory slots;
+//     after column) and of the matching 32 rows of B (N-contiguous: a
+//     K-contiguous B is first copied so by gather_b_kernel, launched just
+//     before, this kernel being its programmatic dependent) into a ring of
+//     `stages` shared-memory slots;
 //     a slot is refilled once the 8 consumer warps have released it.  (With
 //     the loads issued by a consumer lane instead, that warp waits for the
 //     slowest one before each refill, and the last warp to release a slot
 //     issuing its refill was no better: both measured 1.3x slower on B200.)
-//   * warps 0..7 ("column phases"): warp w takes 4 of the box's 32 columns
-//     (w, w + 8, ... when B is K-contiguous; 4w .. 4w + 3 otherwise, so
-//     that one 16-byte load brings 4 values of B); a lane owns 4 consecutive
-//     rows (one 16-byte shared-memory load per column) and all NB columns
-//     of C for them, the values of B read as shared-memory broadcasts.
+//   * warps 0..7 ("column phases"): warp w takes the box's columns 4w ..
+//     4w + 3; a lane owns 4 consecutive rows (one 16-byte shared-memory load
+//     per column) and all NB columns of C for them, the values of B read as
+//     16-byte shared-memory broadcasts.
 //   * at the end of each strip in the range: the 8 phases are summed in
 //     order in shared memory.  A strip owned by one CTA is written to C
 //     (alpha, beta applied; beta == 0 does not read C).  A strip shared by
@@ -31,9 +32,9 @@
 //     results on B200 in testing (cause not found), so it is not.
 //
 // Measured on B200 (M = 65536, K = 4096, column-major A, 4 stages): N = 8
-// with K-contiguous B 194 us (5.6 TB/s of A) and N-contiguous B 180 us
-// (6.0 TB/s), against 220 us for the tiled SIMT kernel; N = 4 169 us
-// (6.3 TB/s).  The packed FMAs took N = 8 from 214 to 194 us: the kernel
+// 180 us with N-contiguous B (6.0 TB/s of A), and 194 us streaming a
+// K-contiguous B as stored (before the copy), against 220 us for the tiled
+// SIMT kernel; N = 4 165 us (6.5 TB/s).  The packed FMAs took N = 8 from 214 to 194 us: the kernel
 // is bound by instruction issue as much as by HBM.  Reading B through the L1
 // cache (LDG broadcasts) instead of staging it in shared memory capped the
 // same structure at 5.0 TB/s with either B.  For 8 < N <= 16 the 64
@@ -180,7 +181,7 @@ __device__ __forceinline__ void finish_strip(const StreamArgs &args, int strip, 
   consumers_sync();  // red and s_last are rewritten at the next strip end
 }
 
-template <int NB, bool BK_>
+template <int NB>
 __global__ void __launch_bounds__(kSThreads, kSCtasPerSm)
     stream_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
                   const __grid_constant__ StreamArgs args) {
@@ -226,14 +227,14 @@ __global__ void __launch_bounds__(kSThreads, kSCtasPerSm)
     uint8_t *dst = smem + s * STAGE;
     mbar_arrive_expect_tx(&full[s], STAGE);
     tma_load_2d(dst, &tmA, &full[s], strip * kSRows, k0);
-    if (BK_)
-      tma_load_2d(dst + A_BYTES, &tmB, &full[s], k0, 0);
-    else
-      tma_load_2d(dst + A_BYTES, &tmB, &full[s], 0, k0);
+    tma_load_2d(dst + A_BYTES, &tmB, &full[s], 0, k0);
   };
   if (warp == kSPhases) {
     // ------------------------------------------------------------ producer
     if (lane == 0) {
+      // B may be a copy written by the kernel launched just before this one
+      // (a programmatic dependent launch); A and C do not depend on it
+      wait_prior_grid();
       int strip = strip0, kb = kb0, j = 0;
       for (; j < nunits; ++j) {
         const int s = j % stages;
@@ -265,20 +266,7 @@ __global__ void __launch_bounds__(kSThreads, kSCtasPerSm)
     if (!bad && !mbar_wait(&full[s], (it / stages) & 1, args.err, kDevErrFullBarrier)) bad = true;
     const float *ta = reinterpret_cast<const float *>(smem + s * STAGE);
     const float *tb = reinterpret_cast<const float *>(smem + s * STAGE + A_BYTES);
-    if constexpr (BK_) {
-      // B box stored [n][k]: columns phase, phase + 8, ... with NB scalar
-      // broadcasts each (the 4-column form below needs more than the 96
-      // registers two CTAs per SM leave, and spills)
-#pragma unroll
-      for (int j = 0; j < kSCols / kSPhases; ++j) {
-        const int c = phase + j * kSPhases;
-        const float4 v = *reinterpret_cast<const float4 *>(ta + c * kSRows + lane * 4);
-#pragma unroll
-        for (int h = 0; h < NB / 2; ++h)
-          fma_rows<NB>(acc, v, h,
-                       make_float2(tb[(2 * h) * kSCols + c], tb[(2 * h + 1) * kSCols + c]));
-      }
-    } else {
+    {
       // B box stored [k][n]: this warp's 4 consecutive columns, NB / 4
       // vector broadcasts each
       constexpr int CW = kSCols / kSPhases;
@@ -340,10 +328,31 @@ int64_t row_stride_bytes(int64_t stride, int64_t inner, int64_t outer) {
   return outer == 1 ? ((inner * 4 + 15) / 16) * 16 : stride * 4;
 }
 
-template <int NB, bool BK_>
-hml_status run_stream(const GemmProblem &p, const hml_sgemm_config &c, cudaStream_t s) {
+// K-contiguous B (K x N) -> an N-contiguous copy [K][nb] with columns N..nb-1
+// zero: the kernel streams that layout faster (B box one contiguous 32 x nb
+// block; measured N = 8, M = 65536, K = 4096: 180 against 194 us).
+__global__ void gather_b_kernel(const float *__restrict__ B, int64_t sbk, int64_t sbn, int K,
+                                int N, float *__restrict__ out, int nb) {
+  allow_dependent_launch();  // the stream kernel waits for the copy itself
+  for (int64_t k = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; k < K;
+       k += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    float v[8];
+#pragma unroll
+    for (int n = 0; n < 8; ++n) v[n] = (n < N) ? B[k * sbk + n * sbn] : 0.0f;
+    float4 *o = reinterpret_cast<float4 *>(out + k * nb);
+    o[0] = make_float4(v[0], v[1], v[2], v[3]);
+    if (nb == 8) o[1] = make_float4(v[4], v[5], v[6], v[7]);
+  }
+}
+
+// One launch of stream_kernel<NB> on p (B N-contiguous); `partial` is the
+// workspace slot area, `early` makes it a programmatic dependent of the
+// previous kernel on the stream (which then wrote B).
+template <int NB>
+hml_status launch_stream_kernel(const GemmProblem &p, const hml_sgemm_config &c, float *partial,
+                                int ctas, bool early, cudaStream_t s) {
   const size_t smem = stream_smem(NB, c.stages);
-  auto kern = stream_kernel<NB, BK_>;
+  auto kern = stream_kernel<NB>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        static_cast<int>(smem));
   if (e != cudaSuccess) {
@@ -356,36 +365,55 @@ hml_status run_stream(const GemmProblem &p, const hml_sgemm_config &c, cudaStrea
   bool ok = tensor_map_2d(&ta, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, p.A, p.M, p.K,
                           row_stride_bytes(p.sak, p.M, p.K), kSRows, kSCols,
                           CU_TENSOR_MAP_SWIZZLE_NONE);
-  if (ok) {
-    if (BK_)
-      ok = tensor_map_2d(&tb, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, p.B, p.K, p.N,
-                         row_stride_bytes(p.sbn, p.K, p.N), kSCols, NB, CU_TENSOR_MAP_SWIZZLE_NONE);
-    else
-      ok = tensor_map_2d(&tb, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, p.B, p.N, p.K,
-                         row_stride_bytes(p.sbk, p.N, p.K), NB, kSCols, CU_TENSOR_MAP_SWIZZLE_NONE);
-  }
+  if (ok)
+    ok = tensor_map_2d(&tb, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, p.B, p.N, p.K,
+                       row_stride_bytes(p.sbk, p.N, p.K), NB, kSCols, CU_TENSOR_MAP_SWIZZLE_NONE);
   if (!ok) return HML_STATUS_CUDA_ERROR;
 
   const int strips = (p.M + kSRows - 1) / kSRows;
-  const int kblocks = (p.K + kSCols - 1) / kSCols;
-  const long long units = static_cast<long long>(strips) * kblocks;
-  const int ctas =
-      static_cast<int>(std::min<long long>(units, kSCtasPerSm * sm_count()));
   StreamArgs args;
   args.p = p;
-  args.kblocks = kblocks;
-  args.units = units;
+  args.kblocks = (p.K + kSCols - 1) / kSCols;
+  args.units = static_cast<long long>(strips) * args.kblocks;
   args.stages = c.stages;
   args.err = device_error_word();
-  void *ws = nullptr;
-  hml_status st = workspace(static_cast<size_t>(ctas) * 2 * kSRows * NB * sizeof(float), s, &ws);
+  args.partial = partial;
+  hml_status st = tile_counters(static_cast<size_t>(strips), s, &args.arrivals);
   if (st != HML_STATUS_SUCCESS) return st;
-  st = tile_counters(static_cast<size_t>(strips), s, &args.arrivals);
-  if (st != HML_STATUS_SUCCESS) return st;
-  args.partial = static_cast<float *>(ws);
-  e = launch_k(kern, dim3(ctas), dim3(kSThreads), smem, s, 1, ta, tb, args);
+  e = launch_k_ex(kern, dim3(ctas), dim3(kSThreads), smem, s, 1, early, ta, tb, args);
   note_cuda_error(e, "stream launch");
   return cuda_status(e);
+}
+
+// K-contiguous B is first copied N-contiguous ([K][NB], in the workspace
+// after the partial-sum slots) and the N-contiguous kernel runs on the copy.
+template <int NB>
+hml_status run_stream(const GemmProblem &p, const hml_sgemm_config &c, cudaStream_t s) {
+  const int strips = (p.M + kSRows - 1) / kSRows;
+  const long long units = static_cast<long long>(strips) * ((p.K + kSCols - 1) / kSCols);
+  const int ctas = static_cast<int>(std::min<long long>(units, kSCtasPerSm * sm_count()));
+  const size_t part_bytes = static_cast<size_t>(ctas) * 2 * kSRows * NB * sizeof(float);
+  const bool copy_b = p.b_kcontig();
+  const size_t copy_bytes = copy_b ? static_cast<size_t>(p.K) * NB * sizeof(float) : 0;
+  void *ws = nullptr;
+  hml_status st = workspace(part_bytes + copy_bytes, s, &ws);
+  if (st != HML_STATUS_SUCCESS) return st;
+  float *partial = static_cast<float *>(ws);
+  if (!copy_b) return launch_stream_kernel<NB>(p, c, partial, ctas, false, s);
+  float *bcopy = partial + part_bytes / sizeof(float);
+  const int blocks = static_cast<int>(std::min<int64_t>((p.K + 255) / 256, 4 * sm_count()));
+  count_launch();
+  gather_b_kernel<<<blocks, 256, 0, s>>>(p.B, p.sbk, p.sbn, p.K, p.N, bcopy, NB);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) {
+    note_cuda_error(e, "stream B copy");
+    return HML_STATUS_CUDA_ERROR;
+  }
+  GemmProblem q = p;
+  q.B = bcopy;
+  q.sbk = NB;
+  q.sbn = 1;
+  return launch_stream_kernel<NB>(q, c, partial, ctas, true, s);
 }
 
 }  // namespace
@@ -401,9 +429,9 @@ int stream_max_stages(int nb) {
 
 // tile_m 128, tile_n = NB in {4, 8} (N <= NB), split_k 1 (the balance across
 // SMs is built in), stages 2.. ring slots within the shared memory of 2 CTAs
-// per SM.  A needs contiguous
-// columns (sam == 1), 16-byte aligned with lda a multiple of 4; B 16-byte
-// aligned with ldb a multiple of 4, either order.
+// per SM.  A needs contiguous columns (sam == 1), 16-byte aligned with lda a
+// multiple of 4.  B: K-contiguous with any leading dimension (it is copied
+// first), or N-contiguous, 16-byte aligned with ldb a multiple of 4.
 hml_status check_stream(const GemmProblem &p, const hml_sgemm_config &c) {
   const int i = nb_index(c.tile_n);
   if (i < 0 || c.tile_m != kSRows || c.split_k != 1) return HML_STATUS_INVALID_VALUE;
@@ -414,21 +442,21 @@ hml_status check_stream(const GemmProblem &p, const hml_sgemm_config &c) {
   if (p.sam != 1 || p.a_kcontig()) return HML_STATUS_NOT_SUPPORTED;
   if (!(p.b_kcontig() || p.sbn == 1)) return HML_STATUS_NOT_SUPPORTED;
   const int64_t sa = row_stride_bytes(p.sak, p.M, p.K);
-  const int64_t sb = p.b_kcontig() ? row_stride_bytes(p.sbn, p.K, p.N)
-                                   : row_stride_bytes(p.sbk, p.N, p.K);
-  if (!aligned16(p.A) || !aligned16(p.B) || sa % 16 != 0 || sb % 16 != 0)
-    return HML_STATUS_NOT_SUPPORTED;
-  if (sa >= (int64_t(1) << 40) || sb >= (int64_t(1) << 40)) return HML_STATUS_NOT_SUPPORTED;
+  if (!aligned16(p.A) || sa % 16 != 0 || sa >= (int64_t(1) << 40)) return HML_STATUS_NOT_SUPPORTED;
+  if (!p.b_kcontig()) {
+    const int64_t sb = row_stride_bytes(p.sbk, p.N, p.K);
+    if (!aligned16(p.B) || sb % 16 != 0 || sb >= (int64_t(1) << 40))
+      return HML_STATUS_NOT_SUPPORTED;
+  }
   return HML_STATUS_SUCCESS;
 }
 
 hml_status launch_stream(const GemmProblem &p, const hml_sgemm_config &c, cudaStream_t s) {
   hml_status st = check_stream(p, c);
   if (st != HML_STATUS_SUCCESS) return st;
-  const bool bk = p.b_kcontig();
   switch (c.tile_n) {
-    case 4: return bk ? run_stream<4, true>(p, c, s) : run_stream<4, false>(p, c, s);
-    case 8: return bk ? run_stream<8, true>(p, c, s) : run_stream<8, false>(p, c, s);
+    case 4: return run_stream<4>(p, c, s);
+    case 8: return run_stream<8>(p, c, s);
     default: return HML_STATUS_INVALID_VALUE;
   }
 }

@@ -43,13 +43,17 @@ LAYOUTS = [(0, 0, 0), (1, 1, 1), (0, 0, 1), (1, 1, 0)]
 @pytest.mark.parametrize("layout", LAYOUTS)
 @pytest.mark.parametrize("nb", [4, 8])
 def test_stream_layouts_and_ragged_shapes(cuda, layout, nb):
-    """TMA needs leading dimensions that are multiples of 4 floats: M and K
-    are, and N is too where B is stored N-contiguous (ldb = N)."""
+    """TMA needs A's leading dimension a multiple of 4 floats (M is), and
+    B's too where B is stored N-contiguous (ldb = N).  A K-contiguous B is
+    copied N-contiguous first, so any ldb works there (K = 333)."""
     order, ta, tb = layout
     cfg = cfg_for(nb)
     b_ncontig = layout in ((0, 0, 1), (1, 1, 0))
     ns = sorted({4, nb}) if b_ncontig else sorted({1, max(1, nb // 2 - 1), nb})
-    for (M, K) in ((1000, 332), (128, 32), (132, 4), (4100, 1000)):
+    shapes = [(1000, 332), (128, 32), (132, 4), (4100, 1000)]
+    if not b_ncontig:
+        shapes.append((1000, 333))
+    for (M, K) in shapes:
         for N in ns:
             got, D, absD = run_case(M, N, K, order, ta, tb, 0.75, -0.5, config=cfg)
             assert_within_fp32_bound(got, D, absD, max(K, 1), what=f"{cfg} {layout} {M}x{N}x{K}")
