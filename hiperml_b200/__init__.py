@@ -8,7 +8,8 @@ fallback for any entry point.
 from ._lib import HmlError, SgemmConfig, lib  # noqa: F401  (loads the .so)
 from .api import (  # noqa: F401
     ALGO_AUTO, ALGO_BF16X3, ALGO_BF16X6, ALGO_SIMT, ALGO_TF32X3, COL_MAJOR, OP_N, OP_T, ROW_MAJOR,
-    config_check, configs, device_error, error_fp64, fill_random, hmlSgemm, hmlSgemmBasic,
+    check_wait_limit, config_check, configs, device_error, error_fp64, fill_random, hmlSgemm,
+    hmlSgemmBasic,
     hmlSgemmKernelConfig, hmlSgemv, hmlSgemvBasic, hmlSgemvKernelConfig, select, select_algo, sgemm,
     sgemm_ex, sgemv_ex, autotune, tune_save, tune_load, tune_clear, set_math_mode, MATH_FP32,
     MATH_FAST, BatchPlan, gemm_descs, sgemm_batched, batch_problem_config)

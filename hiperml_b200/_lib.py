@@ -95,6 +95,7 @@ _SIGS = {
                                      c_int, c_void_p, c_int, c_float, c_void_p, c_void_p, c_int,
                                      ctypes.POINTER(c_double), c_void_p]),
     "hml_device_error": (c_int, [c_int_p]),
+    "hml_check_wait_limit": (c_int, [c_void_p]),
     "hml_release_resources": (c_int, []),
     "hml_launch_count": (c_uint64, []),
     "hml_autotune_sgemm": (c_int, [c_int, c_int, c_int, c_int, c_int, c_int, ctypes.c_uint32,

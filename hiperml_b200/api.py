@@ -224,6 +224,11 @@ def device_error() -> int:
     return code.value
 
 
+def check_wait_limit(stream=None) -> None:
+    """``hml_check_wait_limit``: a kernel whose bounded wait expires."""
+    check(lib.hml_check_wait_limit(_stream(stream)), "hml_check_wait_limit")
+
+
 # ------------------------------------------------------------- autotuning
 MATH_FP32, MATH_FAST = 0, 1
 

@@ -366,6 +366,10 @@ hml_status hml_device_error(int *code) {
   return cuda_status(e);
 }
 
+hml_status hml_check_wait_limit(void *stream) {
+  return check_wait_limit(static_cast<cudaStream_t>(stream));
+}
+
 hml_status hml_release_resources(void) { return release_all(); }
 
 uint64_t hml_launch_count(void) { return launch_count(); }

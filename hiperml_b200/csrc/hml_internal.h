@@ -82,6 +82,9 @@ hml_sgemm_config tc_batch_config(const GemmProblem &p);
 int tc_batch_items(const TcBatch *b);
 int tc_batch_ctas(const TcBatch *b);
 
+// Launches a kernel whose bounded wait expires (verify.cu).
+hml_status check_wait_limit(cudaStream_t s);
+
 // Per-device resources.
 int *device_error_word();  // nullptr on failure
 hml_status workspace(size_t bytes, cudaStream_t s, void **ptr);

@@ -148,7 +148,31 @@ __global__ void err_kernel(GemmProblem p, const double *D, const double *Dabs, d
   }
 }
 
+// A wait that nothing ends: thread 0 waits on an mbarrier no thread arrives
+// on, with the bounded wait of every kernel of the library; it gives up
+// after the limit, records the full-barrier code in the device error word
+// and returns, leaving the context usable.
+__global__ void expired_wait_kernel(int *err) {
+  __shared__ uint64_t bar;
+  if (threadIdx.x == 0) {
+    mbar_init(&bar, 1);
+    fence_mbar_init();
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) mbar_wait(&bar, 0, err, kDevErrFullBarrier);
+}
+
 }  // namespace
+
+hml_status check_wait_limit(cudaStream_t s) {
+  int *err = device_error_word();
+  if (!err) return HML_STATUS_ALLOC_FAILED;
+  count_launch();
+  expired_wait_kernel<<<1, 32, 0, s>>>(err);
+  cudaError_t e = cudaGetLastError();
+  note_cuda_error(e, "expired wait");
+  return cuda_status(e);
+}
 
 hml_status fill_random(float *out, size_t n, uint64_t seed, uint64_t stream_id, int dist,
                        cudaStream_t s) {

@@ -398,6 +398,14 @@ hml_status hml_sgemm_error_fp64(hml_order order, hml_op transA, hml_op transB,
 /* Device-side error word of bounded waits: 0 when clear.  Reading clears. */
 hml_status hml_device_error(int *code);
 
+/* Failure-path check: launches a kernel whose one waiting thread waits on a
+ * barrier that nothing completes.  The bounded wait every kernel of this
+ * library uses gives up after its limit (2 s), writes code 1 (a tile that
+ * never landed) to the device error word and returns, so the device stays
+ * usable; hml_device_error then reports the code.  No counterpart in the
+ * reference, whose kernels have no waits. */
+hml_status hml_check_wait_limit(void *stream);
+
 /* Number of kernels the library has launched since it was loaded. */
 uint64_t hml_launch_count(void);
 
