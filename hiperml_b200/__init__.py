@@ -11,7 +11,7 @@ from .api import (  # noqa: F401
     check_wait_limit, config_check, configs, device_error, error_fp64, fill_random, hmlSgemm,
     hmlSgemmBasic,
     hmlSgemmKernelConfig, hmlSgemv, hmlSgemvBasic, hmlSgemvKernelConfig, select, select_algo, sgemm,
-    sgemm_ex, sgemv_ex, autotune, tune_save, tune_load, tune_clear, set_math_mode, MATH_FP32,
-    MATH_FAST, BatchPlan, gemm_descs, sgemm_batched, batch_problem_config)
+    sgemm_ex, sgemv_ex, autotune, autotune_sgemv, sgemv_select, tune_save, tune_load, tune_clear,
+    set_math_mode, MATH_FP32, MATH_FAST, BatchPlan, gemm_descs, sgemm_batched, batch_problem_config)
 
 __version__ = lib.hml_version().decode()

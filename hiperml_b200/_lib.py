@@ -43,6 +43,12 @@ class TuneEntry(ctypes.Structure):
     _fields_ = [("config", SgemmConfig), ("time_us", ctypes.c_float), ("status", ctypes.c_int32)]
 
 
+class SgemvTuneEntry(ctypes.Structure):
+    """``hml_sgemv_tune_entry``."""
+    _fields_ = [("variant", ctypes.c_int32), ("time_us", ctypes.c_float),
+                ("status", ctypes.c_int32)]
+
+
 class GemmDesc(ctypes.Structure):
     """``hml_gemm_desc``: one problem of a batch (device pointers)."""
     _fields_ = [("transA", ctypes.c_int32), ("transB", ctypes.c_int32), ("M", ctypes.c_int32),
@@ -100,6 +106,9 @@ _SIGS = {
     "hml_launch_count": (c_uint64, []),
     "hml_autotune_sgemm": (c_int, [c_int, c_int, c_int, c_int, c_int, c_int, ctypes.c_uint32,
                                    c_int, ctypes.POINTER(TuneEntry), c_int, c_int_p, c_void_p]),
+    "hml_autotune_sgemv": (c_int, [c_int, c_int, c_int, c_int, c_int,
+                                   ctypes.POINTER(SgemvTuneEntry), c_int, c_int_p, c_void_p]),
+    "hml_sgemv_select": (c_int, [c_int, c_int, c_int, c_int, c_int, c_int_p]),
     "hml_tune_save": (c_int, [c_char_p]),
     "hml_tune_load": (c_int, [c_char_p, c_int_p]),
     "hml_tune_clear": (c_int, []),

@@ -18,7 +18,7 @@ from typing import Optional
 
 import numpy as np
 
-from ._lib import GemmDesc, SgemmConfig, TuneEntry, check, lib
+from ._lib import GemmDesc, SgemmConfig, SgemvTuneEntry, TuneEntry, check, lib
 
 COL_MAJOR, ROW_MAJOR = 0, 1
 OP_N, OP_T = 0, 1
@@ -244,6 +244,28 @@ def autotune(order, transA, transB, M, N, K, families=0, reps=5, stream=None):
                                 ctypes.byref(n), _stream(stream))
     check(st, "hml_autotune_sgemm")
     return [(ents[i].config, ents[i].time_us, ents[i].status) for i in range(n.value)]
+
+
+def autotune_sgemv(order, trans, M, N, reps=5, stream=None):
+    """Measure every variant of the SGEMV kernel for this layout on an M x N
+    problem (``hml_autotune_sgemv``).  Returns a list of (variant, time_us,
+    status); the fastest is recorded in the library's tuned table."""
+    ents = (SgemvTuneEntry * 32)()
+    n = ctypes.c_int()
+    st = lib.hml_autotune_sgemv(order, trans, M, N, reps, ents, 32, ctypes.byref(n),
+                                _stream(stream))
+    check(st, "hml_autotune_sgemv")
+    return [(ents[i].variant, ents[i].time_us, ents[i].status) for i in range(n.value)]
+
+
+def sgemv_select(order, trans, M, N, lda=None) -> int:
+    """The variant ``hml_sgemv_ex`` runs this problem with: the tuned table's,
+    or 0 when the heuristic decides (``hml_sgemv_select``)."""
+    if lda is None:
+        lda = max(1, M if order == COL_MAJOR else N)
+    v = ctypes.c_int()
+    check(lib.hml_sgemv_select(order, trans, M, N, lda, ctypes.byref(v)), "hml_sgemv_select")
+    return v.value
 
 
 def tune_save(path: str) -> None:

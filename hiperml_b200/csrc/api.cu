@@ -229,7 +229,7 @@ hml_status hml_sgemm_ex(hml_order order, hml_op transA, hml_op transB, int M, in
   if (p.M == 0 || p.N == 0) return HML_STATUS_SUCCESS;
   if (p.K == 0 || p.alpha == 0.0f) return launch_scale(p.C, p.M, p.N, p.scm, p.scn, p.beta, s);
   GemvProblem g;
-  if (as_gemv(p, &g)) return launch_gemv(g, 0, s);
+  if (as_gemv(p, &g)) return launch_gemv(g, kGemvTuned, s);
   hml_sgemm_config c;
   st = select_config(p, &c, s);
   if (st != HML_STATUS_SUCCESS) return st;
@@ -322,7 +322,21 @@ hml_status hml_sgemv_ex(hml_order order, hml_op trans, int M, int N, float alpha
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   if (g.P == 0) return HML_STATUS_SUCCESS;
   if (g.Q == 0 || g.alpha == 0.0f) return launch_scale(g.y, g.P, 1, g.incy, 0, g.beta, s);
-  return launch_gemv(g, 0, s);
+  return launch_gemv(g, kGemvTuned, s);
+}
+
+hml_status hml_sgemv_select(hml_order order, hml_op trans, int M, int N, int lda, int *variant) {
+  if (!variant) return HML_STATUS_INVALID_VALUE;
+  GemvProblem g;
+  float y = 0.0f;  // only the layout is read
+  hml_status st = gemv_from_blas(order, trans, M, N, 0.0f, nullptr, lda, nullptr, 0.0f, &y, &g);
+  if (st != HML_STATUS_SUCCESS) return st;
+  int v = 0;
+  *variant = g.P > 0 && g.Q > 0 && gemv_tuned_lookup(g, &v) &&
+                     gemv_variant_valid(gemv_rows_layout(g), v)
+                 ? v
+                 : 0;
+  return HML_STATUS_SUCCESS;
 }
 
 hml_status hml_sgemv_ex_variant(hml_order order, hml_op trans, int M, int N, float alpha,
@@ -334,6 +348,7 @@ hml_status hml_sgemv_ex_variant(hml_order order, hml_op trans, int M, int N, flo
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   if (g.P == 0) return HML_STATUS_SUCCESS;
   if (g.Q == 0 || g.alpha == 0.0f) return launch_scale(g.y, g.P, 1, g.incy, 0, g.beta, s);
+  if (variant < 0) return HML_STATUS_INVALID_VALUE;
   return launch_gemv(g, variant, s);
 }
 

@@ -24,6 +24,7 @@
 
 #include "hml_device.cuh"
 #include "hml_internal.h"
+#include "hml_tune.h"
 
 namespace hml {
 namespace {
@@ -117,7 +118,7 @@ __global__ void __launch_bounds__(kThreads) gemv_rows_kernel(GemvProblem p) {
 constexpr int kColRows = 256;
 constexpr int kColPhases = kThreads / 32 / 2;
 constexpr int kColUnroll = 8;
-constexpr int kMaxColSplit = 16;
+constexpr int kMaxColSplit = kGemvMaxColSplit;
 static_assert(kColRows == kThreads, "thread i finalises row i of the tile");
 
 template <bool VEC>
@@ -267,11 +268,16 @@ bool aligned16(const void *ptr) { return (reinterpret_cast<uintptr_t>(ptr) & 15u
 
 // variant for the row kernel: threads per row (4..256), 0 = heuristic.
 // variant for the column kernel: CTAs per 256-row tile along the columns
-// (1..16), 0 = heuristic.
+// (1..16), 0 = heuristic.  kGemvTuned: the measured table's variant for this
+// shape when it holds one, else the heuristic.
 hml_status launch_gemv(const GemvProblem &p, int variant, cudaStream_t s) {
   if (p.P == 0) return HML_STATUS_SUCCESS;
   if (p.sq != 1 && p.sp != 1) return HML_STATUS_NOT_SUPPORTED;
-  if (p.sq == 1 && !(p.Q == 1 && p.sp == 1)) {
+  if (variant == kGemvTuned) {
+    int v = 0;
+    variant = gemv_tuned_lookup(p, &v) && gemv_variant_valid(gemv_rows_layout(p), v) ? v : 0;
+  }
+  if (gemv_rows_layout(p)) {
     const bool vec = aligned16(p.A) && (p.sp % 4 == 0 || p.P == 1) && p.incx == 1 &&
                      aligned16(p.x);
     int tpr = variant;

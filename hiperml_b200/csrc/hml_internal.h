@@ -51,7 +51,21 @@ hml_status gemv_from_blas(hml_order order, hml_op trans, int M, int N, float alp
                           GemvProblem *out);
 
 // Kernels (one launcher per family).  All are stream ordered.
+// launch_gemv's variant: threads per row (4..256, powers of two) when the
+// rows of A are contiguous, CTAs per 256-row tile (1..kGemvMaxColSplit) when
+// the columns are; 0 = the heuristic; kGemvTuned = the autotuner's measured
+// table, else the heuristic.
+constexpr int kGemvTuned = -1;
+constexpr int kGemvMaxColSplit = 16;
 hml_status launch_gemv(const GemvProblem &p, int variant, cudaStream_t s);
+// Which GEMV kernel serves p: the row kernel (rows of A contiguous) or the
+// column kernel.
+inline bool gemv_rows_layout(const GemvProblem &p) {
+  return p.sq == 1 && !(p.Q == 1 && p.sp == 1);
+}
+inline bool gemv_variant_valid(bool rows, int v) {
+  return rows ? (v >= 4 && v <= 256 && (v & (v - 1)) == 0) : (v >= 1 && v <= kGemvMaxColSplit);
+}
 hml_status launch_scale(float *C, int M, int N, int64_t scm, int64_t scn, float beta,
                         cudaStream_t s);
 hml_status launch_simt(const GemmProblem &p, const hml_sgemm_config &c, cudaStream_t s);

@@ -14,4 +14,7 @@ bool tuned_lookup(const GemmProblem &p, hml_sgemm_config *c);
 // stream under capture is not made to wait.
 bool predictor_lookup(const GemmProblem &p, hml_sgemm_config *c, cudaStream_t s);
 int math_mode();
+// The GEMV variant the measured table holds for this problem (its shape or
+// a neighbour within about a factor 2 with the same layout); false when none.
+bool gemv_tuned_lookup(const GemvProblem &p, int *variant);
 }  // namespace hml

@@ -201,10 +201,11 @@ hml_status host_sgemv(int variant, float *y, const float *A, const float *x, int
   return HML_STATUS_SUCCESS;
 }
 
-// threads per row of the GEMV row kernel from a reference v1 SGEMV rule
+// threads per row of the GEMV row kernel from a reference v1 SGEMV rule;
+// without one, the measured table's variant (else the heuristic)
 int sgemv_variant_for(int N) {
   int type, bs, rs;
-  if (!cfg_v1_sgemv_rule(N, &type, &bs, &rs)) return 0;
+  if (!cfg_v1_sgemv_rule(N, &type, &bs, &rs)) return kGemvTuned;
   int tpr = 4;
   while (tpr < 256 && tpr < 16 * bs) tpr <<= 1;
   return tpr;
@@ -241,7 +242,8 @@ hml_status config_file(int kind, const char *path) {
   const bool got = fgets(head, sizeof head, f) != nullptr;
   fclose(f);
   int n = 0;
-  if (kind == 0 && got && strncmp(head, "#HML-B200 tuning v2", 19) == 0) return tune_load(path, &n);
+  // this library's measured table holds SGEMM and SGEMV records alike
+  if (got && strncmp(head, "#HML-B200 tuning v2", 19) == 0) return tune_load(path, &n);
   return cfg_v1_load(kind, path, &n);
 }
 

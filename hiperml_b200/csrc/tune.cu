@@ -12,10 +12,20 @@
 // configuration allowed by the math mode is recorded in the tuned table that
 // hml_sgemm_ex consults first.
 //
+// The GEMV half (hml_autotune_sgemv) replaces the reference's SGEMV tuner
+// (hmlSgemvKernelConfigOnline, src/hml_sgemv_kernel.cu:391-633), which
+// timed its kernel types per N class on the host clock: here every variant
+// of the kernel that serves the problem's layout (threads per row, or CTAs
+// per column tile) is timed the same way as the SGEMM configurations and the
+// fastest is recorded in a second table that hml_sgemv_ex consults first.
+//
 // Tuned-table file, "#HML-B200 tuning v2":
 //   # device <name> sms <n>
 //   akc bkc M N K : algo tile_m tile_n split_k stages variant time_us
-// (akc/bkc: whether A / B are K-contiguous in the canonical long-M form).
+//   v cols P Q : variant time_us
+// (akc/bkc: whether A / B are K-contiguous in the canonical long-M form;
+// a "v" record is a GEMV: cols = 1 when the columns of A are contiguous,
+// P = length of y, Q = length of x).
 #include <dlfcn.h>
 
 #include <algorithm>
@@ -49,8 +59,21 @@ struct Rec {
   float us;
 };
 
+// GEMV records: layout (0 = rows of A contiguous, 1 = columns), P, Q
+struct GKey {
+  int cols, P, Q;
+  bool operator<(const GKey &o) const {
+    return std::tie(cols, P, Q) < std::tie(o.cols, o.P, o.Q);
+  }
+};
+struct GRec {
+  int variant;
+  float us;
+};
+
 std::mutex g_mu;
 std::map<Key, Rec> g_table;
+std::map<GKey, GRec> g_gemv_table;
 int g_math_mode = HML_MATH_FP32;
 bool g_default_tried = false;  // the shipped table was loaded or ruled out
 
@@ -59,6 +82,8 @@ Key key_of(const GemmProblem &p) {
 }
 
 bool allowed(int algo) { return algo != HML_ALGO_BF16X3 || g_math_mode == HML_MATH_FAST; }
+
+GKey gkey_of(const GemvProblem &p) { return GKey{gemv_rows_layout(p) ? 0 : 1, p.P, p.Q}; }
 
 }  // namespace
 
@@ -128,11 +153,42 @@ bool tuned_lookup(const GemmProblem &p, hml_sgemm_config *c) {
   return true;
 }
 
+bool gemv_tuned_lookup(const GemvProblem &p, int *variant) {
+  load_default_table();
+  std::lock_guard<std::mutex> lk(g_mu);
+  if (g_gemv_table.empty()) return false;
+  const GKey k = gkey_of(p);
+  auto it = g_gemv_table.find(k);
+  if (it != g_gemv_table.end()) {
+    *variant = it->second.variant;
+    return true;
+  }
+  // nearest measured shape of the same layout in log space, within about a
+  // factor 2 in one dimension (the split of the column kernel follows the
+  // number of row tiles, the row kernel's threads per row the row length)
+  double best = 1e300;
+  const GRec *pick = nullptr;
+  for (const auto &kv : g_gemv_table) {
+    if (kv.first.cols != k.cols) continue;
+    const double dp = std::log2(double(kv.first.P) / k.P);
+    const double dq = std::log2(double(kv.first.Q) / k.Q);
+    const double d = dp * dp + dq * dq;
+    if (d < best) {
+      best = d;
+      pick = &kv.second;
+    }
+  }
+  if (!pick || best > 1.0) return false;
+  *variant = pick->variant;
+  return true;
+}
+
 hml_status tune_load(const char *path, int *records) {
   FILE *f = fopen(path, "rb");
   if (!f) return HML_STATUS_IO_ERROR;
   char line[512];
   std::map<Key, Rec> t;
+  std::map<GKey, GRec> gt;
   int n = 0, lineno = 0;
   bool header = false;
   while (fgets(line, sizeof line, f)) {
@@ -143,6 +199,20 @@ hml_status tune_load(const char *path, int *records) {
       continue;
     }
     if (line[0] == '#' || line[0] == '\n') continue;
+    if (line[0] == 'v') {
+      GKey g;
+      GRec r;
+      if (sscanf(line, "v %d %d %d : %d %f", &g.cols, &g.P, &g.Q, &r.variant, &r.us) != 5 ||
+          g.cols < 0 || g.cols > 1 || g.P < 1 || g.Q < 1 ||
+          !gemv_variant_valid(g.cols == 0, r.variant)) {
+        fclose(f);
+        fprintf(stderr, "hml: %s:%d: bad GEMV tuning record: %s", path, lineno, line);
+        return HML_STATUS_CONFIG_ERROR;
+      }
+      gt[g] = r;
+      ++n;
+      continue;
+    }
     Key k;
     hml_sgemm_config c;
     float us;
@@ -172,6 +242,7 @@ hml_status tune_load(const char *path, int *records) {
   std::lock_guard<std::mutex> lk(g_mu);
   g_default_tried = true;  // an explicit table replaces the shipped one
   for (auto &kv : t) g_table[kv.first] = kv.second;
+  for (auto &kv : gt) g_gemv_table[kv.first] = kv.second;
   if (records) *records = n;
   return HML_STATUS_SUCCESS;
 }
@@ -199,6 +270,10 @@ hml_status tune_save(const char *path) {
     fprintf(f, "%d %d %d %d %d : %d %d %d %d %d %d %.3f\n", k.akc, k.bkc, k.M, k.N, k.K, c.algo,
             c.tile_m, c.tile_n, c.split_k, c.stages, c.variant, kv.second.us);
   }
+  if (!g_gemv_table.empty()) fprintf(f, "# v cols P Q : variant time_us\n");
+  for (const auto &kv : g_gemv_table)
+    fprintf(f, "v %d %d %d : %d %.3f\n", kv.first.cols, kv.first.P, kv.first.Q,
+            kv.second.variant, kv.second.us);
   const bool ok = fflush(f) == 0;
   fclose(f);
   return ok ? HML_STATUS_SUCCESS : HML_STATUS_IO_ERROR;
@@ -333,16 +408,101 @@ hml_status autotune(hml_order order, hml_op ta, hml_op tb, int M, int N, int K,
   return best < 1e30f ? HML_STATUS_SUCCESS : HML_STATUS_NOT_SUPPORTED;
 }
 
+hml_status autotune_gemv(hml_order order, hml_op trans, int M, int N, int reps,
+                         hml_sgemv_tune_entry *entries, int max_entries, int *n_entries,
+                         cudaStream_t s) {
+  if (n_entries) *n_entries = 0;
+  if (M < 1 || N < 1 || reps < 1 || reps > 50 || (order != HML_ROW_MAJOR && order != HML_COL_MAJOR) ||
+      (trans != HML_OP_N && trans != HML_OP_T))
+    return HML_STATUS_INVALID_VALUE;
+  const bool cm = order == HML_COL_MAJOR;
+  // A stored M x N with its leading dimension rounded up to 16 bytes
+  const int lda = (cm ? M : N) + 3 - ((cm ? M : N) + 3) % 4;
+  const size_t a_lines = cm ? N : M;
+  const size_t nx = trans == HML_OP_N ? N : M;
+  const size_t ny = trans == HML_OP_N ? M : N;
+  std::lock_guard<std::mutex> lk(g_mu);
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (g_bufs.dev != dev) {
+    g_bufs = TuneBufs();
+    g_bufs.dev = dev;
+  }
+  hml_status st;
+  if ((st = grow(&g_bufs.A, &g_bufs.nA, a_lines * lda, s, 101)) != HML_STATUS_SUCCESS ||
+      (st = grow(&g_bufs.B, &g_bufs.nB, nx, s, 102)) != HML_STATUS_SUCCESS ||
+      (st = grow(&g_bufs.C, &g_bufs.nC, ny, s, 103)) != HML_STATUS_SUCCESS ||
+      (st = grow(&g_bufs.flush, &g_bufs.nflush, size_t(64) << 20, s, 104)) != HML_STATUS_SUCCESS)
+    return st;
+  GemvProblem g;
+  st = gemv_from_blas(order, trans, M, N, 1.0f, g_bufs.A, lda, g_bufs.B, 0.0f, g_bufs.C, &g);
+  if (st != HML_STATUS_SUCCESS) return st;
+  const bool rows = gemv_rows_layout(g);
+  std::vector<int> variants;
+  if (rows)
+    for (int v = 4; v <= 256; v <<= 1) variants.push_back(v);
+  else
+    for (int v = 1; v <= kGemvMaxColSplit; ++v) variants.push_back(v);
+  cudaEvent_t e0, e1;
+  if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess)
+    return HML_STATUS_CUDA_ERROR;
+  const size_t flush_bytes = g_bufs.nflush * sizeof(float);
+  const bool need_flush = static_cast<size_t>(M) * N * 4 < size_t(200) << 20;
+  int count = 0;
+  float best = 1e30f;
+  int best_v = 0;
+  for (int v : variants) {
+    hml_sgemv_tune_entry ent;
+    ent.variant = v;
+    ent.time_us = -1.0f;
+    ent.status = launch_gemv(g, v, s);  // warm-up
+    std::vector<float> ts;
+    for (int r = 0; r < reps && ent.status == HML_STATUS_SUCCESS; ++r) {
+      if (need_flush) cudaMemsetAsync(g_bufs.flush, r & 0xff, flush_bytes, s);
+      cudaEventRecord(e0, s);
+      ent.status = launch_gemv(g, v, s);
+      cudaEventRecord(e1, s);
+      if (cudaEventSynchronize(e1) != cudaSuccess) {
+        ent.status = HML_STATUS_CUDA_ERROR;
+        break;
+      }
+      float ms = 0.0f;
+      cudaEventElapsedTime(&ms, e0, e1);
+      ts.push_back(ms * 1000.0f);
+      if (ts.size() == 1 && ts[0] > 4.0f * best) break;
+    }
+    if (ent.status == HML_STATUS_SUCCESS && !ts.empty()) {
+      std::sort(ts.begin(), ts.end());
+      ent.time_us = ts[ts.size() / 2];
+      if (ent.time_us < best) {
+        best = ent.time_us;
+        best_v = v;
+      }
+    } else if (ent.status == HML_STATUS_SUCCESS) {
+      ent.status = HML_STATUS_CUDA_ERROR;
+    }
+    cudaGetLastError();
+    if (entries && count < max_entries) entries[count] = ent;
+    ++count;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (n_entries) *n_entries = std::min(count, max_entries);
+  if (best < 1e30f) g_gemv_table[gkey_of(g)] = GRec{best_v, best};
+  return best < 1e30f ? HML_STATUS_SUCCESS : HML_STATUS_CUDA_ERROR;
+}
+
 hml_status tune_clear() {
   std::lock_guard<std::mutex> lk(g_mu);
   g_table.clear();
+  g_gemv_table.clear();
   g_default_tried = true;  // cleared means empty: the shipped table stays out
   return HML_STATUS_SUCCESS;
 }
 
 int tune_size() {
   std::lock_guard<std::mutex> lk(g_mu);
-  return static_cast<int>(g_table.size());
+  return static_cast<int>(g_table.size() + g_gemv_table.size());
 }
 
 hml_status set_math_mode(int mode) {
@@ -360,6 +520,13 @@ hml_status hml_autotune_sgemm(hml_order order, hml_op transA, hml_op transB, int
                               int max_entries, int *n_entries, void *stream) {
   return hml::autotune(order, transA, transB, M, N, K, families, reps, entries, max_entries,
                        n_entries, static_cast<cudaStream_t>(stream));
+}
+
+hml_status hml_autotune_sgemv(hml_order order, hml_op trans, int M, int N, int reps,
+                              hml_sgemv_tune_entry *entries, int max_entries, int *n_entries,
+                              void *stream) {
+  return hml::autotune_gemv(order, trans, M, N, reps, entries, max_entries, n_entries,
+                            static_cast<cudaStream_t>(stream));
 }
 
 hml_status hml_tune_save(const char *path) {

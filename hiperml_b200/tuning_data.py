@@ -20,6 +20,10 @@ files): the autotuner's measured best configuration, among the FP32-accurate
 families, for each of the library's reference workload shapes:
 
     python -m hiperml_b200.tuning_data --table hiperml_b200/data/tuned_b200.txt
+
+The table also holds the measured best SGEMV variant of the reference
+workloads' SGEMV shapes (``hml_autotune_sgemv``); ``--gemv-only`` re-measures
+just those and keeps the SGEMM records.
 """
 from __future__ import annotations
 
@@ -96,16 +100,37 @@ TABLE_SHAPES = ((4096, 16, 4096, 0, 0), (65536, 8, 4096, 0, 0), (65536, 32, 4096
                 (65536, 64, 4096, 0, 0), (65536, 128, 4096, 0, 0), (8192, 8192, 8192, 0, 0))
 
 
-def make_table(path, shapes=TABLE_SHAPES, reps: int = 5) -> None:
+# The reference workloads' SGEMV shapes (order, trans, M, N): the column-major
+# 32768 x 4096 A applied as A x (column kernel) and as A^T x (row kernel).
+GEMV_TABLE_SHAPES = ((0, 0, 32768, 4096), (0, 1, 32768, 4096))
+
+
+def make_gemv_records(shapes=GEMV_TABLE_SHAPES, reps: int = 9) -> None:
+    """Autotunes the SGEMV variants of each shape into the current table."""
+    from . import api
+    for (order, trans, M, N) in shapes:
+        ents = api.autotune_sgemv(order, trans, M, N, reps=reps)
+        t, v = min((t, v) for v, t, st in ents if st == 0 and t > 0)
+        print(f"SGEMV order={order} trans={trans} M={M} N={N}: variant {v} {t:.1f} us "
+              f"(all: {[(v, round(t, 1)) for v, t, _ in ents]})", flush=True)
+
+
+def make_table(path, shapes=TABLE_SHAPES, reps: int = 5, gemv_only: bool = False) -> None:
     """Autotunes each shape over the FP32-accurate families (SIMT, BF16X6) and
-    saves the resulting tuned table."""
+    each SGEMV shape, and saves the resulting tuned table.  gemv_only: keep
+    the SGEMM records of the table already at `path` and re-measure only the
+    SGEMV ones."""
     from . import api
     api.tune_clear()
-    fams = (1 << api.ALGO_SIMT) | (1 << api.ALGO_BF16X6)
-    for (M, N, K, ta, tb) in shapes:
-        ents = api.autotune(api.COL_MAJOR, ta, tb, M, N, K, families=fams, reps=reps)
-        best = min(((t, c) for c, t, st in ents if st == 0 and t > 0), key=lambda e: e[0])
-        print(f"M={M} N={N} K={K} ta={ta} tb={tb}: {best[1]} {best[0]:.1f} us", flush=True)
+    if gemv_only:
+        api.tune_load(str(path))
+    else:
+        fams = (1 << api.ALGO_SIMT) | (1 << api.ALGO_BF16X6)
+        for (M, N, K, ta, tb) in shapes:
+            ents = api.autotune(api.COL_MAJOR, ta, tb, M, N, K, families=fams, reps=reps)
+            best = min(((t, c) for c, t, st in ents if st == 0 and t > 0), key=lambda e: e[0])
+            print(f"M={M} N={N} K={K} ta={ta} tb={tb}: {best[1]} {best[0]:.1f} us", flush=True)
+    make_gemv_records()
     api.tune_save(str(path))
 
 
@@ -124,6 +149,8 @@ def main(argv=None):
     ap.add_argument("out", nargs="?")
     ap.add_argument("--table", default=None,
                     help="write the tuned table of the reference workload shapes to this file")
+    ap.add_argument("--gemv-only", action="store_true",
+                    help="with --table: keep the file's SGEMM records, re-measure the SGEMV ones")
     ap.add_argument("--count", type=int, default=5000)
     ap.add_argument("--seed", type=int, default=5)
     ap.add_argument("--reps", type=int, default=3)
@@ -136,7 +163,7 @@ def main(argv=None):
                          "and its other columns kept")
     args = ap.parse_args(argv)
     if args.table:
-        make_table(args.table)
+        make_table(args.table, gemv_only=args.gemv_only)
         return 0
     if not args.out:
         ap.error("OUT.npz is required")

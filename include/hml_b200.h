@@ -329,13 +329,40 @@ hml_status hml_sgemv_ex(hml_order order, hml_op trans, int M, int N,
 
 /* Same, forcing a kernel variant: for A with contiguous rows the number of
  * threads that share one row (4, 8, ..., 256); for A with contiguous
- * columns the thread-block-cluster split of the columns (1..8).  0 = the
- * heuristic.  Replaces launching one chosen SGEMV kernel of the reference's
- * repository (hmlSgemvKernelSelect + launch, src/hml_sgemv_kernel.cu:315-355). */
+ * columns the number of CTAs that split the columns of one 256-row tile
+ * (1..16).  0 = the heuristic.  Replaces launching one chosen SGEMV kernel of
+ * the reference's repository (hmlSgemvKernelSelect + launch,
+ * src/hml_sgemv_kernel.cu:315-355). */
 hml_status hml_sgemv_ex_variant(hml_order order, hml_op trans, int M, int N,
                                 float alpha, const float *A, int lda,
                                 const float *x, float beta, float *y,
                                 int variant, void *stream);
+
+/* The variant hml_sgemv_ex runs this problem with: the tuned table's
+ * (*variant > 0), or 0 when the heuristic decides.  Host only, no launch. */
+hml_status hml_sgemv_select(hml_order order, hml_op trans, int M, int N,
+                            int lda, int *variant);
+
+/* One measured SGEMV variant. */
+typedef struct hml_sgemv_tune_entry {
+  int32_t variant; /* as in hml_sgemv_ex_variant                          */
+  float time_us;   /* median device time of one call, -1 when not timed   */
+  int32_t status;  /* hml_status of the trial                             */
+} hml_sgemv_tune_entry;
+
+/* Measures every variant of the SGEMV kernel that serves this layout (7
+ * thread-per-row widths, or 16 column splits) on an M x N problem with the
+ * leading dimension rounded up to a multiple of 4 floats and uniform[-1,1]
+ * operands: one warm-up call, then `reps` calls timed with CUDA events on
+ * the stream, L2 flushed before each when A fits in it, median kept.  Writes
+ * up to max_entries results (*n_entries = count) and records the fastest
+ * variant in the tuned table (saved and loaded with hml_tune_save /
+ * hml_tune_load as "v" records) that hml_sgemv_ex, the SGEMM N = 1 route and
+ * hmlSgemv consult first.  Replaces the reference's online SGEMV tuner
+ * (hmlSgemvKernelConfigOnline, src/hml_sgemv_kernel.cu:391-633). */
+hml_status hml_autotune_sgemv(hml_order order, hml_op trans, int M, int N,
+                              int reps, hml_sgemv_tune_entry *entries,
+                              int max_entries, int *n_entries, void *stream);
 
 /* ------------------------------------------------- host-pointer path */
 

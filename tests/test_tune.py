@@ -98,13 +98,78 @@ def test_shipped_table_parses_and_covers_the_reference_workloads():
         pytest.skip("no shipped table")
     hml.tune_clear()
     try:
-        assert hml.tune_load(SHIPPED) == len(td.TABLE_SHAPES)
+        assert hml.tune_load(SHIPPED) == len(td.TABLE_SHAPES) + len(td.GEMV_TABLE_SHAPES)
         keys = set()
         for line in open(SHIPPED):
-            if line.startswith("#"):
+            if line.startswith("#") or line.startswith("v "):
                 continue
             akc, bkc, M, N, K = (int(x) for x in line.split(":")[0].split())
             keys.add((M, N, K))
         assert {(M, N, K) for (M, N, K, _ta, _tb) in td.TABLE_SHAPES} <= keys
+        # every SGEMV shape of the reference workloads has a measured variant
+        for (order, trans, M, N) in td.GEMV_TABLE_SHAPES:
+            assert hml.sgemv_select(order, trans, M, N) > 0
     finally:
         hml.tune_clear()
+
+
+def test_gemv_records_round_trip(tmp_path):
+    """"v" records: the SGEMV half of the tuned table, keyed by layout and
+    (length of y, length of x); hml_sgemv_select reports what hml_sgemv_ex
+    would run."""
+    hml.tune_clear()
+    f = tmp_path / "v.cfg"
+    _write(f, ["v 0 32768 4096 : 128 85.0\n",      # rows of A contiguous
+               "v 1 32768 4096 : 8 86.5\n"])       # columns contiguous
+    assert hml.tune_load(str(f)) == 2
+    assert lib.hml_tune_size() == 2
+    # row-major y = A x: rows contiguous; column-major: columns contiguous
+    assert hml.sgemv_select(hml.ROW_MAJOR, hml.OP_N, 32768, 4096) == 128
+    assert hml.sgemv_select(hml.COL_MAJOR, hml.OP_N, 32768, 4096) == 8
+    # y = A^T x on a column-major 4096 x 32768 A is the rows-contiguous layout
+    assert hml.sgemv_select(hml.COL_MAJOR, hml.OP_T, 4096, 32768) == 128
+    # a neighbour within a factor 2 in one dimension takes its variant
+    assert hml.sgemv_select(hml.ROW_MAJOR, hml.OP_N, 20000, 4096) == 128
+    # further away the heuristic decides
+    assert hml.sgemv_select(hml.ROW_MAJOR, hml.OP_N, 4096, 512) == 0
+    g = tmp_path / "w.cfg"
+    hml.tune_save(str(g))
+    text = g.read_text()
+    assert "v 0 32768 4096 : 128 85.000" in text and "v 1 32768 4096 : 8 86.500" in text
+    hml.tune_clear()
+    assert hml.sgemv_select(hml.ROW_MAJOR, hml.OP_N, 32768, 4096) == 0
+    # the reference's SGEMV configuration entry point reads this format too
+    hml.hmlSgemvKernelConfig(str(g))
+    assert lib.hml_tune_size() == 2
+    assert hml.sgemv_select(hml.COL_MAJOR, hml.OP_N, 32768, 4096) == 8
+    hml.tune_clear()
+
+
+@pytest.mark.parametrize("line", [
+    "v 0 32768 4096 : 100 1.0\n",     # threads per row not a power of two
+    "v 0 32768 4096 : 512 1.0\n",     # more than 256 threads per row
+    "v 1 32768 4096 : 17 1.0\n",      # column split above 16
+    "v 1 32768 4096 : 0 1.0\n",       # column split below 1
+    "v 2 32768 4096 : 8 1.0\n",       # bad layout flag
+    "v 0 0 4096 : 8 1.0\n",           # empty y
+    "v 0 32768 4096 : 8\n",           # too few fields
+])
+def test_gemv_bad_records_rejected(tmp_path, line):
+    hml.tune_clear()
+    f = tmp_path / "bad.cfg"
+    _write(f, [line])
+    with pytest.raises(hml.HmlError):
+        hml.tune_load(str(f))
+    assert lib.hml_tune_size() == 0
+
+
+def test_autotune_sgemv_rejects_bad_arguments():
+    """Argument checks come before any device work."""
+    for args in ((hml.ROW_MAJOR, hml.OP_N, 0, 16), (hml.ROW_MAJOR, hml.OP_N, 16, 0),
+                 (7, hml.OP_N, 16, 16), (hml.ROW_MAJOR, 9, 16, 16)):
+        with pytest.raises(hml.HmlError):
+            hml.autotune_sgemv(*args, reps=1)
+    with pytest.raises(hml.HmlError):
+        hml.autotune_sgemv(hml.ROW_MAJOR, hml.OP_N, 64, 64, reps=0)
+    with pytest.raises(hml.HmlError):
+        hml.sgemv_select(hml.ROW_MAJOR, hml.OP_N, 64, 64, lda=10)  # lda < N
