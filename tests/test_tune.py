@@ -173,3 +173,11 @@ def test_autotune_sgemv_rejects_bad_arguments():
         hml.autotune_sgemv(hml.ROW_MAJOR, hml.OP_N, 64, 64, reps=0)
     with pytest.raises(hml.HmlError):
         hml.sgemv_select(hml.ROW_MAJOR, hml.OP_N, 64, 64, lda=10)  # lda < N
+
+
+def test_sgemv_negative_variant_rejected():
+    """A forced SGEMV variant is >= 0 (0 = heuristic); a negative one is an
+    argument error, returned before any device work (the pointers are never
+    dereferenced)."""
+    with pytest.raises(hml.HmlError):
+        hml.sgemv_ex(hml.ROW_MAJOR, hml.OP_N, 64, 64, 1.0, 256, 64, 512, 0.0, 768, variant=-1)
