@@ -32,23 +32,65 @@ namespace {
 constexpr int kThreads = 256;
 
 // ----------------------------------------------------------------- rows
-template <int TPR, bool VEC>
-__global__ void __launch_bounds__(kThreads) gemv_rows_kernel(GemvProblem p) {
+// Sum of the TPR partial sums of each row of the CTA (threads r*TPR ..
+// r*TPR+TPR-1); the result is valid in the row's thread t == 0.  The order
+// is fixed: lanes by a shuffle tree, then the row's warps in index order.
+template <int TPR, bool REUSE>
+__device__ __forceinline__ float row_total(float acc, float *red, int r, int t) {
+  if (TPR >= 32) {
+    acc = warp_sum(acc);
+    if (TPR > 32) {
+      if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+      __syncthreads();
+      if (t == 0) {
+        acc = 0.0f;
+#pragma unroll
+        for (int w = 0; w < TPR / 32; ++w) acc += red[r * (TPR / 32) + w];
+      }
+      if (REUSE) __syncthreads();  // red is read before anyone writes it again
+    }
+  } else {
+#pragma unroll
+    for (int o = TPR / 2; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+  }
+  return acc;
+}
+
+// RPC = 256 / TPR rows per CTA, TPR threads per row.  With split > 1 (few
+// long rows), `split` CTAs take disjoint ranges of the same rows' columns
+// (whole float4 groups when VEC, the last rank also the Q % 4 tail) and
+// publish per-rank row sums to `partial` ([split][P]); the last CTA of the
+// row block to arrive (a per-block arrival counter, reset by that CTA) adds
+// them up, rank j of a row summed by the row's thread j % TPR in rank order
+// and the TPR results by the same tree as above, so results are
+// deterministic.  SPLIT = false is the one-CTA-per-row-block form (split
+// must be 1), compiled without the split bookkeeping (48 registers for the
+// 16-byte form with 128 threads per row, 5 CTAs per SM, as before the split
+// existed; 56 with it).
+template <int TPR, bool VEC, bool SPLIT>
+__global__ void __launch_bounds__(kThreads) gemv_rows_kernel(GemvProblem p, int split_arg,
+                                                             float *partial, unsigned *arrivals) {
   constexpr int RPC = kThreads / TPR;  // rows per CTA
   __shared__ float red[kThreads / 32];
+  __shared__ unsigned last;
+  const int split = SPLIT ? split_arg : 1;
   const int t = threadIdx.x % TPR;
   const int r = threadIdx.x / TPR;
-  const int64_t row = static_cast<int64_t>(blockIdx.x) * RPC + r;
+  const int rank = SPLIT ? static_cast<int>(blockIdx.x % split) : 0;
+  const int64_t blk = SPLIT ? blockIdx.x / split : blockIdx.x;
+  const int64_t row = blk * RPC + r;
   float acc = 0.0f;
   if (row < p.P) {
     const float *a = p.A + row * p.sp;
     if (VEC) {
       const int Q4 = p.Q >> 2;
+      const int qc = (Q4 + split - 1) / split;
+      const int qb = min(Q4, rank * qc), qe = min(Q4, qb + qc);
       const float4 *a4 = reinterpret_cast<const float4 *>(a);
       const float4 *x4 = reinterpret_cast<const float4 *>(p.x);
       float acc1 = 0.0f, acc2 = 0.0f, acc3 = 0.0f;
-      int q = t;
-      for (; q + 3 * TPR < Q4; q += 4 * TPR) {
+      int q = qb + t;
+      for (; q + 3 * TPR < qe; q += 4 * TPR) {
         float4 v0 = ldg_stream4(reinterpret_cast<const float *>(a4 + q));
         float4 v1 = ldg_stream4(reinterpret_cast<const float *>(a4 + q + TPR));
         float4 v2 = ldg_stream4(reinterpret_cast<const float *>(a4 + q + 2 * TPR));
@@ -64,7 +106,7 @@ __global__ void __launch_bounds__(kThreads) gemv_rows_kernel(GemvProblem p) {
         acc3 = fmaf(v3.x, w3.x, acc3); acc3 = fmaf(v3.y, w3.y, acc3);
         acc3 = fmaf(v3.z, w3.z, acc3); acc3 = fmaf(v3.w, w3.w, acc3);
       }
-      for (; q < Q4; q += TPR) {
+      for (; q < qe; q += TPR) {
         float4 v = ldg_stream4(reinterpret_cast<const float *>(a4 + q));
         float4 w = __ldg(x4 + q);
         acc = fmaf(v.x, w.x, acc); acc = fmaf(v.y, w.y, acc);
@@ -72,71 +114,83 @@ __global__ void __launch_bounds__(kThreads) gemv_rows_kernel(GemvProblem p) {
       }
       acc += acc1 + (acc2 + acc3);
       const int qt = (Q4 << 2) + t;
-      if (t < (p.Q & 3)) acc = fmaf(a[qt], __ldg(p.x + qt), acc);
+      if (rank == split - 1 && t < (p.Q & 3)) acc = fmaf(a[qt], __ldg(p.x + qt), acc);
     } else {
+      const int qc = (p.Q + split - 1) / split;
+      const int64_t qb64 = static_cast<int64_t>(rank) * qc;
+      const int qb = qb64 < p.Q ? static_cast<int>(qb64) : p.Q;
+      const int qe = min(p.Q - qb, qc) + qb;
       float acc1 = 0.0f;
-      int q = t;
-      for (; q + TPR < p.Q; q += 2 * TPR) {
+      int q = qb + t;
+      for (; q + TPR < qe; q += 2 * TPR) {
         acc = fmaf(ldg_stream(a + q), __ldg(p.x + q * p.incx), acc);
         acc1 = fmaf(ldg_stream(a + q + TPR), __ldg(p.x + (q + TPR) * p.incx), acc1);
       }
-      if (q < p.Q) acc = fmaf(ldg_stream(a + q), __ldg(p.x + q * p.incx), acc);
+      if (q < qe) acc = fmaf(ldg_stream(a + q), __ldg(p.x + q * p.incx), acc);
       acc += acc1;
     }
   }
-  // reduce the TPR partial sums of this row
-  if (TPR >= 32) {
-    acc = warp_sum(acc);
-    if (TPR > 32) {
-      if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
-      __syncthreads();
-      if (t == 0) {
-        acc = 0.0f;
-#pragma unroll
-        for (int w = 0; w < TPR / 32; ++w) acc += red[r * (TPR / 32) + w];
-      }
+  acc = row_total<TPR, SPLIT>(acc, red, r, t);
+  if (!SPLIT) {
+    if (t == 0 && row < p.P) {
+      float *y = p.y + row * p.incy;
+      *y = axpby(p.alpha, acc, p.beta, y);
     }
-  } else {
-#pragma unroll
-    for (int o = TPR / 2; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    return;
   }
+  // publish this rank's row sums; the block's last CTA to arrive adds them
+  if (t == 0 && row < p.P) __stcg(partial + static_cast<int64_t>(rank) * p.P + row, acc);
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) last = atomicAdd(&arrivals[blk], 1u) == static_cast<unsigned>(split - 1);
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  float s = 0.0f;
+  if (row < p.P)
+    for (int j = t; j < split; j += TPR) s += __ldcg(partial + static_cast<int64_t>(j) * p.P + row);
+  s = row_total<TPR, false>(s, red, r, t);
   if (t == 0 && row < p.P) {
     float *y = p.y + row * p.incy;
-    *y = axpby(p.alpha, acc, p.beta, y);
+    *y = axpby(p.alpha, s, p.beta, y);
   }
+  if (threadIdx.x == 0) arrivals[blk] = 0u;  // ready for the next call
 }
 
 // ----------------------------------------------------------------- cols
-// A CTA covers kColRows = 256 rows: warp w takes row group w & 1 (128 rows)
-// and column phase w >> 1 (columns qbeg + phase, + 4, + 8, ...).  VEC: lane
-// owns rows group_base + 4*lane .. +3 (16-byte loads); else rows
-// group_base + lane + 32*j for j < 4.  Eight columns are loaded before any
-// is used, and registers are capped at 32 so that 8 CTAs fit on an SM
+// A CTA covers a tile of kColRows = 256 rows: warp w takes row group w & 1
+// (128 rows) and column phase w >> 1 (columns qbeg + phase, + 4, + 8, ...).
+// NARROW (P <= 128, a single 128-row tile): all 8 warps take the one row
+// group, in 8 column phases.  VEC: lane owns rows group_base + 4*lane .. +3
+// (16-byte loads); else rows group_base + lane + 32*j for j < 4; a lane
+// whose rows all lie past P does no loads.  Eight columns are loaded before
+// any is used, and registers are capped at 32 so that 8 CTAs fit on an SM
 // (measured on B200, 32768 x 4096, split 8: 6.6 TB/s; with 48 registers and
 // 5 CTAs per SM 6.1 TB/s; the earlier 128-row CTAs with 4 loads in flight
 // reduced through cluster shared memory 5.3 TB/s).
 constexpr int kColRows = 256;
-constexpr int kColPhases = kThreads / 32 / 2;
 constexpr int kColUnroll = 8;
 constexpr int kMaxColSplit = kGemvMaxColSplit;
 static_assert(kColRows == kThreads, "thread i finalises row i of the tile");
 
-template <bool VEC>
+template <bool VEC, bool NARROW>
 __global__ void __launch_bounds__(kThreads, 8) gemv_cols_kernel(GemvProblem p, int split,
                                                              float *partial, unsigned *arrivals) {
+  constexpr int kTileRows = NARROW ? 128 : kColRows;
+  constexpr int S = NARROW ? kThreads / 32 : kThreads / 32 / 2;  // column phases
   __shared__ float4 part[kThreads / 32][32];
   __shared__ float sum[kColRows];
   __shared__ unsigned last;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int group = warp & 1, phase = warp >> 1;
+  const int group = NARROW ? 0 : warp & 1, phase = NARROW ? warp : warp >> 1;
   const int rank = static_cast<int>(blockIdx.x % split);
   const int64_t tile = blockIdx.x / split;
-  const int64_t row0 = tile * kColRows;
+  const int64_t row0 = tile * kTileRows;
   const int64_t gbase = row0 + group * 128;
   const int qc = (p.Q + split - 1) / split;
-  const int qbeg = rank * qc;
-  const int qend = min(p.Q, qbeg + qc);
-  constexpr int S = kColPhases;  // column stride of one warp
+  const int64_t qbeg64 = static_cast<int64_t>(rank) * qc;
+  const int qbeg = qbeg64 < p.Q ? static_cast<int>(qbeg64) : p.Q;
+  const int qend = min(p.Q - qbeg, qc) + qbeg;
 
   float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
   const int64_t myrow = VEC ? gbase + 4 * lane : gbase + lane;
@@ -178,7 +232,7 @@ __global__ void __launch_bounds__(kThreads, 8) gemv_cols_kernel(GemvProblem p, i
       acc.z = fmaf(v.z, xv, acc.z); acc.w = fmaf(v.w, xv, acc.w);
     }
     acc.x += acc1.x; acc.y += acc1.y; acc.z += acc1.z; acc.w += acc1.w;
-  } else {
+  } else if (myrow < p.P) {
     // ragged last tile: element-wise with bounds checks
     float v[4] = {0.f, 0.f, 0.f, 0.f};
     for (int q = qbeg + phase; q < qend; q += S) {
@@ -195,7 +249,7 @@ __global__ void __launch_bounds__(kThreads, 8) gemv_cols_kernel(GemvProblem p, i
   // combine the column phases: part[w][lane] holds this lane's 4 rows
   part[warp][lane] = acc;
   __syncthreads();
-  {
+  if (threadIdx.x < kTileRows) {
     // thread i owns row offset i of the tile: group i / 128, and within the
     // group the lane slot / component that holds it; phases summed in order
     const int i = static_cast<int>(threadIdx.x);
@@ -204,33 +258,54 @@ __global__ void __launch_bounds__(kThreads, 8) gemv_cols_kernel(GemvProblem p, i
     const int comp = VEC ? r & 3 : r >> 5;
     float s = 0.0f;
 #pragma unroll
-    for (int ph = 0; ph < kColPhases; ++ph) {
-      const float4 v = part[2 * ph + g][slot_lane];
+    for (int ph = 0; ph < S; ++ph) {
+      const float4 v = part[NARROW ? ph : 2 * ph + g][slot_lane];
       s += comp == 0 ? v.x : comp == 1 ? v.y : comp == 2 ? v.z : v.w;
     }
     sum[i] = s;
   }
   const int64_t rr = row0 + threadIdx.x;
   if (split > 1) {
-    // publish this CTA's partial; the tile's last CTA to arrive sums the
-    // split partials in rank order
-    if (rr < p.P) __stcg(partial + static_cast<int64_t>(rank) * p.P + rr, sum[threadIdx.x]);
+    // publish this CTA's partial ([tile][rank][kTileRows] in the workspace);
+    // the tile's last CTA to arrive sums the split partials
+    float *tp = partial + tile * split * kTileRows;
+    if (threadIdx.x < kTileRows) __stcg(tp + rank * kTileRows + threadIdx.x, sum[threadIdx.x]);
     __threadfence();
     __syncthreads();
     if (threadIdx.x == 0) last = atomicAdd(&arrivals[tile], 1u) == static_cast<unsigned>(split - 1);
     __syncthreads();
     if (!last) return;
     __threadfence();
-    if (rr < p.P) {
-      float s = 0.0f;
-      for (int r = 0; r < split; ++r) s += __ldcg(partial + static_cast<int64_t>(r) * p.P + rr);
+    // thread i adds 4 rows (quad i % QUADS) over the ranks k = slice,
+    // slice + SLICES, ... in order (16-byte loads); the SLICES sums of a row
+    // are then added in slice order
+    constexpr int QUADS = kTileRows / 4, SLICES = kThreads / QUADS;
+    const int quad = static_cast<int>(threadIdx.x) % QUADS;
+    const int slice = static_cast<int>(threadIdx.x) / QUADS;
+    float4 t4 = make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll 8
+    for (int k = slice; k < split; k += SLICES) {
+      const float4 v = __ldcg(reinterpret_cast<const float4 *>(tp + k * kTileRows) + quad);
+      t4.x += v.x; t4.y += v.y; t4.z += v.z; t4.w += v.w;
+    }
+    float4 *flat = &part[0][0];  // SLICES x QUADS = 256 entries
+    flat[slice * QUADS + quad] = t4;
+    __syncthreads();
+    if (threadIdx.x < kTileRows && rr < p.P) {
+      const int q = static_cast<int>(threadIdx.x) >> 2, c = threadIdx.x & 3;
+      float total = 0.0f;
+#pragma unroll
+      for (int sl = 0; sl < SLICES; ++sl) {
+        const float4 v = flat[sl * QUADS + q];
+        total += c == 0 ? v.x : c == 1 ? v.y : c == 2 ? v.z : v.w;
+      }
       float *y = p.y + rr * p.incy;
-      *y = axpby(p.alpha, s, p.beta, y);
+      *y = axpby(p.alpha, total, p.beta, y);
     }
     if (threadIdx.x == 0) arrivals[tile] = 0u;  // ready for the next call
   } else {
     __syncthreads();
-    if (rr < p.P) {
+    if (threadIdx.x < kTileRows && rr < p.P) {
       float *y = p.y + rr * p.incy;
       *y = axpby(p.alpha, sum[threadIdx.x], p.beta, y);
     }
@@ -247,17 +322,39 @@ __global__ void scale_kernel(float *C, int M, int N, int64_t scm, int64_t scn, f
   }
 }
 
+// Few long rows: the columns of each row are split over several CTAs so
+// that about 7/8 of the CTAs that fit on the GPU at once (8 per SM) run,
+// each thread keeping at least 8 float4 of its row (measured on B200,
+// 64 x 200000: one CTA per row 65.7 us).
+constexpr int kMaxRowSplit = 64;
+
 template <int TPR>
 hml_status run_rows(const GemvProblem &p, bool vec, cudaStream_t s) {
   constexpr int RPC = kThreads / TPR;
   const int64_t blocks = (static_cast<int64_t>(p.P) + RPC - 1) / RPC;
   if (blocks > 0x7fffffff) return HML_STATUS_NOT_SUPPORTED;
-  count_launch();
-  if (vec)
-    gemv_rows_kernel<TPR, true><<<static_cast<unsigned>(blocks), kThreads, 0, s>>>(p);
-  else
-    gemv_rows_kernel<TPR, false><<<static_cast<unsigned>(blocks), kThreads, 0, s>>>(p);
-  cudaError_t e = cudaGetLastError();
+  int split = 1;
+  const int64_t want = static_cast<int64_t>(sm_count()) * 8 * 7 / 8;
+  if (blocks < want) {
+    split = static_cast<int>(std::min<int64_t>(kMaxRowSplit, want / blocks));
+    while (split > 1 && p.Q / (static_cast<int64_t>(split) * TPR * 4) < 8) --split;
+  }
+  float *partial = nullptr;
+  unsigned *arrivals = nullptr;
+  if (split > 1) {
+    void *ws = nullptr;
+    hml_status st = workspace(static_cast<size_t>(split) * p.P * sizeof(float), s, &ws);
+    if (st != HML_STATUS_SUCCESS) return st;
+    st = tile_counters(static_cast<size_t>(blocks), s, &arrivals);
+    if (st != HML_STATUS_SUCCESS) return st;
+    partial = static_cast<float *>(ws);
+  }
+  const dim3 grid(static_cast<unsigned>(blocks * split));
+  auto kernel = vec ? (split > 1 ? gemv_rows_kernel<TPR, true, true>
+                                  : gemv_rows_kernel<TPR, true, false>)
+                    : (split > 1 ? gemv_rows_kernel<TPR, false, true>
+                                 : gemv_rows_kernel<TPR, false, false>);
+  cudaError_t e = launch_k(kernel, grid, dim3(kThreads), 0, s, 1, p, split, partial, arrivals);
   note_cuda_error(e, "gemv_rows");
   return cuda_status(e);
 }
@@ -266,10 +363,11 @@ bool aligned16(const void *ptr) { return (reinterpret_cast<uintptr_t>(ptr) & 15u
 
 }  // namespace
 
-// variant for the row kernel: threads per row (4..256), 0 = heuristic.
-// variant for the column kernel: CTAs per 256-row tile along the columns
-// (1..16), 0 = heuristic.  kGemvTuned: the measured table's variant for this
-// shape when it holds one, else the heuristic.
+// variant for the row kernel: threads per row (4..256), 0 = heuristic (the
+// split of long rows over CTAs is always the heuristic's).  variant for the
+// column kernel: CTAs per row tile along the columns (1..128), 0 =
+// heuristic.  kGemvTuned: the measured table's variant for this shape when
+// it holds one, else the heuristic.
 hml_status launch_gemv(const GemvProblem &p, int variant, cudaStream_t s) {
   if (p.P == 0) return HML_STATUS_SUCCESS;
   if (p.sq != 1 && p.sp != 1) return HML_STATUS_NOT_SUPPORTED;
@@ -302,24 +400,27 @@ hml_status launch_gemv(const GemvProblem &p, int variant, cudaStream_t s) {
   }
   // columns contiguous
   const bool vec = aligned16(p.A) && (p.sq % 4 == 0 || p.Q == 1);
-  const int64_t tiles = (static_cast<int64_t>(p.P) + kColRows - 1) / kColRows;
+  const bool narrow = p.P <= 128;
+  const int tile_rows = narrow ? 128 : kColRows;
+  const int64_t tiles = (static_cast<int64_t>(p.P) + tile_rows - 1) / tile_rows;
   int split = variant;
   if (split == 0) {
     // about 7/8 of the CTAs that fit on the GPU at once, in one wave
     // (measured on B200, 32768 x 4096, 8 CTAs per SM resident: split 8 =
     // 1024 CTAs 6.6 TB/s, split 9 = 1152 CTAs 5.9 TB/s, split 10 (a second
-    // wave) 5.3 TB/s), each with >= 64 columns
+    // wave) 5.3 TB/s), each with >= 64 columns; few row tiles take up to
+    // kMaxColSplit CTAs each
     static const int per_sm = [] {
       int n = 0;
-      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, gemv_cols_kernel<true>, kThreads, 0) !=
-              cudaSuccess ||
+      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, gemv_cols_kernel<true, false>,
+                                                        kThreads, 0) != cudaSuccess ||
           n < 1)
         n = 1;
       return n;
     }();
     const int64_t resident = static_cast<int64_t>(per_sm) * sm_count() * 7 / 8;
-    split = static_cast<int>(resident / tiles);
-    split = max(1, min(split, kMaxColSplit));
+    split = static_cast<int>(std::min<int64_t>(kMaxColSplit, resident / tiles));
+    split = max(1, split);
     while (split > 1 && p.Q / split < 64) --split;
   }
   if (split < 1 || split > kMaxColSplit) return HML_STATUS_INVALID_VALUE;
@@ -328,17 +429,17 @@ hml_status launch_gemv(const GemvProblem &p, int variant, cudaStream_t s) {
   unsigned *arrivals = nullptr;
   if (split > 1) {
     void *ws = nullptr;
-    hml_status st = workspace(static_cast<size_t>(split) * p.P * sizeof(float), s, &ws);
+    hml_status st = workspace(static_cast<size_t>(tiles) * split * tile_rows * sizeof(float), s,
+                              &ws);
     if (st != HML_STATUS_SUCCESS) return st;
     st = tile_counters(static_cast<size_t>(tiles), s, &arrivals);
     if (st != HML_STATUS_SUCCESS) return st;
     partial = static_cast<float *>(ws);
   }
   const dim3 grid(static_cast<unsigned>(tiles * split));
-  cudaError_t e = vec ? launch_k(gemv_cols_kernel<true>, grid, dim3(kThreads), 0, s, 1, p, split,
-                                 partial, arrivals)
-                      : launch_k(gemv_cols_kernel<false>, grid, dim3(kThreads), 0, s, 1, p, split,
-                                 partial, arrivals);
+  auto kernel = vec ? (narrow ? gemv_cols_kernel<true, true> : gemv_cols_kernel<true, false>)
+                    : (narrow ? gemv_cols_kernel<false, true> : gemv_cols_kernel<false, false>);
+  cudaError_t e = launch_k(kernel, grid, dim3(kThreads), 0, s, 1, p, split, partial, arrivals);
   note_cuda_error(e, "gemv_cols");
   return cuda_status(e);
 }

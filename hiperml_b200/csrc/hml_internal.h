@@ -52,11 +52,12 @@ hml_status gemv_from_blas(hml_order order, hml_op trans, int M, int N, float alp
 
 // Kernels (one launcher per family).  All are stream ordered.
 // launch_gemv's variant: threads per row (4..256, powers of two) when the
-// rows of A are contiguous, CTAs per 256-row tile (1..kGemvMaxColSplit) when
-// the columns are; 0 = the heuristic; kGemvTuned = the autotuner's measured
-// table, else the heuristic.
+// rows of A are contiguous, CTAs per row tile (1..kGemvMaxColSplit; a tile
+// is 256 rows, or 128 when P <= 128) when the columns are; 0 = the
+// heuristic; kGemvTuned = the autotuner's measured table, else the
+// heuristic.
 constexpr int kGemvTuned = -1;
-constexpr int kGemvMaxColSplit = 16;
+constexpr int kGemvMaxColSplit = 128;
 hml_status launch_gemv(const GemvProblem &p, int variant, cudaStream_t s);
 // Which GEMV kernel serves p: the row kernel (rows of A contiguous) or the
 // column kernel.

@@ -70,7 +70,7 @@ def test_gemv_rows_variants(cuda, variant):
     assert_within_fp32_bound(got, D, absD, N)
 
 
-@pytest.mark.parametrize("variant", [1, 2, 3, 5, 8, 11, 16])
+@pytest.mark.parametrize("variant", [1, 2, 3, 5, 8, 11, 16, 24, 64, 128])
 def test_gemv_cols_split(cuda, variant):
     """The column kernel with `variant` CTAs per 256-row tile (the last to
     finish sums the partials in rank order), ragged rows and columns."""
@@ -104,6 +104,58 @@ def test_gemv_cols_split_repeatable(cuda):
     D, absD = expected(A, x, np.zeros(M, np.float32), 1.0, 0.0, False)
     for v, o in outs:
         assert_within_fp32_bound(o, D, absD, N, what=f"split {v}")
+
+
+# Short-wide problems: y has few entries and A's rows are long.  Column
+# layout (y = A x, A column-major): P <= 128 runs the 128-row tile with 8
+# column phases, and up to 128 CTAs split the columns of one tile.  Row
+# layout (y = A^T x): few long rows are split over several CTAs per row.
+SHORT_WIDE = [(1, 5000), (3, 70001), (16, 100000), (64, 200000), (100, 30001), (128, 65536),
+              (129, 40000), (255, 33333), (256, 65536), (512, 65536), (2048, 16384)]
+
+
+@pytest.mark.parametrize("shape", SHORT_WIDE, ids=lambda s: f"{s[0]}x{s[1]}")
+@pytest.mark.parametrize("layout", ["cols", "rows"])
+def test_gemv_short_wide(cuda, shape, layout):
+    import torch
+    P, Q = shape
+    rng = np.random.default_rng(P * 7 + Q)
+    opA = rng.standard_normal((P, Q)).astype(np.float32)  # the logical op(A)
+    x = rng.standard_normal(Q).astype(np.float32)
+    y0 = rng.uniform(-1, 1, P).astype(np.float32)
+    # cols: A = op(A) column-major, y = A x; rows: A = op(A)^T column-major
+    # (Q x P), y = A^T x, whose rows are op(A)'s rows, contiguous
+    if layout == "cols":
+        store = torch.from_numpy(np.ascontiguousarray(opA.T)).cuda()  # columns contiguous
+        args = (hml.COL_MAJOR, hml.OP_N, P, Q)
+        lda = P
+    else:
+        store = torch.from_numpy(np.ascontiguousarray(opA)).cuda()    # rows contiguous
+        args = (hml.COL_MAJOR, hml.OP_T, Q, P)
+        lda = Q
+    xd = to_dev(x)
+    outs = []
+    for _ in range(2):
+        y = to_dev(y0)
+        hml.sgemv_ex(*args, 1.5, store, lda, xd, -0.5, y)
+        outs.append(to_host(y))
+    assert np.array_equal(outs[0], outs[1])  # deterministic split reductions
+    D, absD = oracle.dgemm(opA, x.reshape(-1, 1), y0.reshape(-1, 1), 1.5, -0.5,
+                           with_abs=True)
+    assert_within_fp32_bound(outs[0], D[:, 0], absD[:, 0], Q, what=f"{layout} {shape}")
+
+
+@pytest.mark.parametrize("variant", [1, 7, 32, 128])
+def test_gemv_cols_narrow_forced_splits(cuda, variant):
+    """The 128-row tile with a forced split, odd P (ragged lanes) and a
+    column count that the split does not divide."""
+    P, Q = 77, 9999
+    A = dg.matrix(P, Q, 106, 0, dg.UNIFORM, order="C")
+    x = dg.fill(Q, 106, 1)
+    y = dg.fill(P, 106, 2)
+    got = run_gemv(hml.COL_MAJOR, hml.OP_N, A, 0, x, y, 1.0, 2.0, variant=variant)
+    D, absD = expected(A, x, y, 1.0, 2.0, False)
+    assert_within_fp32_bound(got, D, absD, Q)
 
 
 def test_beta_zero_does_not_read_y(cuda):
