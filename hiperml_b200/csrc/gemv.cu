@@ -173,6 +173,59 @@ constexpr int kColUnroll = 8;
 constexpr int kMaxColSplit = kGemvMaxColSplit;
 static_assert(kColRows == kThreads, "thread i finalises row i of the tile");
 
+// End of a column-kernel CTA: sum[i] holds this CTA's sum for row i of its
+// tile.  split == 1: write y.  Otherwise publish the partial ([tile][rank]
+// [kTileRows] in the workspace); the tile's last CTA to arrive sums the
+// split partials with 16-byte loads: thread i adds 4 rows (quad i % QUADS)
+// over the ranks k = slice, slice + SLICES, ... in order, and the SLICES
+// sums of a row are then added in slice order through shared memory
+// (`flat`, 256 float4), so results are deterministic.
+template <int kTileRows>
+__device__ __forceinline__ void finish_tile(const GemvProblem &p, int64_t tile, int rank, int split,
+                                            float *partial, unsigned *arrivals, const float *sum,
+                                            float4 *flat, unsigned *last) {
+  const int64_t rr = tile * kTileRows + threadIdx.x;
+  if (split == 1) {
+    __syncthreads();
+    if (threadIdx.x < kTileRows && rr < p.P) {
+      float *y = p.y + rr * p.incy;
+      *y = axpby(p.alpha, sum[threadIdx.x], p.beta, y);
+    }
+    return;
+  }
+  float *tp = partial + tile * split * kTileRows;
+  if (threadIdx.x < kTileRows) __stcg(tp + rank * kTileRows + threadIdx.x, sum[threadIdx.x]);
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) *last = atomicAdd(&arrivals[tile], 1u) == static_cast<unsigned>(split - 1);
+  __syncthreads();
+  if (!*last) return;
+  __threadfence();
+  constexpr int QUADS = kTileRows / 4, SLICES = kThreads / QUADS;
+  const int quad = static_cast<int>(threadIdx.x) % QUADS;
+  const int slice = static_cast<int>(threadIdx.x) / QUADS;
+  float4 t4 = make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll 8
+  for (int k = slice; k < split; k += SLICES) {
+    const float4 v = __ldcg(reinterpret_cast<const float4 *>(tp + k * kTileRows) + quad);
+    t4.x += v.x; t4.y += v.y; t4.z += v.z; t4.w += v.w;
+  }
+  flat[slice * QUADS + quad] = t4;
+  __syncthreads();
+  if (threadIdx.x < kTileRows && rr < p.P) {
+    const int q = static_cast<int>(threadIdx.x) >> 2, c = threadIdx.x & 3;
+    float total = 0.0f;
+#pragma unroll
+    for (int sl = 0; sl < SLICES; ++sl) {
+      const float4 v = flat[sl * QUADS + q];
+      total += c == 0 ? v.x : c == 1 ? v.y : c == 2 ? v.z : v.w;
+    }
+    float *y = p.y + rr * p.incy;
+    *y = axpby(p.alpha, total, p.beta, y);
+  }
+  if (threadIdx.x == 0) arrivals[tile] = 0u;  // ready for the next call
+}
+
 template <bool VEC, bool NARROW>
 __global__ void __launch_bounds__(kThreads, 8) gemv_cols_kernel(GemvProblem p, int split,
                                                              float *partial, unsigned *arrivals) {
@@ -264,52 +317,101 @@ __global__ void __launch_bounds__(kThreads, 8) gemv_cols_kernel(GemvProblem p, i
     }
     sum[i] = s;
   }
-  const int64_t rr = row0 + threadIdx.x;
-  if (split > 1) {
-    // publish this CTA's partial ([tile][rank][kTileRows] in the workspace);
-    // the tile's last CTA to arrive sums the split partials
-    float *tp = partial + tile * split * kTileRows;
-    if (threadIdx.x < kTileRows) __stcg(tp + rank * kTileRows + threadIdx.x, sum[threadIdx.x]);
-    __threadfence();
-    __syncthreads();
-    if (threadIdx.x == 0) last = atomicAdd(&arrivals[tile], 1u) == static_cast<unsigned>(split - 1);
-    __syncthreads();
-    if (!last) return;
-    __threadfence();
-    // thread i adds 4 rows (quad i % QUADS) over the ranks k = slice,
-    // slice + SLICES, ... in order (16-byte loads); the SLICES sums of a row
-    // are then added in slice order
-    constexpr int QUADS = kTileRows / 4, SLICES = kThreads / QUADS;
-    const int quad = static_cast<int>(threadIdx.x) % QUADS;
-    const int slice = static_cast<int>(threadIdx.x) / QUADS;
-    float4 t4 = make_float4(0.f, 0.f, 0.f, 0.f);
-#pragma unroll 8
-    for (int k = slice; k < split; k += SLICES) {
-      const float4 v = __ldcg(reinterpret_cast<const float4 *>(tp + k * kTileRows) + quad);
-      t4.x += v.x; t4.y += v.y; t4.z += v.z; t4.w += v.w;
-    }
-    float4 *flat = &part[0][0];  // SLICES x QUADS = 256 entries
-    flat[slice * QUADS + quad] = t4;
-    __syncthreads();
-    if (threadIdx.x < kTileRows && rr < p.P) {
-      const int q = static_cast<int>(threadIdx.x) >> 2, c = threadIdx.x & 3;
-      float total = 0.0f;
+  finish_tile<kTileRows>(p, tile, rank, split, partial, arrivals, sum, &part[0][0], &last);
+}
+
+// Short results (P <= 128) with 16-byte loads: LPC lanes share a column
+// (LPC = the power of two >= ceil(P / 4); lane l takes the 4 rows of quad
+// l % LPC in column slot l / LPC), so a warp covers 32 / LPC columns per
+// step and every lane loads; the 8 warps take interleaved column slots, 8
+// steps loaded before any is used.  The column slots of a warp are added by
+// a fixed shuffle tree, the warps in index order through shared memory;
+// `split` CTAs take column ranges and finish as the column kernel does.
+template <int LPC>
+__global__ void __launch_bounds__(kThreads, 8) gemv_short_kernel(GemvProblem p, int split,
+                                                              float *partial, unsigned *arrivals) {
+  constexpr int kTileRows = 128;
+  constexpr int CPW = 32 / LPC;                // column slots per warp
+  constexpr int CS = CPW * (kThreads / 32);    // columns per CTA step
+  __shared__ float4 part[kThreads / 32][32];
+  __shared__ float sum[kColRows];
+  __shared__ unsigned last;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int quad = lane % LPC, slot = lane / LPC;
+  const int rank = static_cast<int>(blockIdx.x);  // a single row tile
+  const int qc = (p.Q + split - 1) / split;
+  const int64_t qbeg64 = static_cast<int64_t>(rank) * qc;
+  const int qbeg = qbeg64 < p.Q ? static_cast<int>(qbeg64) : p.Q;
+  const int qend = min(p.Q - qbeg, qc) + qbeg;
+  const int row = 4 * quad;
+  const int first = qbeg + warp * CPW + slot;  // this lane's first column
+
+  float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
+  if (row + 3 < p.P) {
+    float4 acc1 = make_float4(0.f, 0.f, 0.f, 0.f);
+    const int64_t astep = static_cast<int64_t>(CS) * p.sq, xstep = static_cast<int64_t>(CS) * p.incx;
+    int q = first;
+    const float *ac = p.A + row + static_cast<int64_t>(q) * p.sq;
+    const float *xc = p.x + static_cast<int64_t>(q) * p.incx;
+    for (; q + (kColUnroll - 1) * CS < qend;
+         q += kColUnroll * CS, ac += kColUnroll * astep, xc += kColUnroll * xstep) {
+      float4 v[kColUnroll];
 #pragma unroll
-      for (int sl = 0; sl < SLICES; ++sl) {
-        const float4 v = flat[sl * QUADS + q];
-        total += c == 0 ? v.x : c == 1 ? v.y : c == 2 ? v.z : v.w;
+      for (int u = 0; u < kColUnroll; ++u) v[u] = ldg_stream4(ac + u * astep);
+#pragma unroll
+      for (int u = 0; u < kColUnroll; u += 2) {
+        const float x0 = __ldg(xc + u * xstep);
+        const float x1 = __ldg(xc + (u + 1) * xstep);
+        acc.x = fmaf(v[u].x, x0, acc.x); acc.y = fmaf(v[u].y, x0, acc.y);
+        acc.z = fmaf(v[u].z, x0, acc.z); acc.w = fmaf(v[u].w, x0, acc.w);
+        acc1.x = fmaf(v[u + 1].x, x1, acc1.x); acc1.y = fmaf(v[u + 1].y, x1, acc1.y);
+        acc1.z = fmaf(v[u + 1].z, x1, acc1.z); acc1.w = fmaf(v[u + 1].w, x1, acc1.w);
       }
-      float *y = p.y + rr * p.incy;
-      *y = axpby(p.alpha, total, p.beta, y);
     }
-    if (threadIdx.x == 0) arrivals[tile] = 0u;  // ready for the next call
-  } else {
-    __syncthreads();
-    if (threadIdx.x < kTileRows && rr < p.P) {
-      float *y = p.y + rr * p.incy;
-      *y = axpby(p.alpha, sum[threadIdx.x], p.beta, y);
+    for (; q < qend; q += CS) {
+      const float4 v = ldg_stream4(p.A + row + static_cast<int64_t>(q) * p.sq);
+      const float xv = __ldg(p.x + static_cast<int64_t>(q) * p.incx);
+      acc.x = fmaf(v.x, xv, acc.x); acc.y = fmaf(v.y, xv, acc.y);
+      acc.z = fmaf(v.z, xv, acc.z); acc.w = fmaf(v.w, xv, acc.w);
     }
+    acc.x += acc1.x; acc.y += acc1.y; acc.z += acc1.z; acc.w += acc1.w;
+  } else if (row < p.P) {
+    // the last, partial quad: element-wise (a 16-byte load could pass the
+    // end of the last column)
+    float v[4] = {0.f, 0.f, 0.f, 0.f};
+    for (int q = first; q < qend; q += CS) {
+      const float xv = __ldg(p.x + static_cast<int64_t>(q) * p.incx);
+      const float *col = p.A + static_cast<int64_t>(q) * p.sq;
+#pragma unroll
+      for (int j = 0; j < 4; ++j)
+        if (row + j < p.P) v[j] = fmaf(ldg_stream(col + row + j), xv, v[j]);
+    }
+    acc = make_float4(v[0], v[1], v[2], v[3]);
   }
+  // column slots of the warp: lanes quad, quad + LPC, ... (xor over the
+  // slot bits, fixed order)
+#pragma unroll
+  for (int o = 16; o >= LPC; o >>= 1) {
+    acc.x += __shfl_xor_sync(0xffffffffu, acc.x, o);
+    acc.y += __shfl_xor_sync(0xffffffffu, acc.y, o);
+    acc.z += __shfl_xor_sync(0xffffffffu, acc.z, o);
+    acc.w += __shfl_xor_sync(0xffffffffu, acc.w, o);
+  }
+  if (lane < LPC) part[warp][lane] = acc;
+  __syncthreads();
+  if (threadIdx.x < kTileRows) {
+    const int i = static_cast<int>(threadIdx.x), qd = i >> 2, c = i & 3;
+    float sv = 0.0f;
+    if (qd < LPC) {
+#pragma unroll
+      for (int w = 0; w < kThreads / 32; ++w) {
+        const float4 v = part[w][qd];
+        sv += c == 0 ? v.x : c == 1 ? v.y : c == 2 ? v.z : v.w;
+      }
+    }
+    sum[i] = sv;
+  }
+  finish_tile<kTileRows>(p, 0, rank, split, partial, arrivals, sum, &part[0][0], &last);
 }
 
 __global__ void scale_kernel(float *C, int M, int N, int64_t scm, int64_t scn, float beta) {
@@ -365,7 +467,7 @@ bool aligned16(const void *ptr) { return (reinterpret_cast<uintptr_t>(ptr) & 15u
 
 // variant for the row kernel: threads per row (4..256), 0 = heuristic (the
 // split of long rows over CTAs is always the heuristic's).  variant for the
-// column kernel: CTAs per row tile along the columns (1..128), 0 =
+// column kernel: CTAs per row tile along the columns (1..256), 0 =
 // heuristic.  kGemvTuned: the measured table's variant for this shape when
 // it holds one, else the heuristic.
 hml_status launch_gemv(const GemvProblem &p, int variant, cudaStream_t s) {
@@ -418,8 +520,11 @@ hml_status launch_gemv(const GemvProblem &p, int variant, cudaStream_t s) {
         n = 1;
       return n;
     }();
+    // (one 128-row tile of a short result may take up to 256 CTAs, a wider
+    // tile 128: the tile's last CTA reads split x rows partials)
     const int64_t resident = static_cast<int64_t>(per_sm) * sm_count() * 7 / 8;
-    split = static_cast<int>(std::min<int64_t>(kMaxColSplit, resident / tiles));
+    const int cap = narrow ? kMaxColSplit : kMaxColSplit / 2;
+    split = static_cast<int>(std::min<int64_t>(cap, resident / tiles));
     split = max(1, split);
     while (split > 1 && p.Q / split < 64) --split;
   }
@@ -439,6 +544,16 @@ hml_status launch_gemv(const GemvProblem &p, int variant, cudaStream_t s) {
   const dim3 grid(static_cast<unsigned>(tiles * split));
   auto kernel = vec ? (narrow ? gemv_cols_kernel<true, true> : gemv_cols_kernel<true, false>)
                     : (narrow ? gemv_cols_kernel<false, true> : gemv_cols_kernel<false, false>);
+  if (vec && narrow) {
+    // every lane on columns: LPC lanes per column, LPC >= ceil(P / 4)
+    const int p4 = (p.P + 3) / 4;
+    kernel = p4 <= 1   ? gemv_short_kernel<1>
+             : p4 <= 2 ? gemv_short_kernel<2>
+             : p4 <= 4 ? gemv_short_kernel<4>
+             : p4 <= 8 ? gemv_short_kernel<8>
+             : p4 <= 16 ? gemv_short_kernel<16>
+                        : gemv_short_kernel<32>;
+  }
   cudaError_t e = launch_k(kernel, grid, dim3(kThreads), 0, s, 1, p, split, partial, arrivals);
   note_cuda_error(e, "gemv_cols");
   return cuda_status(e);

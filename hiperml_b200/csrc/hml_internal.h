@@ -57,7 +57,7 @@ hml_status gemv_from_blas(hml_order order, hml_op trans, int M, int N, float alp
 // heuristic; kGemvTuned = the autotuner's measured table, else the
 // heuristic.
 constexpr int kGemvTuned = -1;
-constexpr int kGemvMaxColSplit = 128;
+constexpr int kGemvMaxColSplit = 256;
 hml_status launch_gemv(const GemvProblem &p, int variant, cudaStream_t s);
 // Which GEMV kernel serves p: the row kernel (rows of A contiguous) or the
 // column kernel.

@@ -443,7 +443,7 @@ hml_status autotune_gemv(hml_order order, hml_op trans, int M, int N, int reps,
     for (int v = 4; v <= 256; v <<= 1) variants.push_back(v);
   else
     for (int v : {1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 11, 12, 13, 14, 15, 16, 20, 24, 32, 48, 64, 96,
-                  128})
+                  128, 192, 256})
       variants.push_back(v);
   cudaEvent_t e0, e1;
   if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess)

@@ -331,7 +331,7 @@ hml_status hml_sgemv_ex(hml_order order, hml_op trans, int M, int N,
  * threads that share one row (4, 8, ..., 256; few long rows are also split
  * over several CTAs, as the heuristic decides); for A with contiguous
  * columns the number of CTAs that split the columns of one row tile (256
- * rows, 128 when the result has at most 128 entries), 1..128.  0 = the
+ * rows, 128 when the result has at most 128 entries), 1..256.  0 = the
  * heuristic.  Replaces launching one chosen SGEMV kernel of the reference's
  * repository (hmlSgemvKernelSelect + launch, src/hml_sgemv_kernel.cu:315-355). */
 hml_status hml_sgemv_ex_variant(hml_order order, hml_op trans, int M, int N,
@@ -352,7 +352,7 @@ typedef struct hml_sgemv_tune_entry {
 } hml_sgemv_tune_entry;
 
 /* Measures every variant of the SGEMV kernel that serves this layout (7
- * thread-per-row widths, or 23 column splits from 1 to 128) on an M x N
+ * thread-per-row widths, or 25 column splits from 1 to 256) on an M x N
  * problem with the leading dimension rounded up to a multiple of 4 floats
  * and uniform[-1,1] operands: one warm-up call, then `reps` calls timed with CUDA events on
  * the stream, L2 flushed before each when A fits in it, median kept.  Writes

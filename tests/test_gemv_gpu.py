@@ -70,7 +70,7 @@ def test_gemv_rows_variants(cuda, variant):
     assert_within_fp32_bound(got, D, absD, N)
 
 
-@pytest.mark.parametrize("variant", [1, 2, 3, 5, 8, 11, 16, 24, 64, 128])
+@pytest.mark.parametrize("variant", [1, 2, 3, 5, 8, 11, 16, 24, 64, 128, 256])
 def test_gemv_cols_split(cuda, variant):
     """The column kernel with `variant` CTAs per 256-row tile (the last to
     finish sums the partials in rank order), ragged rows and columns."""
@@ -156,6 +156,24 @@ def test_gemv_cols_narrow_forced_splits(cuda, variant):
     got = run_gemv(hml.COL_MAJOR, hml.OP_N, A, 0, x, y, 1.0, 2.0, variant=variant)
     D, absD = expected(A, x, y, 1.0, 2.0, False)
     assert_within_fp32_bound(got, D, absD, Q)
+
+
+@pytest.mark.parametrize("P,pad", [(2, 2), (4, 0), (5, 3), (8, 0), (30, 2), (61, 3), (64, 0),
+                                   (97, 3), (128, 0)])
+@pytest.mark.parametrize("variant", [0, 1, 3, 40, 256])
+def test_gemv_short_kernel(cuda, P, pad, variant):
+    """16-byte column layout with P <= 128 (LPC = 1..32 lanes per column,
+    P % 4 != 0 leaves a partial last quad), leading dimension padded to a
+    multiple of 4, forced and heuristic splits, ragged column count."""
+    Q = 12347
+    A = dg.matrix(P, Q, 107, 0, dg.NORMAL, order="C")
+    x = dg.fill(Q, 107, 1, dg.NORMAL)
+    y = dg.fill(P, 107, 2)
+    outs = [run_gemv(hml.COL_MAJOR, hml.OP_N, A, pad, x, y, -1.0, 0.75, variant=variant)
+            for _ in range(2)]
+    assert np.array_equal(outs[0], outs[1])
+    D, absD = expected(A, x, y, -1.0, 0.75, False)
+    assert_within_fp32_bound(outs[0], D, absD, Q, what=f"P={P} split={variant}")
 
 
 def test_beta_zero_does_not_read_y(cuda):

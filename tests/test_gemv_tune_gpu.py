@@ -13,7 +13,7 @@ from tests.gpu_util import assert_within_fp32_bound, to_dev, to_host
 pytestmark = pytest.mark.gpu
 
 ROW_VARIANTS = [4, 8, 16, 32, 64, 128, 256]
-COL_VARIANTS = list(range(1, 17)) + [20, 24, 32, 48, 64, 96, 128]
+COL_VARIANTS = list(range(1, 17)) + [20, 24, 32, 48, 64, 96, 128, 192, 256]
 
 
 def _store(A, order):

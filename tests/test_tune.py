@@ -148,7 +148,7 @@ def test_gemv_records_round_trip(tmp_path):
 @pytest.mark.parametrize("line", [
     "v 0 32768 4096 : 100 1.0\n",     # threads per row not a power of two
     "v 0 32768 4096 : 512 1.0\n",     # more than 256 threads per row
-    "v 1 32768 4096 : 129 1.0\n",     # column split above 128
+    "v 1 32768 4096 : 257 1.0\n",     # column split above 256
     "v 1 32768 4096 : 0 1.0\n",       # column split below 1
     "v 2 32768 4096 : 8 1.0\n",       # bad layout flag
     "v 0 0 4096 : 8 1.0\n",           # empty y
