@@ -10,16 +10,21 @@
 //             one-CTA-per-row hmlSgemvKernelBasicN
 //             (include/hml_sgemv_kernel_template.h:19-106), whose volatile
 //             warp-synchronous tail is unsafe under independent thread
-//             scheduling.
+//             scheduling.  Few long rows are split over several CTAs per
+//             row (the reference's one CTA per row leaves most SMs idle).
 //  gemv_cols  A(p,q) columns contiguous (sp == 1): column-major y = A x.
 //             Each lane owns 4 consecutive rows (one 16-byte load per
 //             column), the 8 warps of a CTA take 2 row groups x 4
 //             interleaved column phases, and `split` CTAs take disjoint
 //             column ranges of the same 256 rows.  Partial sums are combined
 //             in a fixed order: the phases in shared memory, the split CTAs
-//             through a per-stream workspace, summed in rank order by
+//             through a per-stream workspace, summed in a fixed order
+//             (fixed slices of the ranks, then the slices in order) by
 //             whichever CTA of the tile finishes last (a per-tile arrival
 //             counter, reset by that CTA), so results are deterministic.
+//  gemv_short the same layout for P <= 128 with 16-byte loads: several
+//             columns per warp so that every lane loads, one 128-row tile
+//             split over up to 256 CTAs.
 #include <algorithm>
 
 #include "hml_device.cuh"
