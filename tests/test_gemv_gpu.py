@@ -73,7 +73,7 @@ def test_gemv_rows_variants(cuda, variant):
 @pytest.mark.parametrize("variant", [1, 2, 3, 5, 8, 11, 16, 24, 64, 128, 256])
 def test_gemv_cols_split(cuda, variant):
     """The column kernel with `variant` CTAs per 256-row tile (the last to
-    finish sums the partials in rank order), ragged rows and columns."""
+    finish sums the partials in a fixed order), ragged rows and columns."""
     M, N = 1531, 700
     A = dg.matrix(M, N, 103, 0, dg.UNIFORM, order="C")
     x = dg.fill(N, 103, 1)
@@ -84,7 +84,7 @@ def test_gemv_cols_split(cuda, variant):
 
 
 def test_gemv_cols_split_repeatable(cuda):
-    """Split partials are summed in rank order whatever order the CTAs finish
+    """Split partials are summed in a fixed order whatever order the CTAs finish
     in: repeated calls give identical bits, and the per-tile arrival counters
     are left ready for the next call (also after a call with another split)."""
     import torch
