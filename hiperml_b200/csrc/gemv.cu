@@ -332,8 +332,13 @@ __global__ void __launch_bounds__(kThreads, 8) gemv_cols_kernel(GemvProblem p, i
 // steps loaded before any is used.  The column slots of a warp are added by
 // a fixed shuffle tree, the warps in index order through shared memory;
 // `split` CTAs take column ranges and finish as the column kernel does.
+// A single tile runs at most 256 CTAs (under 2 per SM), so registers are
+// not capped for occupancy: 16 columns per lane are loaded before any is
+// used, twice the column kernel's, to halve the memory round trips of a
+// CTA's short column range.
+constexpr int kShortUnroll = 16;
 template <int LPC>
-__global__ void __launch_bounds__(kThreads, 8) gemv_short_kernel(GemvProblem p, int split,
+__global__ void __launch_bounds__(kThreads, 2) gemv_short_kernel(GemvProblem p, int split,
                                                               float *partial, unsigned *arrivals) {
   constexpr int kTileRows = 128;
   constexpr int CPW = 32 / LPC;                // column slots per warp
@@ -358,13 +363,13 @@ __global__ void __launch_bounds__(kThreads, 8) gemv_short_kernel(GemvProblem p, 
     int q = first;
     const float *ac = p.A + row + static_cast<int64_t>(q) * p.sq;
     const float *xc = p.x + static_cast<int64_t>(q) * p.incx;
-    for (; q + (kColUnroll - 1) * CS < qend;
-         q += kColUnroll * CS, ac += kColUnroll * astep, xc += kColUnroll * xstep) {
-      float4 v[kColUnroll];
+    for (; q + (kShortUnroll - 1) * CS < qend;
+         q += kShortUnroll * CS, ac += kShortUnroll * astep, xc += kShortUnroll * xstep) {
+      float4 v[kShortUnroll];
 #pragma unroll
-      for (int u = 0; u < kColUnroll; ++u) v[u] = ldg_stream4(ac + u * astep);
+      for (int u = 0; u < kShortUnroll; ++u) v[u] = ldg_stream4(ac + u * astep);
 #pragma unroll
-      for (int u = 0; u < kColUnroll; u += 2) {
+      for (int u = 0; u < kShortUnroll; u += 2) {
         const float x0 = __ldg(xc + u * xstep);
         const float x1 = __ldg(xc + (u + 1) * xstep);
         acc.x = fmaf(v[u].x, x0, acc.x); acc.y = fmaf(v[u].y, x0, acc.y);
