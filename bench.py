@@ -1,7 +1,7 @@
 """Benchmark of the skinny SGEMM/SGEMV path on B200.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload sweep|c1|gemv_n|gemv_t|square]
+                    [--workload sweep|c1|gemv_n|gemv_t|square|batched]
 
 Default workload ("sweep"): the skinny SGEMM precision sweep, C = A * B
 column-major with M = 65536, K = 4096 and N in {8, 32, 64, 128}, A and B
@@ -11,10 +11,16 @@ hml_sgemm_ex with the library's own configuration choice.  A is 1 GiB
 (> the 126 MB L2), so no L2 flush is needed between steps.
 
 The JSON line reports useful TFLOPS (2*M*N*K per GEMM), the roofline of the
-dominant kernel, an end-to-end figure through the host-pointer C ABI
-(hml_host_sgemm, pinned host buffers, copies inside the timed region), the
-reference's CPU loop as a CPU baseline, the SM clocks sampled during the
-timed region and the number of library kernel launches in it.
+dominant kernel (its algorithmic bytes, A and B read once and C written once,
+over its event-timed duration against the measured HBM copy rate), an
+end-to-end figure through the host-pointer C ABI (hml_host_sgemm, pinned host
+buffers, copies inside the timed region), the reference's CPU loop as a CPU
+baseline, the SM clocks sampled during the timed region and the number of
+library kernel launches in it.  With the default workload it also carries
+``workloads``: one short measured entry for each of the other configurations
+(c1 with L2 flushed, both SGEMV forms, the square 8192^3 problem, the
+log-uniform sweep, the sweep forced onto FP32 SIMT, the batched 1024-problem
+plan against separate calls, and the configuration predictor's regret).
 
 With torchrun (N > 1) every rank runs the same per-GPU workload on its own
 data (weak scaling: the GEMMs are independent row blocks of a larger
@@ -25,6 +31,7 @@ ranks.  --impl reference times the reference's own CPU implementation
 from __future__ import annotations
 
 import argparse
+import importlib.util
 import json
 import os
 import statistics
@@ -39,6 +46,11 @@ METRIC = "skinny SGEMM TFLOPS & % roofline: split-BF16 TC vs FP32 SIMT at FP32 a
 UNIT = "TFLOPS"
 
 SWEEP_M, SWEEP_K, SWEEP_N = 65536, 4096, (8, 32, 64, 128)
+SIMT_PEAK_NOMINAL = 148 * 128 * 2 * 1.965e-3  # TFLOP/s: 148 SMs x 128 FMA lanes x 2 x 1.965 GHz
+ALGO_NAMES = {1: "simt", 2: "bf16x3", 3: "bf16x6", 4: "tf32x3"}
+# BF16-product equivalents of one useful multiply-add per split form (a TF32
+# product runs at half the BF16 rate)
+PRODUCTS = {2: 3, 3: 6, 4: 6}
 
 
 def parse():
@@ -51,13 +63,28 @@ def parse():
                     choices=["sweep", "c1", "gemv_n", "gemv_t", "square", "batched"])
     ap.add_argument("--algo", default="auto", choices=["auto", "simt", "bf16x3", "bf16x6", "tf32x3"],
                     help="force one algorithm family (default: the library's choice)")
+    ap.add_argument("--dist", default="uniform", choices=["uniform", "loguniform"],
+                    help="sweep/c1/square inputs: uniform[-1,1] or log-uniform 1e-3..1e3")
     ap.add_argument("--rows", type=int, default=None,
                     help="sweep workload: M other than 65536 (small cases for profiler captures)")
     ap.add_argument("--only-n", type=int, default=None,
                     help="sweep workload: run only this N (profiler captures)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-workloads", action="store_true",
+                    help="default workload: leave out the per-configuration entries")
     return ap.parse_args()
+
+
+def load_datagen():
+    """hiperml_b200/datagen.py as a stand-alone module (pure numpy): the
+    reference arm draws its inputs with it without importing the package,
+    which would load the library."""
+    path = os.path.join(ROOT, "hiperml_b200", "datagen.py")
+    spec = importlib.util.spec_from_file_location("hml_datagen_standalone", path)
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
 
 
 # ------------------------------------------------------------------ peaks
@@ -194,16 +221,20 @@ def bytes_of(kind, M, N, K):
     return 4.0 * (M * K + Q + P)
 
 
-def config_desc(name):
+DIST_DESC = {"uniform": "uniform[-1,1]", "loguniform": "log-uniform magnitude 1e-3..1e3, random sign"}
+
+
+def config_desc(name, dist="uniform"):
+    """The workload, identical in both arms' JSON lines."""
     if name == "sweep":
         return {"workload": f"skinny SGEMM C=A*B col-major, M={SWEEP_M}, K={SWEEP_K}, "
                             f"N in {list(SWEEP_N)} (one step = the 4 GEMMs)",
                 "M": SWEEP_M, "K": SWEEP_K, "N": list(SWEEP_N), "alpha": 1.0, "beta": 0.0,
-                "layout": "column-major NN", "inputs": "uniform[-1,1], seed 0",
+                "layout": "column-major NN", "inputs": f"{DIST_DESC[dist]}, seed 0",
                 "l2": "A is 1 GiB per GEMM (> 126 MB L2): inputs larger than L2, no flush"}
     if name == "c1":
         return {"workload": "skinny SGEMM col-major M=4096, N=16, K=4096", "M": 4096, "N": 16,
-                "K": 4096, "inputs": "uniform[-1,1], seed 0",
+                "K": 4096, "inputs": f"{DIST_DESC[dist]}, seed 0",
                 "l2": "L2 flushed (256 MiB write) before every step"}
     if name in ("gemv_n", "gemv_t"):
         return {"workload": f"SGEMV y={'A' if name == 'gemv_n' else 'A^T'}*x, A 32768x4096 "
@@ -218,7 +249,7 @@ def config_desc(name):
                 "shapes_seed": BATCH_SEED, "inputs": "N(0,1), seed 3",
                 "storage": "leading dimensions rounded up to 4 floats, 256-byte aligned bases",
                 "l2": "about 15 GB of operands per step (> 126 MB L2): no flush"}
-    return {"workload": "square SGEMM 8192^3 col-major", "inputs": "uniform[-1,1], seed 0",
+    return {"workload": "square SGEMM 8192^3 col-major", "inputs": f"{DIST_DESC[dist]}, seed 0",
             "l2": "compute bound; inputs 256 MiB each"}
 
 
@@ -227,14 +258,14 @@ def cpu_reference_sample(problems, seconds=10.0, threads=None):
     """Times the reference's own hmlSgemmCpu / hmlSgemvCpu (oracle/_ref, or
     the C restatement when the reference build is absent) on row slices of
     each problem, on all host cores (one independent row block per thread).
-    Returns (TFLOPS, cores, kind, sample description)."""
+    Returns (TFLOPS, cores, kind, sample description, seconds timed, passes)."""
     import ctypes
     from concurrent.futures import ThreadPoolExecutor
 
     import numpy as np
 
     import oracle
-    from hiperml_b200 import datagen as dg
+    dg = load_datagen()
 
     cores = threads or os.cpu_count() or 1
     kind = "reference" if oracle.ref_available() else "port"
@@ -287,7 +318,7 @@ def cpu_reference_sample(problems, seconds=10.0, threads=None):
     desc = (f"{passes} pass(es) over {cores * rows_per_thread} rows of each problem "
             f"({', '.join(f'{k} M={M} N={N} K={K}' for (k, M, N, K) in problems)}), "
             f"one row block per thread, {elapsed:.1f} s")
-    return total_flops / elapsed / 1e12, cores, kind, desc
+    return total_flops / elapsed / 1e12, cores, kind, desc, elapsed, passes
 
 
 def run_reference(args):
@@ -301,19 +332,24 @@ def run_reference(args):
         problems = problems[:64]
     per_step = max(1.0, 120.0 / max(1, args.steps + args.warmup))
     per_step = min(per_step, 10.0)
-    vals = []
+    vals, secs = [], []
     cores = kind = desc = None
     for i in range(args.warmup + args.steps):
-        v, cores, kind, desc = cpu_reference_sample(problems, seconds=per_step)
+        v, cores, kind, desc, el, _ = cpu_reference_sample(problems, seconds=per_step)
         if i >= args.warmup:
             vals.append(v)
+            secs.append(el)
     value = statistics.median(vals)
     step_flops = sum(flops_of(*p) for p in problems)
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT,
-        "sample_problems": len(problems),
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": step_flops / (value * 1e12) * 1e3, "higher_is_better": True,
+        # what one timed step actually ran: a bounded row sample of the
+        # workload (the full workload at this rate is reported beside it)
+        "ms_per_step": statistics.mean(secs) * 1e3,
+        "ms_per_step_kind": "timed CPU sample per step (bounded row slices of the workload)",
+        "ms_per_full_workload_at_sample_rate": step_flops / (value * 1e12) * 1e3,
+        "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": config_desc(args.workload),
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": kind,
@@ -325,40 +361,60 @@ def run_reference(args):
 
 
 # -------------------------------------------------------------------- ours
-def run_ours(args):
+class Ctx:
+    """Device, stream and process-group state of one rank."""
+
+    def __init__(self):
+        import torch
+        self.world = int(os.environ.get("WORLD_SIZE", "1"))
+        self.rank = int(os.environ.get("RANK", "0"))
+        self.local = int(os.environ.get("LOCAL_RANK", "0"))
+        self.dist_on = self.world > 1
+        if self.dist_on:
+            import datetime
+
+            import torch.distributed as dist
+            torch.cuda.set_device(self.local)
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        self.dev = torch.device("cuda", self.local)
+        torch.cuda.set_device(self.dev)
+        self.stream = torch.cuda.current_stream()
+
+    def barrier(self):
+        if self.dist_on:
+            import torch.distributed as dist
+            dist.barrier()
+
+    def close(self):
+        if self.dist_on:
+            import torch.distributed as dist
+            dist.barrier()
+            dist.destroy_process_group()
+
+
+def measure_gemms(ctx, problems, algo, dist, steps, warmup, flush_l2, clocks=None,
+                  err_check=True):
+    """Runs `problems` (one step) `warmup` + `steps` times through
+    hml_sgemm_ex / hml_sgemv_ex and times them with CUDA events on the
+    launching stream.  Returns a dict with the step time (max over ranks),
+    per-problem times and configurations, launch counts and FP64 errors."""
     import torch
 
     import hiperml_b200 as hml
     from hiperml_b200 import datagen as dg
     from hiperml_b200.dist import max_over_ranks
 
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    dist_on = world > 1
-    if dist_on:
-        import datetime
-
-        import torch.distributed as dist
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-    dev = torch.device("cuda", local)
-    torch.cuda.set_device(dev)
-    stream = torch.cuda.current_stream()
-
-    problems = workload_problems(args.workload, args.rows, args.only_n)
-    algo = {"auto": None, "simt": 1, "bf16x3": 2, "bf16x6": 3, "tf32x3": 4}[args.algo]
-
-    # ---- device operands (one A shared by the sweep's GEMMs)
+    dev, stream, rank = ctx.dev, ctx.stream, ctx.rank
+    dist_code = {"uniform": dg.UNIFORM, "loguniform": dg.LOGUNIFORM}[dist]
     bufs = []
     Ashared = None
     for (k, M, N, K) in problems:
         if k == "sgemm":
             if Ashared is None or Ashared.numel() != M * K:
                 Ashared = torch.empty(M * K, dtype=torch.float32, device=dev)
-                hml.fill_random(Ashared, 0 + rank * 1000, 0, dg.UNIFORM)
+                hml.fill_random(Ashared, 0 + rank * 1000, 0, dist_code)
             B = torch.empty(K * N, dtype=torch.float32, device=dev)
-            hml.fill_random(B, 0 + rank * 1000, 1, dg.UNIFORM)
+            hml.fill_random(B, 0 + rank * 1000, 1, dist_code)
             C = torch.zeros(M * N, dtype=torch.float32, device=dev)
             cfg = hml.select(0, 0, 0, M, N, K) if algo is None else \
                 hml.select_algo(0, 0, 0, M, N, K, algo)
@@ -372,9 +428,7 @@ def run_ours(args):
             hml.fill_random(x, 1 + rank * 1000, 1, dg.NORMAL)
             y = torch.zeros(P, dtype=torch.float32, device=dev)
             bufs.append((k, M, N, K, A, x, y, None))
-    flush = None
-    if args.workload == "c1":
-        flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)  # 256 MiB
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev) if flush_l2 else None
 
     def launch(item):
         k, M, N, K, A, B, C, cfg = item
@@ -388,11 +442,11 @@ def run_ours(args):
 
     n_items = len(bufs)
     ev = [[(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
-           for _ in range(n_items)] for _ in range(args.steps)]
+           for _ in range(n_items)] for _ in range(steps)]
 
     def step(i=None):
         if flush is not None:
-            flush.fill_(float(i or 0))
+            flush.fill_(float(i or 0))  # 256 MiB write: nothing of the operands stays in L2
         for j, item in enumerate(bufs):
             if i is not None:
                 ev[i][j][0].record(stream)
@@ -400,171 +454,291 @@ def run_ours(args):
             if i is not None:
                 ev[i][j][1].record(stream)
 
-    for _ in range(args.warmup):
+    for _ in range(warmup):
         step()
     torch.cuda.synchronize()
     if hml.device_error() != 0:
         raise RuntimeError("device wait expired during warm-up")
-
-    if dist_on:
-        dist.barrier()
+    ctx.barrier()
     torch.cuda.synchronize()
     launches0 = hml.lib.hml_launch_count()
     t0 = torch.cuda.Event(enable_timing=True)
     t1 = torch.cuda.Event(enable_timing=True)
-    with ClockSampler(local) as clocks:
+    sampler = clocks if clocks is not None else ClockSampler(ctx.local, period=1.0)
+    with sampler:
         t0.record(stream)
-        for i in range(args.steps):
+        for i in range(steps):
             step(i)
         t1.record(stream)
         torch.cuda.synchronize()
     launches = hml.lib.hml_launch_count() - launches0
-    if dist_on:
-        dist.barrier()
+    ctx.barrier()
     elapsed_ms = t0.elapsed_time(t1)
-    per_kernel_ms = [statistics.mean(ev[i][j][0].elapsed_time(ev[i][j][1]) for i in
-                                     range(args.steps)) for j in range(n_items)]
+    per_kernel_ms = [statistics.mean(ev[i][j][0].elapsed_time(ev[i][j][1]) for i in range(steps))
+                     for j in range(n_items)]
     if flush is not None:
         # the flush is outside the measured GEMM events; time only the GEMMs
         elapsed_ms = sum(sum(ev[i][j][0].elapsed_time(ev[i][j][1]) for j in range(n_items))
-                         for i in range(args.steps))
+                         for i in range(steps))
     elapsed_ms = max_over_ranks(elapsed_ms, dev)
     if hml.device_error() != 0:
         raise RuntimeError("device wait expired in the timed region")
-
-    step_flops = sum(flops_of(k, M, N, K) for (k, M, N, K, *_rest) in bufs)
-    value = step_flops * args.steps * world / (elapsed_ms * 1e-3) / 1e12
-    pk = peaks()
-    # dominant kernel = longest per-launch time
-    dom = max(range(n_items), key=lambda j: per_kernel_ms[j])
-    k, M, N, K, *_ = bufs[dom]
-    alg_bytes = bytes_of(k, M, N, K)
-    alg_flops = flops_of(k, M, N, K)
-    dom_s = per_kernel_ms[dom] * 1e-3
-    dcfg = bufs[dom][7]
-    algo_names = {1: "simt", 2: "bf16x3", 3: "bf16x6", 4: "tf32x3"}
-    key = f"{args.workload}:{k}:{M}x{N}x{K}:{algo_names.get(dcfg.algo, 'gemv') if dcfg else 'gemv'}"
-    traffic = traffic_table().get(key)
-    ai = alg_flops / alg_bytes
-    roof = {"bound": "hbm", "achieved": alg_bytes / dom_s / 1e9, "peak": pk["hbm_gbs"],
-            "unit": "GB/s", "frac": alg_bytes / dom_s / 1e9 / pk["hbm_gbs"],
-            "traffic": traffic, "kernel": key, "alg_bytes_per_launch": alg_bytes,
-            "alg_flops_per_launch": alg_flops, "ms_per_launch": per_kernel_ms[dom],
-            "peak_source": pk["source"], "arith_intensity": ai}
-    if dcfg is not None and dcfg.algo in (2, 3, 4):
-        ridge = pk["bf16_tflops_sustained"] * 1e12 / (pk["hbm_gbs"] * 1e9)
-        # tensor work in BF16-product units: a TF32 product runs at half the
-        # BF16 rate, so TF32X3's three count as six
-        products = {2: 3, 3: 6, 4: 6}[dcfg.algo]
-        if ai * products > ridge:
-            tc = alg_flops * products / dom_s / 1e12
-            roof.update({"bound": "tensor", "achieved": tc, "peak": pk["bf16_tflops_sustained"],
-                         "unit": "TFLOP/s", "frac": tc / pk["bf16_tflops_sustained"]})
-    if dcfg is not None and dcfg.algo == 1:
-        # SIMT FP32: nominal 148 SMs x 128 FMA lanes x 2 x 1.965 GHz
-        roof["simt_fp32_tflops"] = alg_flops / dom_s / 1e12
-        roof["simt_fp32_peak_nominal"] = 148 * 128 * 2 * 1.965e-3
-
     per_shape = []
     for j, (k, M, N, K, A, B, C, cfg) in enumerate(bufs):
         entry = {"kind": k, "M": M, "N": N, "K": K, "ms": per_kernel_ms[j],
                  "tflops": flops_of(k, M, N, K) / (per_kernel_ms[j] * 1e-3) / 1e12,
                  "gbs": bytes_of(k, M, N, K) / (per_kernel_ms[j] * 1e-3) / 1e9,
                  "config": repr(cfg) if cfg is not None else "gemv"}
-        if k == "sgemm" and rank == 0:
+        if k == "sgemm" and rank == 0 and err_check:
             err = hml.error_fp64(0, 0, 0, M, N, K, 1.0, A, M, B, K, 0.0, None, C, M)
             entry["max_rel_err_fp64"] = err[0]
             entry["rms_rel_err_fp64"] = err[1]
             entry["compwise_err_fp64"] = err[2]
         per_shape.append(entry)
+    step_flops = sum(flops_of(k, M, N, K) for (k, M, N, K, *_r) in bufs)
+    return {"bufs": bufs, "elapsed_ms": elapsed_ms, "per_kernel_ms": per_kernel_ms,
+            "launches": launches, "per_shape": per_shape, "step_flops": step_flops,
+            "value": step_flops * steps * ctx.world / (elapsed_ms * 1e-3) / 1e12,
+            "ms_per_step": elapsed_ms / steps}
+
+
+def roofline_of(kind, M, N, K, cfg, ms, key, pk):
+    """Roofline of one kernel launch.  Memory-bound forms (every SIMT and GEMV
+    launch, and the split forms below their tensor ridge): the algorithmic
+    bytes (A and B read once, C written once) over the launch time against
+    the measured HBM copy rate.  A split form above its ridge (the square
+    problem) is bounded by the tensor pipe: useful FLOP/s against the
+    sustained BF16 peak divided by the form's BF16 products per useful
+    multiply-add.  tensor_pipe_frac reports the tensor-pipe work the split
+    forms do (BF16-product units) against the sustained BF16 peak."""
+    alg_bytes = bytes_of(kind, M, N, K)
+    alg_flops = flops_of(kind, M, N, K)
+    s = ms * 1e-3
+    ai = alg_flops / alg_bytes
+    roof = {"bound": "hbm", "achieved": alg_bytes / s / 1e9, "peak": pk["hbm_gbs"],
+            "unit": "GB/s", "frac": alg_bytes / s / 1e9 / pk["hbm_gbs"],
+            "traffic": traffic_table().get(key), "kernel": key,
+            "alg_bytes_per_launch": alg_bytes, "alg_flops_per_launch": alg_flops,
+            "ms_per_launch": ms, "peak_source": pk["source"], "arith_intensity": ai}
+    if cfg is not None and cfg.algo in PRODUCTS:
+        products = PRODUCTS[cfg.algo]
+        tensor_peak = pk["bf16_tflops_sustained"]
+        roof["tensor_pipe_frac"] = alg_flops * products / s / 1e12 / tensor_peak
+        roof["tensor_products_per_mac"] = products
+        useful_cap = tensor_peak / products  # TFLOP/s of useful work at the tensor peak
+        hbm_time = alg_bytes / (pk["hbm_gbs"] * 1e9)
+        tensor_time = alg_flops / (useful_cap * 1e12)
+        if tensor_time > hbm_time:
+            roof.update({"bound": "tensor", "achieved": alg_flops / s / 1e12, "peak": useful_cap,
+                         "unit": "TFLOP/s (useful 2MNK; peak = sustained BF16 / products)",
+                         "frac": alg_flops / s / 1e12 / useful_cap})
+    if cfg is not None and cfg.algo == 1:
+        roof["simt_fp32_tflops"] = alg_flops / s / 1e12
+        roof["simt_fp32_peak_nominal"] = SIMT_PEAK_NOMINAL
+        roof["simt_fp32_frac_nominal"] = alg_flops / s / 1e12 / SIMT_PEAK_NOMINAL
+    return roof
+
+
+def kernel_key(workload, kind, M, N, K, cfg):
+    return f"{workload}:{kind}:{M}x{N}x{K}:{ALGO_NAMES.get(cfg.algo, 'gemv') if cfg else 'gemv'}"
+
+
+def workload_entry(ctx, name, algo=None, dist="uniform", steps=10, warmup=3):
+    """One short measured entry of a non-headline configuration."""
+    problems = workload_problems(name)
+    r = measure_gemms(ctx, problems, algo, dist, steps, warmup, flush_l2=(name == "c1"))
+    pk = peaks()
+    dom = max(range(len(r["bufs"])), key=lambda j: r["per_kernel_ms"][j])
+    k, M, N, K, *_x, cfg = r["bufs"][dom]
+    roof = roofline_of(k, M, N, K, cfg, r["per_kernel_ms"][dom],
+                       kernel_key(name, k, M, N, K, cfg), pk)
+    errs = [e for e in r["per_shape"] if "max_rel_err_fp64" in e]
+    step_bytes = sum(bytes_of(k, M, N, K) for (k, M, N, K, *_r) in r["bufs"])
+    out = {"workload": name, "config": config_desc(name, dist),
+           "selection": "automatic" if algo is None else f"forced {ALGO_NAMES[algo]}",
+           "steps": steps, "warmup": warmup, "ms_per_step": r["ms_per_step"],
+           "tflops": r["value"] / ctx.world,
+           "gbs": step_bytes / (r["ms_per_step"] * 1e-3) / 1e9,
+           "roofline": {kk: roof[kk] for kk in ("bound", "achieved", "peak", "unit", "frac",
+                                                "kernel", "tensor_pipe_frac")
+                        if kk in roof},
+           "per_shape": r["per_shape"]}
+    if errs:
+        out["max_rel_err_fp64"] = max(e["max_rel_err_fp64"] for e in errs)
+        out["compwise_err_fp64"] = max(e["compwise_err_fp64"] for e in errs)
+    return out
+
+
+def predictor_entry(ctx, live_shapes=4, live_reps=3):
+    """Regret of the shipped configuration predictor: on the 1000 held-out
+    shapes of the measured dataset (exhaustive autotune times), against the
+    best fixed configuration and the built-in heuristic; and live, on a few
+    unseen shapes autotuned now over the FP32-accurate families."""
+    import numpy as np
+
+    import hiperml_b200 as hml
+    from hiperml_b200 import predictor as pr
+    from hiperml_b200 import tuning_data as td
+    if not (os.path.exists(pr.DATASET) and os.path.exists(pr.MODEL)):
+        return {"workload": "predictor", "unavailable": "no shipped dataset or network"}
+    d = td.load(pr.DATASET)
+    shapes, times, cfgs = d["shapes"], d["times_us"], d["configs"]
+    n_tr = min(4000, int(0.8 * len(shapes)))
+    te = slice(n_tr, None)
+    hml.tune_clear()
+    pr.load(pr.MODEL)
+    t0 = time.perf_counter()
+    pred = pr.predict_batch(shapes[te])
+    r_pred = pr.summarize(pr.regret(times[te], pred, cfgs))
+    fixed = pr.best_fixed_config(times[:n_tr], cfgs)
+    r_fixed = pr.summarize(pr.regret(times[te], np.full(len(pred), fixed), cfgs))
+    live = []
+    cfg_t = [tuple(int(x) for x in c) for c in cfgs]
+    for (M, N, K, ta, tb) in td.sample_shapes(live_shapes, 4242):
+        j = pr.predict_batch(np.array([[M, N, K, ta, tb]]))[0]
+        ents = hml.autotune(0, int(ta), int(tb), int(M), int(N), int(K),
+                            families=(1 << hml.ALGO_SIMT) | (1 << hml.ALGO_BF16X6), reps=live_reps)
+        t = {c.as_tuple(): us for c, us, st in ents if st == 0 and us > 0}
+        if cfg_t[j] in t:
+            live.append({"shape": [int(M), int(N), int(K), int(ta), int(tb)],
+                         "regret": t[cfg_t[j]] / min(t.values()) - 1.0})
+    hml.tune_clear()
+    pr.clear()
+    heur = pr.heuristic_choices(shapes[te], cfgs)
+    r_heur = pr.summarize(pr.regret(times[te], heur, cfgs))
+    return {"workload": "predictor",
+            "config": {"dataset": "5000 shapes (M,N,K log-uniform [1,65536]x[1,256]x[16,16384], "
+                                  "random transposes), each autotuned over the configuration "
+                                  "space on a B200; network trained on the first 4000",
+                       "held_out": int(len(pred))},
+            "held_out_regret": r_pred, "fixed_default_regret": r_fixed,
+            "heuristic_regret": r_heur,
+            "live_regret": live,
+            "live_regret_mean": (float(np.mean([x["regret"] for x in live])) if live else None),
+            "seconds": time.perf_counter() - t0}
+
+
+def run_ours(args):
+    import torch
+
+    import hiperml_b200 as hml
+    from hiperml_b200.dist import max_over_ranks
+
+    ctx = Ctx()
+    algo = {"auto": None, "simt": 1, "bf16x3": 2, "bf16x6": 3, "tf32x3": 4}[args.algo]
+    problems = workload_problems(args.workload, args.rows, args.only_n)
+    clocks = ClockSampler(ctx.local)
+    r = measure_gemms(ctx, problems, algo, args.dist, args.steps, args.warmup,
+                      flush_l2=(args.workload == "c1"), clocks=clocks)
+    bufs = r["bufs"]
+    pk = peaks()
+    # dominant kernel = longest per-launch time
+    dom = max(range(len(bufs)), key=lambda j: r["per_kernel_ms"][j])
+    k, M, N, K, *_x, dcfg = bufs[dom]
+    roof = roofline_of(k, M, N, K, dcfg, r["per_kernel_ms"][dom],
+                       kernel_key(args.workload, k, M, N, K, dcfg), pk)
 
     # ---- end to end through the host-pointer C ABI (pinned host buffers)
     e2e = None
     if not args.no_e2e and all(b[0] == "sgemm" for b in bufs):
         e2e_steps = max(1, min(args.steps, 5))
         hosts = []
-        for (k, M, N, K, A, B, C, cfg) in bufs:
-            hA = A.cpu().pin_memory() if not hosts or hosts[-1][0].numel() != A.numel() else hosts[-1][0]
+        for (k_, M_, N_, K_, A, B, C, cfg) in bufs:
+            hA = A.cpu().pin_memory() if not hosts or hosts[-1][0].numel() != A.numel() \
+                else hosts[-1][0]
             hB = B.cpu().pin_memory()
-            hC = torch.empty(M * N, dtype=torch.float32).pin_memory()
-            hosts.append((hA, hB, hC, M, N, K))
+            hC = torch.empty(M_ * N_, dtype=torch.float32).pin_memory()
+            hosts.append((hA, hB, hC, M_, N_, K_))
+
         # column-major C = A B  ==  row-major C^T = B^T A^T : hmlSgemm(C, B, A, N, M, K)
         def e2e_step():
-            for (hA, hB, hC, M, N, K) in hosts:
-                from hiperml_b200._lib import check
+            from hiperml_b200._lib import check
+            for (hA, hB, hC, M_, N_, K_) in hosts:
                 check(hml.lib.hml_host_sgemm(0, hC.data_ptr(), hB.data_ptr(), hA.data_ptr(),
-                                             N, M, K, 1.0, 0.0), "hml_host_sgemm")
+                                             N_, M_, K_, 1.0, 0.0), "hml_host_sgemm")
         e2e_step()
-        if dist_on:
-            dist.barrier()
+        ctx.barrier()
         ts = time.perf_counter()
         for _ in range(e2e_steps):
             e2e_step()
         te = time.perf_counter() - ts
-        te = max_over_ranks(te, dev)
-        h2d = sum(4 * (M * K + K * N) for (_, _, _, M, N, K) in hosts)
-        d2h = sum(4 * M * N for (_, _, _, M, N, K) in hosts)
-        e2e = {"value": step_flops * e2e_steps * world / te / 1e12, "unit": UNIT,
+        te = max_over_ranks(te, ctx.dev)
+        h2d = sum(4 * (M_ * K_ + K_ * N_) for (_, _, _, M_, N_, K_) in hosts)
+        d2h = sum(4 * M_ * N_ for (_, _, _, M_, N_, K_) in hosts)
+        e2e = {"value": r["step_flops"] * e2e_steps * ctx.world / te / 1e12, "unit": UNIT,
                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                "api": "hml_host_sgemm (reference-facing hmlSgemm ABI), pinned host buffers",
                "steps": e2e_steps}
+        del hosts
 
     cpu = None
-    if not args.no_cpu_baseline and rank == 0 and world == 1:
-        v, cores, kind, desc = cpu_reference_sample([(k, M, N, K) for (k, M, N, K, *_r) in bufs],
-                                                    seconds=10.0)
+    if not args.no_cpu_baseline and ctx.rank == 0 and ctx.world == 1:
+        v, cores, kind, desc, _, _ = cpu_reference_sample(
+            [(k_, M_, N_, K_) for (k_, M_, N_, K_, *_r) in bufs], seconds=10.0)
         cpu = {"value": v, "unit": UNIT, "cores": cores, "kind": kind, "sample": desc}
 
-    if rank == 0:
+    # ---- the other configurations, one short entry each (default run only)
+    workloads = None
+    if (args.workload == "sweep" and not args.no_workloads and args.rows is None
+            and args.only_n is None and algo is None and args.dist == "uniform"):
+        del bufs
+        r.pop("bufs")
+        torch.cuda.empty_cache()
+        workloads = []
+        for name, a, dist_ in (("c1", None, "uniform"), ("gemv_n", None, "uniform"),
+                               ("gemv_t", None, "uniform"), ("square", None, "uniform"),
+                               ("square", None, "loguniform"), ("sweep", None, "loguniform"),
+                               ("sweep", 1, "uniform")):
+            workloads.append(workload_entry(ctx, name, a, dist_))
+            torch.cuda.empty_cache()
+        simt = workloads[-1]
+        workloads.append({"workload": "split_over_simt",
+                          "sweep_speedup": r["value"] / (simt["tflops"] * ctx.world),
+                          "per_n_speedup": {
+                              str(s["N"]): simt["per_shape"][i]["ms"] / r["per_shape"][i]["ms"]
+                              for i, s in enumerate(r["per_shape"])}})
+        workloads.append(batched_entry(ctx, steps=10, warmup=3))
+        torch.cuda.empty_cache()
+        if ctx.rank == 0:
+            workloads.append(predictor_entry(ctx))
+
+    if ctx.rank == 0:
         line = {
-            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "metric": METRIC, "value": r["value"], "unit": UNIT, "n_gpus": ctx.world,
             "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": elapsed_ms / args.steps, "higher_is_better": True,
+            "ms_per_step": r["ms_per_step"], "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": dict(config_desc(args.workload),
-                           parallelism=f"independent per-GPU problems x{world}",
-                           selection=("the library's automatic choice: the B200 tuned table "
-                                      "shipped as data/tuned_b200.txt (autotuner-measured), "
-                                      "else the learned predictor" if algo is None else
-                                      f"forced family {args.algo}: the library's heuristic "
-                                      "configuration of that family"),
-                           **({"rows_override": args.rows} if args.rows else {}),
-                           **({"only_n": args.only_n} if args.only_n else {})),
+            "config": config_desc(args.workload, args.dist),
+            "run": {"parallelism": f"independent per-GPU problems x{ctx.world}",
+                    "selection": ("the library's automatic choice: the B200 tuned table "
+                                  "shipped as data/tuned_b200.txt (autotuner-measured), "
+                                  "else the learned predictor" if algo is None else
+                                  f"forced family {args.algo}: the library's heuristic "
+                                  "configuration of that family"),
+                    **({"rows_override": args.rows} if args.rows else {}),
+                    **({"only_n": args.only_n} if args.only_n else {})},
             "roofline": roof, "cpu_baseline": cpu, "e2e": e2e,
-            "clocks": clocks.summary(), "gpu_launches": int(launches),
-            "per_shape": per_shape,
+            "clocks": clocks.summary(), "gpu_launches": int(r["launches"]),
+            "per_shape": r["per_shape"],
         }
+        if workloads is not None:
+            line["workloads"] = workloads
         print(json.dumps(line), flush=True)
-    if dist_on:
-        dist.barrier()
-        dist.destroy_process_group()
+    ctx.close()
     return 0
 
 
-def run_batched(args):
+def batched_entry(ctx, steps, warmup, clocks=None, with_e2e=False):
     """The batched workload: one persistent launch (replayed from a CUDA
     graph) per step, against the same 1024 problems as separate calls."""
-    import numpy as np
+    import numpy as np  # noqa: F401
     import torch
 
     import hiperml_b200 as hml
     from hiperml_b200 import datagen as dg
     from hiperml_b200.dist import max_over_ranks
 
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    dist_on = world > 1
-    if dist_on:
-        import datetime
-
-        import torch.distributed as dist
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-    dev = torch.device("cuda", local)
-    torch.cuda.set_device(dev)
-    stream = torch.cuda.current_stream()
-
+    dev, stream, rank, world = ctx.dev, ctx.stream, ctx.rank, ctx.world
     shapes = batch_shapes()
     r4 = lambda x: (x + 3) // 4 * 4
     a64 = lambda x: (x + 63) // 64 * 64
@@ -589,33 +763,32 @@ def run_batched(args):
     plan = hml.BatchPlan(hml.COL_MAJOR, descs)
     info = plan.info()
 
-    for _ in range(args.warmup):
+    for _ in range(warmup):
         plan.graph_launch(stream)
     torch.cuda.synchronize()
-    if dist_on:
-        dist.barrier()
+    ctx.barrier()
     torch.cuda.synchronize()
     evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
-           for _ in range(args.steps)]
+           for _ in range(steps)]
     launches0 = hml.lib.hml_launch_count()
     t0 = torch.cuda.Event(enable_timing=True)
     t1 = torch.cuda.Event(enable_timing=True)
-    with ClockSampler(local) as clocks:
+    sampler = clocks if clocks is not None else ClockSampler(ctx.local, period=1.0)
+    with sampler:
         t0.record(stream)
-        for i in range(args.steps):
+        for i in range(steps):
             evs[i][0].record(stream)
             plan.graph_launch(stream)
             evs[i][1].record(stream)
         t1.record(stream)
         torch.cuda.synchronize()
     launches = hml.lib.hml_launch_count() - launches0
-    if dist_on:
-        dist.barrier()
+    ctx.barrier()
     elapsed_ms = t0.elapsed_time(t1)
     per_launch_ms = statistics.mean(a.elapsed_time(b) for a, b in evs)
     elapsed_ms = max_over_ranks(elapsed_ms, dev)
     step_flops = info["flops"]
-    value = step_flops * args.steps * world / (elapsed_ms * 1e-3) / 1e12
+    value = step_flops * steps * world / (elapsed_ms * 1e-3) / 1e12
 
     # ---- accuracy on a sample of problems (FP64 on the GPU)
     errs = []
@@ -627,7 +800,7 @@ def run_batched(args):
 
     # ---- the same problems as 1024 separate calls (device pointers)
     def separate(config_of):
-        reps = max(1, min(args.steps, 3))
+        reps = max(1, min(steps, 3))
         cfgs = [config_of(d) for d in descs]
         for d, c in zip(descs, cfgs):  # warm-up
             hml.sgemm_ex(0, d[0], d[1], d[2], d[3], d[4], 1.0, d[6], d[7], d[8], d[9], 0.0, d[11],
@@ -650,11 +823,11 @@ def run_batched(args):
     # ---- end to end: pinned host operands copied in, one graph launch,
     # every C copied back
     e2e = None
-    if not args.no_e2e:
+    if with_e2e:
         hA = poolA.cpu().pin_memory()
         hB = poolB.cpu().pin_memory()
         hC = torch.empty(poolC.numel(), dtype=torch.float32).pin_memory()
-        reps = max(1, min(args.steps, 2))
+        reps = max(1, min(steps, 2))
 
         def e2e_step():
             poolA.copy_(hA, non_blocking=True)
@@ -684,41 +857,48 @@ def run_batched(args):
             "kernel": "batch plan (tc_batch_kernel<32|64|128> + batched_kernel + split_b_batch_kernel)",
             "alg_bytes_per_launch": alg_bytes, "alg_flops_per_launch": step_flops,
             "ms_per_launch": per_launch_ms, "peak_source": pk["source"],
-            "simt_fp32_tflops": step_flops / dom_s / 1e12,
-            "simt_fp32_peak_nominal": 148 * 128 * 2 * 1.965e-3,
+            "useful_tflops": step_flops / dom_s / 1e12,
             "note": ("one graph launch of the whole plan: BF16X6 tensor-core tiles for N > 8 "
-                     "(tc_batch_kernel<128,3> dominates) and FP32 SIMT tiles for N <= 8; "
-                     "achieved = the plan's algorithmic bytes over its event-timed duration")}
-
-    cpu = None
-    if not args.no_cpu_baseline and rank == 0 and world == 1:
-        sample = [("sgemm", M, N, K) for (_ta, _tb, M, N, K) in shapes[:64]]
-        v, cores, kind, desc = cpu_reference_sample(sample, seconds=10.0)
-        cpu = {"value": v, "unit": UNIT, "cores": cores, "kind": kind,
-               "sample": "first 64 problems of the batch: " + desc}
-
-    if rank == 0:
-        line = {
-            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
-            "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": elapsed_ms / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": dict(config_desc("batched"),
-                           parallelism=f"independent per-GPU batches x{world}"),
-            "roofline": roof, "cpu_baseline": cpu, "e2e": e2e,
-            "clocks": clocks.summary(), "gpu_launches": int(launches),
+                     "and FP32 SIMT tiles for N <= 8; achieved = the plan's algorithmic bytes "
+                     "over its event-timed duration")}
+    plan.close()
+    return {"workload": "batched", "value": value, "elapsed_ms": elapsed_ms,
+            "ms_per_step": elapsed_ms / steps, "steps": steps, "warmup": warmup,
+            "tflops": value / world, "launches": launches, "roofline": roof, "e2e": e2e,
+            "config": config_desc("batched"),
             "batch": {"tiles": info["tiles"], "ctas": info["ctas"],
                       "separate_simt_calls_tflops": sep_simt,
                       "separate_auto_calls_tflops": sep_auto,
                       "speedup_vs_separate_simt": value / world / sep_simt,
+                      "speedup_vs_separate_auto": value / world / sep_auto,
                       "max_rel_err_fp64_sample": max(e[0] for e in errs) if errs else None,
-                      "max_compwise_err_fp64_sample": max(e[2] for e in errs) if errs else None},
+                      "max_compwise_err_fp64_sample": max(e[2] for e in errs) if errs else None}}
+
+
+def run_batched(args):
+    ctx = Ctx()
+    clocks = ClockSampler(ctx.local)
+    b = batched_entry(ctx, args.steps, args.warmup, clocks=clocks, with_e2e=not args.no_e2e)
+    cpu = None
+    if not args.no_cpu_baseline and ctx.rank == 0 and ctx.world == 1:
+        sample = [("sgemm", M, N, K) for (_ta, _tb, M, N, K) in batch_shapes()[:64]]
+        v, cores, kind, desc, _, _ = cpu_reference_sample(sample, seconds=10.0)
+        cpu = {"value": v, "unit": UNIT, "cores": cores, "kind": kind,
+               "sample": "first 64 problems of the batch: " + desc}
+    if ctx.rank == 0:
+        line = {
+            "metric": METRIC, "value": b["value"], "unit": UNIT, "n_gpus": ctx.world,
+            "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": b["ms_per_step"], "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": config_desc("batched"),
+            "run": {"parallelism": f"independent per-GPU batches x{ctx.world}"},
+            "roofline": b["roofline"], "cpu_baseline": cpu, "e2e": b["e2e"],
+            "clocks": clocks.summary(), "gpu_launches": int(b["launches"]),
+            "batch": b["batch"],
         }
         print(json.dumps(line), flush=True)
-    plan.close()
-    if dist_on:
-        dist.barrier()
-        dist.destroy_process_group()
+    ctx.close()
     return 0
 
 

@@ -96,6 +96,8 @@ _SIGS = {
     "hml_cfg_v1_sgemm_rule": (c_int, [c_int, c_int, c_int_p, c_int_p]),
     "hml_cfg_v1_sgemv_rule": (c_int, [c_int, c_int_p, c_int_p, c_int_p]),
     "hml_cfg_v1_clear": (None, []),
+    "hml_cfg_v1_save": (c_int, [c_int, c_char_p]),
+    "hml_sgemm_v1_config": (c_int, [c_int, c_int, c_int, ctypes.POINTER(SgemmConfig)]),
     "hml_fill_random": (c_int, [c_void_p, c_size_t, c_uint64, c_uint64, c_int, c_void_p]),
     "hml_sgemm_error_fp64": (c_int, [c_int, c_int, c_int, c_int, c_int, c_int, c_float, c_void_p,
                                      c_int, c_void_p, c_int, c_float, c_void_p, c_void_p, c_int,

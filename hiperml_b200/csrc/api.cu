@@ -371,13 +371,21 @@ hml_status hml_sgemm_error_fp64(hml_order order, hml_op transA, hml_op transB, i
 
 hml_status hml_device_error(int *code) {
   if (!code) return HML_STATUS_INVALID_VALUE;
-  int *w = device_error_word();
-  if (!w) return HML_STATUS_ALLOC_FAILED;
+  *code = 0;
+  // the allocation-free entry point's own word first; it allocates nothing
+  int na = 0;
+  hml_status st = noalloc_take_error(&na);
+  if (st != HML_STATUS_SUCCESS) return st;
+  // the library's word exists once a kernel that records errors has run
+  int *w = device_error_word_if_any();
   int h = 0;
-  cudaError_t e = cudaMemcpy(&h, w, sizeof(int), cudaMemcpyDeviceToHost);
-  if (e == cudaSuccess && h != 0) e = cudaMemset(w, 0, sizeof(int));
-  note_cuda_error(e, "device_error");
-  *code = h;
+  cudaError_t e = cudaSuccess;
+  if (w) {
+    e = cudaMemcpy(&h, w, sizeof(int), cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess && h != 0) e = cudaMemset(w, 0, sizeof(int));
+    note_cuda_error(e, "device_error");
+  }
+  *code = h != 0 ? h : na;
   return cuda_status(e);
 }
 

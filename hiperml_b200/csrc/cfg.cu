@@ -11,10 +11,18 @@
 // cHmlMaxBlockStops = 16) and a malformed or out-of-range line rejects the
 // whole file with HML_STATUS_CONFIG_ERROR instead of writing out of bounds.
 //
-// The rules name Fermi/Kepler kernels that do not exist here.  They are kept
-// as hints: an SGEMM rule's rowStops picks the SIMT tile height closest to
-// 16*rowStops, an SGEMV rule's blockStops picks 16*blockStops threads per
-// row of the row kernel.  A measured B200 table always takes precedence.
+// The rules name Fermi/Kepler kernels that do not exist here.  They steer
+// the reference-facing host calls, as in the reference: hmlSgemm runs a
+// problem a rule covers on the tiled SIMT kernel with the tile nearest to the
+// rule's (16*rowStops rows, 16*colStops columns; select.cu v1_rule_config),
+// hmlSgemv on the row kernel with 16*blockStops threads per row.  The
+// device-pointer ABI (hml_sgemm_ex, hml_sgemv_ex) ignores them and keeps the
+// measured B200 table.
+//
+// cfg_v1_save writes the loaded rules back in the same grammar and in the
+// order of the reference's printers (src/hml_sgemm_kernel.cu:557-568,
+// src/hml_sgemv_kernel.cu:634-645): SGEMM for K = 2..96 and colStops =
+// 1..16, SGEMV for N = 0..1024, each rule whose rowStops is positive.
 #include <cstdio>
 #include <cstring>
 #include <mutex>
@@ -95,7 +103,55 @@ hml_status cfg_v1_load(int kind, const char *path, int *rules) {
     g_sgemv_loaded = true;
   }
   if (rules) *rules = n;
+  if (kind == 0)
+    fprintf(stderr,
+            "hml: %d SGEMM v1 rules from %s: hmlSgemm maps them onto FP32 SIMT tiles; "
+            "hml_sgemm_ex keeps the measured B200 table\n",
+            n, path);
   return HML_STATUS_SUCCESS;
+}
+
+hml_status cfg_v1_save(int kind, const char *path) {
+  if (!path || (kind != 0 && kind != 1)) return HML_STATUS_INVALID_VALUE;
+  std::vector<SgemmRule> gm;
+  std::vector<SgemvRule> gv;
+  {
+    std::lock_guard<std::mutex> lk(g_mu);
+    if (kind == 0 ? !g_sgemm_loaded : !g_sgemv_loaded) return HML_STATUS_CONFIG_ERROR;
+    if (kind == 0) {
+      for (int K = 0; K <= kMaxK; ++K)
+        for (int c = 0; c <= kMaxStops; ++c) gm.push_back(g_sgemm[K][c]);
+    } else {
+      gv.assign(g_sgemv, g_sgemv + kMaxN + 1);
+    }
+  }
+  FILE *f = fopen(path, "wb");
+  if (!f) return HML_STATUS_IO_ERROR;
+  bool ok = true;
+  if (kind == 0) {
+    ok = fprintf(f,
+                 "#SGEMM smart kernel config file v1.0\n"
+                 "#written by hml-b200 from the rules it loaded\n"
+                 "#rule: K colStops : kernelType rowStops  (kernelType 0 basic, 1 var-K, "
+                 "2 const-K; colStops = (N + 15) / 16)\n") > 0;
+    for (int K = 2; ok && K <= kMaxK; ++K)
+      for (int c = 1; ok && c <= kMaxStops; ++c) {
+        const SgemmRule &r = gm[K * (kMaxStops + 1) + c];
+        if (r.row_stops > 0) ok = fprintf(f, "%d %d : %d %d\n", K, c, r.type, r.row_stops) > 0;
+      }
+  } else {
+    ok = fprintf(f,
+                 "#SGEMV smart kernel config file v1.0\n"
+                 "#written by hml-b200 from the rules it loaded\n"
+                 "#rule: N : kernelType blockStops rowStops  (N 0 serves N > 1024)\n") > 0;
+    for (int N = 0; ok && N <= kMaxN; ++N) {
+      const SgemvRule &r = gv[N];
+      if (r.row_stops > 0)
+        ok = fprintf(f, "%d : %d %d %d\n", N, r.type, r.block_stops, r.row_stops) > 0;
+    }
+  }
+  if (fclose(f) != 0) ok = false;
+  return ok ? HML_STATUS_SUCCESS : HML_STATUS_IO_ERROR;
 }
 
 // The reference's keying: K' = min(K, 96), colStops = ceil(min(N, 96) / 16)
@@ -148,6 +204,8 @@ hml_status hml_cfg_v1_sgemv_rule(int N, int *type, int *block_stops, int *row_st
   return hml::cfg_v1_sgemv_rule(N, type, block_stops, row_stops) ? HML_STATUS_SUCCESS
                                                                   : HML_STATUS_CONFIG_ERROR;
 }
+
+hml_status hml_cfg_v1_save(int kind, const char *path) { return hml::cfg_v1_save(kind, path); }
 
 void hml_cfg_v1_clear(void) { hml::cfg_v1_clear(); }
 

@@ -102,6 +102,9 @@ hml_status check_wait_limit(cudaStream_t s);
 
 // Per-device resources.
 int *device_error_word();  // nullptr on failure
+int *device_error_word_if_any();  // nullptr when not allocated yet (allocates nothing)
+// Reads and clears the allocation-free entry point's error word (sgemm_tc.cu).
+hml_status noalloc_take_error(int *code);
 hml_status workspace(size_t bytes, cudaStream_t s, void **ptr);
 // n zero-initialised counters private to (device, stream).  Kernels that use
 // them leave every counter at zero again when they finish.

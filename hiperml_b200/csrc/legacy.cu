@@ -154,9 +154,20 @@ hml_status host_sgemm(bool basic, float *C, const float *A, const float *B, int 
         st = run_config(p, cfg, h.comp);
       }
     } else {
-      st = hml_sgemm_ex(HML_ROW_MAJOR, HML_OP_N, HML_OP_N, rc, N, K, alpha,
-                        dA + static_cast<size_t>(r0) * K, K, dB, N, beta,
-                        dC + static_cast<size_t>(r0) * N, N, h.comp);
+      // a loaded reference v1 rule decides, as in the reference's hmlSgemm
+      // (src/hml_sgemm.cu:166-167); otherwise the library's own selection
+      GemmProblem p;
+      st = gemm_from_blas(HML_ROW_MAJOR, HML_OP_N, HML_OP_N, rc, N, K, alpha,
+                          dA + static_cast<size_t>(r0) * K, K, dB, N, beta,
+                          dC + static_cast<size_t>(r0) * N, N, &p);
+      if (st != HML_STATUS_SUCCESS) return st;
+      hml_sgemm_config v1;
+      if (p.N > 1 && p.K > 0 && p.alpha != 0.0f && v1_rule_config(p, K, N, &v1))
+        st = run_config(p, v1, h.comp);
+      else
+        st = hml_sgemm_ex(HML_ROW_MAJOR, HML_OP_N, HML_OP_N, rc, N, K, alpha,
+                          dA + static_cast<size_t>(r0) * K, K, dB, N, beta,
+                          dC + static_cast<size_t>(r0) * N, N, h.comp);
     }
     if (st != HML_STATUS_SUCCESS) return st;
     HML_TRY(cudaEventRecord(h.out_ready[c], h.comp));
@@ -292,5 +303,20 @@ hml_status hml_host_sgemv(int basic, float *y, const float *A, const float *x, i
 }
 
 hml_status hml_config_file(int kind, const char *path) { return hml::config_file(kind, path); }
+
+hml_status hml_sgemm_v1_config(int M, int N, int K, hml_sgemm_config *config) {
+  using namespace hml;
+  if (!config) return HML_STATUS_INVALID_VALUE;
+  if (M < 1 || N < 1 || K < 1) return HML_STATUS_INVALID_VALUE;
+  // a dense row-major problem on aligned dummy pointers: only the layout and
+  // the sizes matter to the choice
+  alignas(16) static float dummy[4];
+  GemmProblem p;
+  hml_status st = gemm_from_blas(HML_ROW_MAJOR, HML_OP_N, HML_OP_N, M, N, K, 1.0f, dummy, K,
+                                 dummy, N, 0.0f, dummy, N, &p);
+  if (st != HML_STATUS_SUCCESS) return st;
+  if (p.N <= 1) return HML_STATUS_CONFIG_ERROR;  // served by the GEMV kernels
+  return v1_rule_config(p, K, N, config) ? HML_STATUS_SUCCESS : HML_STATUS_CONFIG_ERROR;
+}
 
 }  // extern "C"

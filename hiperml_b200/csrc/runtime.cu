@@ -64,6 +64,13 @@ int sm_count() {
   return n;
 }
 
+int *device_error_word_if_any() {
+  const int d = current_device();
+  std::lock_guard<std::mutex> lk(g_mu);
+  auto it = g_err_words.find(d);
+  return it != g_err_words.end() ? it->second : nullptr;
+}
+
 int *device_error_word() {
   const int d = current_device();
   std::lock_guard<std::mutex> lk(g_mu);

@@ -20,6 +20,7 @@ int tc_num_shapes();
 void tc_shape(int v, int *bm, int *bn);
 bool tc_config_fits(int bn, int ns, int stages);
 int tc_ns(int algo);
+bool cfg_v1_sgemm_rule(int K, int N, int *type, int *row_stops);
 
 namespace {
 
@@ -81,6 +82,12 @@ hml_sgemm_config heuristic_config(const GemmProblem &p, int algo) {
   else if (p.N <= 32) var = (p.M >= 256 * 2 * sm_count()) ? 3 : 2;
   else if (p.N <= 64) var = (p.M >= 256 * sm_count()) ? 4 : 7;
   else var = (p.M >= 256 * sm_count()) ? 5 : 8;
+  return simt_config(p, var);
+}
+
+// The tiled SIMT configuration of micro-tile shape `var` for this problem:
+// split_k so the grid covers the machine, the deepest ring that fits.
+hml_sgemm_config simt_config(const GemmProblem &p, int var) {
   int bm, bn, wk;
   simt_shape(var, &bm, &bn, &wk);
   const int per_sm = (bm * bn <= 128 * 16 * 2) ? 2 : 1;
@@ -91,8 +98,44 @@ hml_sgemm_config heuristic_config(const GemmProblem &p, int algo) {
   int stages = 2;
   for (int s : {3, 4, 6})
     if (static_cast<size_t>(bm + bn) * 128 * s <= budget) stages = s;
-  c = {HML_ALGO_SIMT, bm, bn, split, stages, var};
-  return c;
+  return hml_sgemm_config{HML_ALGO_SIMT, bm, bn, split, stages, var};
+}
+
+// A reference v1 SGEMM rule (src/hml_sgemm_kernel.cu:189-237: kernel type
+// and rowStops for the class K' = min(K, 96), colStops = ceil(min(N, 96) /
+// 16) of a row-major M x N x K problem) mapped onto the tiled SIMT family,
+// the counterpart of the reference's tiled SIMT kernels: a tile of
+// 16 * rowStops rows (basic kernel: 6 x 6 stops) becomes the 128- or
+// 256-row SIMT tile nearest to it, its 16 * colStops columns the narrowest
+// SIMT tile width that holds min(N, 16 * colStops) of the problem's columns.
+// False when no rule applies or the mapped configuration cannot run.
+bool v1_rule_config(const GemmProblem &p, int K_row, int N_row, hml_sgemm_config *c) {
+  int type = 0, row_stops = 0;
+  if (!cfg_v1_sgemm_rule(K_row, N_row, &type, &row_stops)) return false;
+  const int col_stops = type == 0 ? 6 : (std::min(N_row, 96) + 15) / 16;
+  const int rows = 16 * (type == 0 ? 6 : row_stops);
+  const int want_m = rows >= 192 ? 256 : 128;
+  const int want_n = std::min(p.N, 16 * col_stops);
+  int best = -1, best_bn = 0, widest = -1, widest_bn = 0;
+  for (int v = 0; v < simt_num_shapes(); ++v) {
+    int bm, bn, wk;
+    simt_shape(v, &bm, &bn, &wk);
+    if (bm != want_m) continue;
+    if (bn >= want_n && (best < 0 || bn < best_bn)) {
+      best = v;
+      best_bn = bn;
+    }
+    if (bn > widest_bn) {
+      widest = v;
+      widest_bn = bn;
+    }
+  }
+  if (best < 0) best = widest;
+  if (best < 0) return false;
+  const hml_sgemm_config cand = simt_config(p, best);
+  if (!check_config_ok(p, cand)) return false;
+  *c = cand;
+  return true;
 }
 
 hml_status select_config(const GemmProblem &p, hml_sgemm_config *c, cudaStream_t s) {

@@ -1715,15 +1715,24 @@ namespace {
 
 constexpr size_t kNoAllocScratchBytes = size_t(4) << 20;  // 4 MiB per device
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+// The error word of the bounded waits of calls made through this entry point:
+// file scope too, so that no call allocates it.  hml_device_error reads and
+// clears it together with the library's other error word.
+static __device__ int g_noalloc_error;
 
 constexpr int kNoAllocMaxDevices = 64;
 std::mutex g_noalloc_mu;
-void *g_noalloc_addr[kNoAllocMaxDevices];
+struct NoAllocAddrs {
+  void *scratch = nullptr;
+  int *err = nullptr;
+};
+NoAllocAddrs g_noalloc_addr[kNoAllocMaxDevices];
 
-// Device address of the scratch array on the current device.  In host code
-// the array's name is only a host-side stand-in, so the address is looked up
-// once per device (with that device current) and cached.
-hml_status noalloc_scratch(void **out) {
+// Device addresses of the scratch array and the error word on the current
+// device.  In host code the arrays' names are only host-side stand-ins, so
+// the addresses are looked up once per device (with that device current) and
+// cached.
+hml_status noalloc_setup(NoAllocAddrs *out) {
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) {
@@ -1732,17 +1741,20 @@ hml_status noalloc_scratch(void **out) {
   }
   if (dev < 0 || dev >= kNoAllocMaxDevices) return HML_STATUS_NOT_SUPPORTED;
   std::lock_guard<std::mutex> lk(g_noalloc_mu);
-  if (!g_noalloc_addr[dev]) {
-    void *addr = nullptr;
-    e = cudaGetSymbolAddress(&addr, g_noalloc_scratch);
-    if (e != cudaSuccess || !addr) {
+  NoAllocAddrs &a = g_noalloc_addr[dev];
+  if (!a.scratch) {
+    void *scratch = nullptr, *err = nullptr;
+    e = cudaGetSymbolAddress(&scratch, g_noalloc_scratch);
+    if (e == cudaSuccess) e = cudaGetSymbolAddress(&err, g_noalloc_error);
+    if (e != cudaSuccess || !scratch || !err) {
       note_cuda_error(e != cudaSuccess ? e : cudaErrorInvalidSymbol,
                       "noalloc: cudaGetSymbolAddress");
       return HML_STATUS_CUDA_ERROR;
     }
-    g_noalloc_addr[dev] = addr;
+    a.err = static_cast<int *>(err);
+    a.scratch = scratch;
   }
-  *out = g_noalloc_addr[dev];
+  *out = a;
   return HML_STATUS_SUCCESS;
 }
 
@@ -1753,37 +1765,64 @@ size_t noalloc_bytes_needed(const GemmProblem &p, const hml_sgemm_config &c) {
   return static_cast<size_t>(ns) * n_pad * k_pad * 2;
 }
 
-// The launch of run_tc with the B planes in `planes` (the static array) and
-// no device error word (bounded waits still end; nothing is recorded).
+// The launch of run_tc with the B planes in the static array and the static
+// error word.
 template <int BN, int NS, bool AK>
-hml_status run_tc_static(const GemmProblem &p, const hml_sgemm_config &c, void *scratch,
+hml_status run_tc_static(const GemmProblem &p, const hml_sgemm_config &c, const NoAllocAddrs &a,
                          cudaStream_t s) {
   const int k_pad = ((p.K + kChunkK - 1) / kChunkK) * kChunkK;
   const int n_pad = ((p.N + BN - 1) / BN) * BN;
-  auto *planes = static_cast<__nv_bfloat16 *>(scratch);
+  auto *planes = static_cast<__nv_bfloat16 *>(a.scratch);
   hml_status st = split_b<NS>(p, planes, k_pad, n_pad, s);
   if (st != HML_STATUS_SUCCESS) return st;
-  return launch_tc_planes<BN, NS, AK>(p, c, planes, k_pad, n_pad, nullptr, s);
+  return launch_tc_planes<BN, NS, AK>(p, c, planes, k_pad, n_pad, a.err, s);
 }
 
 template <int NS>
-hml_status run_tc_static_ns(const GemmProblem &p, const hml_sgemm_config &c, void *scratch,
-                            cudaStream_t s) {
+hml_status run_tc_static_ns(const GemmProblem &p, const hml_sgemm_config &c,
+                            const NoAllocAddrs &a, cudaStream_t s) {
   const bool ak = p.a_kcontig();
   switch (c.tile_n) {
-    case 16: return ak ? run_tc_static<16, NS, true>(p, c, scratch, s)
-                       : run_tc_static<16, NS, false>(p, c, scratch, s);
-    case 32: return ak ? run_tc_static<32, NS, true>(p, c, scratch, s)
-                       : run_tc_static<32, NS, false>(p, c, scratch, s);
-    case 64: return ak ? run_tc_static<64, NS, true>(p, c, scratch, s)
-                       : run_tc_static<64, NS, false>(p, c, scratch, s);
-    case 128: return ak ? run_tc_static<128, NS, true>(p, c, scratch, s)
-                        : run_tc_static<128, NS, false>(p, c, scratch, s);
+    case 16: return ak ? run_tc_static<16, NS, true>(p, c, a, s)
+                       : run_tc_static<16, NS, false>(p, c, a, s);
+    case 32: return ak ? run_tc_static<32, NS, true>(p, c, a, s)
+                       : run_tc_static<32, NS, false>(p, c, a, s);
+    case 64: return ak ? run_tc_static<64, NS, true>(p, c, a, s)
+                       : run_tc_static<64, NS, false>(p, c, a, s);
+    case 128: return ak ? run_tc_static<128, NS, true>(p, c, a, s)
+                        : run_tc_static<128, NS, false>(p, c, a, s);
     default: return HML_STATUS_INVALID_VALUE;
   }
 }
 
 }  // namespace
+
+// Reads and clears the error word of the allocation-free entry point on the
+// current device; 0 when that entry point was never set up there.  Copies to
+// and from the symbol allocate nothing.
+hml_status noalloc_take_error(int *code) {
+  *code = 0;
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) {
+    note_cuda_error(e, "noalloc: cudaGetDevice");
+    return HML_STATUS_CUDA_ERROR;
+  }
+  if (dev < 0 || dev >= kNoAllocMaxDevices) return HML_STATUS_SUCCESS;
+  {
+    std::lock_guard<std::mutex> lk(g_noalloc_mu);
+    if (!g_noalloc_addr[dev].err) return HML_STATUS_SUCCESS;
+  }
+  int h = 0;
+  e = cudaMemcpyFromSymbol(&h, g_noalloc_error, sizeof(int));
+  if (e == cudaSuccess && h != 0) {
+    const int zero = 0;
+    e = cudaMemcpyToSymbol(g_noalloc_error, &zero, sizeof(int));
+  }
+  note_cuda_error(e, "noalloc: error word");
+  *code = h;
+  return cuda_status(e);
+}
 }  // namespace hml
 
 extern "C" hml_status hml_sgemm_ex_config_noalloc(hml_order order, hml_op transA, hml_op transB,
@@ -1805,12 +1844,12 @@ extern "C" hml_status hml_sgemm_ex_config_noalloc(hml_order order, hml_op transA
   if (st != HML_STATUS_SUCCESS) return st;
   if (noalloc_bytes_needed(p, *config) > kNoAllocScratchBytes) {
     note_text_error("noalloc: the BF16 planes of B need more than the 4 MiB static scratch "
-                    "(planes x ceil(N/tile_n)*tile_n x ceil(K/64)*64 x 2 bytes)");
+                    "(planes x ceil(min(M,N)/tile_n)*tile_n x ceil(K/64)*64 x 2 bytes)");
     return HML_STATUS_INVALID_VALUE;
   }
-  void *scratch = nullptr;
-  st = noalloc_scratch(&scratch);
+  NoAllocAddrs addrs;
+  st = noalloc_setup(&addrs);
   if (st != HML_STATUS_SUCCESS) return st;
-  return config->algo == HML_ALGO_BF16X3 ? run_tc_static_ns<2>(p, *config, scratch, s)
-                                         : run_tc_static_ns<3>(p, *config, scratch, s);
+  return config->algo == HML_ALGO_BF16X3 ? run_tc_static_ns<2>(p, *config, addrs, s)
+                                         : run_tc_static_ns<3>(p, *config, addrs, s);
 }

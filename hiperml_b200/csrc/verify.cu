@@ -92,8 +92,13 @@ __global__ void __launch_bounds__(256) dgemm_ref_kernel(GemmProblem p, const flo
         double c = 0.0;
         if (p.beta != 0.0f && C0) c = static_cast<double>(C0[gm * p.scm + gn * p.scn]);
         const double al = static_cast<double>(p.alpha), be = static_cast<double>(p.beta);
-        D[gm + gn * p.M] = al * acc[i][j] + be * c;
-        Dabs[gm + gn * p.M] = fabs(al) * aacc[i][j] + fabs(be) * fabs(c);
+        // two rounded products and a rounded sum, no contraction: the same
+        // operations as the CPU oracle, so both give the same FP64 value
+        // (the k sums above agree too: FP32 x FP32 products are exact in
+        // FP64, and both add them in increasing k from zero)
+        D[gm + gn * p.M] = __dadd_rn(__dmul_rn(al, acc[i][j]), __dmul_rn(be, c));
+        Dabs[gm + gn * p.M] =
+            __dadd_rn(__dmul_rn(fabs(al), aacc[i][j]), __dmul_rn(fabs(be), fabs(c)));
       }
     }
 }

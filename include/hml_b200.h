@@ -124,22 +124,30 @@ hml_status hml_sgemm_select(hml_order order, hml_op transA, hml_op transB,
  * their own pool, latency-critical paths where cudaMalloc's implicit device
  * synchronisation is not acceptable, and hosts that forbid allocation after
  * start-up.  hml_sgemm_ex_config with the same configuration computes the
- * same result but keeps the BF16 planes of B in a workspace it grows with
- * cudaMalloc; this variant keeps them in a fixed 4 MiB array compiled into
- * the library (every GPU that loads the library holds it until exit).
+ * same result, bit for bit, but keeps the BF16 planes of B in a workspace it
+ * grows with cudaMalloc; this variant keeps them in a fixed 4 MiB array
+ * compiled into the library (every GPU that loads the library holds it until
+ * exit).
  *   - config->algo must be HML_ALGO_BF16X3 or HML_ALGO_BF16X6.
- *   - Limit: planes x ceil(N / tile_n) * tile_n x ceil(K / 64) * 64 x 2 bytes
- *     <= 4 MiB (planes = 2 for BF16X3, 3 for BF16X6); larger problems are
- *     rejected with HML_STATUS_INVALID_VALUE and a message in
+ *   - Limit: the library computes a problem whose N exceeds its M as the
+ *     transposed problem (C^T = B^T A^T), so the planes are cut from the
+ *     shorter of M and N.  With S = min(M, N):
+ *     planes x ceil(S / tile_n) * tile_n x ceil(K / 64) * 64 x 2 bytes
+ *     must not exceed 4 MiB (planes = 2 for BF16X3, 3 for BF16X6); larger
+ *     problems are rejected with HML_STATUS_INVALID_VALUE and a message in
  *     hml_last_error().
- *   - The first call on a device looks up the array's device address
- *     (cudaGetSymbolAddress) with that device current; make that first call
- *     before any stream capture.
- *   - Every call shares the one array: calls that overlap on the GPU (on
- *     different streams) race.  Nothing in it needs to start at zero; each
- *     call rewrites the part it uses.
- *   - No device error word is kept: a bounded wait that expires still ends
- *     the kernel, but is not recorded for hml_device_error(). */
+ *   - The first call on a device looks up the addresses of the array and of
+ *     the entry point's error word (cudaGetSymbolAddress) with that device
+ *     current; make that first call before any stream capture.
+ *   - Every call on a device shares the one array, which keeps the last
+ *     call's contents: calls that overlap on the GPU (on different streams,
+ *     or from different host threads) race and corrupt each other's planes,
+ *     so serialise them (one stream, or events between streams).  Nothing
+ *     in the array needs to start at zero; each call rewrites the part it
+ *     uses.
+ *   - A bounded wait that expires ends the kernel and records its code in an
+ *     error word that is also a file-scope device variable;
+ *     hml_device_error() reads and clears it (without allocating). */
 hml_status hml_sgemm_ex_config_noalloc(hml_order order, hml_op transA,
                                        hml_op transB, int M, int N, int K,
                                        float alpha, const float *A, int lda,
@@ -398,6 +406,22 @@ hml_status hml_cfg_v1_sgemm_rule(int K, int N, int *type, int *row_stops);
 hml_status hml_cfg_v1_sgemv_rule(int N, int *type, int *block_stops,
                                  int *row_stops);
 void hml_cfg_v1_clear(void);
+
+/* Writes the loaded v1 rules of `kind` back in the reference's grammar and
+ * rule order (hmlSgemmKernelConfigPrint src/hml_sgemm_kernel.cu:557-568,
+ * hmlSgemvKernelConfigPrint src/hml_sgemv_kernel.cu:634-645): '#' comment
+ * lines, then one rule per line for every entry whose rowStops is positive.
+ * HML_STATUS_CONFIG_ERROR when no v1 file of that kind is loaded. */
+hml_status hml_cfg_v1_save(int kind, const char *path);
+
+/* The configuration hmlSgemm runs a row-major M x N x K problem with when a
+ * loaded v1 SGEMM rule covers it: the rule's tile (16*rowStops rows,
+ * 16*colStops columns; the basic kernel's 96 x 96) mapped onto the nearest
+ * tiled SIMT shape.  The reference's selection this stands in for is
+ * hmlSgemmKernelSelect (src/hml_sgemm_kernel.cu:189-237).
+ * HML_STATUS_CONFIG_ERROR when no rule applies (hmlSgemm then uses the
+ * library's own selection). */
+hml_status hml_sgemm_v1_config(int M, int N, int K, hml_sgemm_config *config);
 
 /* ------------------------------------------------------------ utilities */
 

@@ -12,7 +12,8 @@ from hiperml_b200._lib import LIB_PATH, SgemmConfig, lib
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 INC = os.path.join(ROOT, "include")
-REF = "/root/reference"
+# the reference tree, when the environment names it (the shipped .cfg files)
+REF = os.environ.get("HML_REFERENCE_DIR", "")
 
 INVALID = 1
 

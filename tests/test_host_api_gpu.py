@@ -52,6 +52,13 @@ def test_hmlSgemv_matches_reference_golden(cuda, case, basic):
     out = y.copy()
     (hml.hmlSgemvBasic if basic else hml.hmlSgemv)(out, A, x, M, N, case["alpha"], case["beta"])
     assert_within_fp32_bound(out, D[:, 0], absD[:, 0], N)
+    # the reference's own hmlSgemvCpu output on the same inputs: both FP32
+    # results lie within the FP32 bound of the FP64 value, so within twice it
+    # of each other
+    ref = ARR["sgemv_" + case["name"]].astype(np.float64)
+    assert np.all(np.abs(out.astype(np.float64) - ref) <= 4 * (N + 2) * 2.0 ** -24 * absD[:, 0]
+                  + 1e-37)
+    assert np.all(np.abs(ref - D[:, 0]) <= 2 * (N + 2) * 2.0 ** -24 * absD[:, 0] + 1e-37)
 
 
 def test_errors_raise_instead_of_exit(cuda):

@@ -176,6 +176,26 @@ def test_tc_precision_sweep_full_size(cuda, algo, N):
             assert err[0] <= 1e-5, err
 
 
+@pytest.mark.parametrize("dist", [dg.UNIFORM, dg.LOGUNIFORM], ids=["uniform", "loguniform"])
+def test_tc_square_8192_full_size(cuda, dist):
+    """The precision sweep's square problem, 8192^3, uniform[-1,1] and
+    log-uniform (1e-3..1e3, random sign) inputs: the library's automatic
+    choice and forced BF16X6, checked in FP64 on the GPU."""
+    import torch
+    M = N = K = 8192
+    A = torch.empty(M * K, device="cuda")
+    B = torch.empty(K * N, device="cuda")
+    C = torch.zeros(M * N, device="cuda")
+    hml.fill_random(A, 4, 0, dist)
+    hml.fill_random(B, 4, 1, dist)
+    for cfg in (None, hml.select_algo(0, 0, 0, M, N, K, X6)):
+        C.zero_()
+        hml.sgemm_ex(0, 0, 0, M, N, K, 1.0, A, M, B, K, 0.0, C, M, config=cfg)
+        err = hml.error_fp64(0, 0, 0, M, N, K, 1.0, A, M, B, K, 0.0, None, C, M)
+        assert err[0] <= 2e-6 and err[2] <= 2 * gamma(K + 2), (cfg, err)
+        assert err[0] > 0.0
+
+
 def test_no_device_error_left(cuda):
     assert hml.device_error() == 0
 
