@@ -47,10 +47,14 @@ UNIT = "TFLOPS"
 
 SWEEP_M, SWEEP_K, SWEEP_N = 65536, 4096, (8, 32, 64, 128)
 SIMT_PEAK_NOMINAL = 148 * 128 * 2 * 1.965e-3  # TFLOP/s: 148 SMs x 128 FMA lanes x 2 x 1.965 GHz
-ALGO_NAMES = {1: "simt", 2: "bf16x3", 3: "bf16x6", 4: "tf32x3"}
+ALGO_NAMES = {1: "simt", 2: "bf16x3", 3: "bf16x6", 4: "tf32x3", 5: "fp16x3"}
+ALGO_CODES = {"auto": None, "simt": 1, "bf16x3": 2, "bf16x6": 3, "tf32x3": 4, "fp16x3": 5}
 # BF16-product equivalents of one useful multiply-add per split form (a TF32
 # product runs at half the BF16 rate)
-PRODUCTS = {2: 3, 3: 6, 4: 6}
+PRODUCTS = {2: 3, 3: 6, 4: 6, 5: 3}
+# the least tensor work that gives FP32-level accuracy: a 3-product split
+# (hi*hi + hi*lo + lo*hi); the problem's tensor roofline uses it
+MIN_PRODUCTS = 3
 
 
 def parse():
@@ -61,7 +65,7 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="sweep",
                     choices=["sweep", "c1", "gemv_n", "gemv_t", "square", "batched"])
-    ap.add_argument("--algo", default="auto", choices=["auto", "simt", "bf16x3", "bf16x6", "tf32x3"],
+    ap.add_argument("--algo", default="auto", choices=list(ALGO_CODES),
                     help="force one algorithm family (default: the library's choice)")
     ap.add_argument("--dist", default="uniform", choices=["uniform", "loguniform"],
                     help="sweep/c1/square inputs: uniform[-1,1] or log-uniform 1e-3..1e3")
@@ -503,35 +507,37 @@ def measure_gemms(ctx, problems, algo, dist, steps, warmup, flush_l2, clocks=Non
 
 
 def roofline_of(kind, M, N, K, cfg, ms, key, pk):
-    """Roofline of one kernel launch.  Memory-bound forms (every SIMT and GEMV
-    launch, and the split forms below their tensor ridge): the algorithmic
-    bytes (A and B read once, C written once) over the launch time against
-    the measured HBM copy rate.  A split form above its ridge (the square
-    problem) is bounded by the tensor pipe: useful FLOP/s against the
-    sustained BF16 peak divided by the form's BF16 products per useful
-    multiply-add.  tensor_pipe_frac reports the tensor-pipe work the split
-    forms do (BF16-product units) against the sustained BF16 peak."""
+    """Roofline of one kernel launch, set by the problem, not by the form that
+    runs it.  Its memory floor is the algorithmic bytes (A and B read once, C
+    written once) at the measured HBM copy rate; its compute floor is the
+    useful 2MNK at the sustained BF16 tensor peak divided by MIN_PRODUCTS
+    (the least tensor work that keeps FP32-level accuracy).  The larger floor
+    bounds it: `frac` = that floor over the measured launch time.  Every
+    skinny and GEMV shape is HBM-bound; the square 8192^3 problem is
+    tensor-bound.  tensor_pipe_frac reports the tensor-pipe work the running
+    split form does (its BF16 products per useful multiply-add) against the
+    sustained BF16 peak."""
     alg_bytes = bytes_of(kind, M, N, K)
     alg_flops = flops_of(kind, M, N, K)
     s = ms * 1e-3
     ai = alg_flops / alg_bytes
+    tensor_peak = pk["bf16_tflops_sustained"]
+    useful_cap = tensor_peak / MIN_PRODUCTS  # TFLOP/s of useful work at the tensor peak
+    hbm_time = alg_bytes / (pk["hbm_gbs"] * 1e9)
+    tensor_time = alg_flops / (useful_cap * 1e12)
     roof = {"bound": "hbm", "achieved": alg_bytes / s / 1e9, "peak": pk["hbm_gbs"],
             "unit": "GB/s", "frac": alg_bytes / s / 1e9 / pk["hbm_gbs"],
             "traffic": traffic_table().get(key), "kernel": key,
             "alg_bytes_per_launch": alg_bytes, "alg_flops_per_launch": alg_flops,
             "ms_per_launch": ms, "peak_source": pk["source"], "arith_intensity": ai}
+    if kind == "sgemm" and tensor_time > hbm_time:
+        roof.update({"bound": "tensor", "achieved": alg_flops / s / 1e12, "peak": useful_cap,
+                     "unit": f"TFLOP/s (useful 2MNK; peak = sustained BF16 / {MIN_PRODUCTS})",
+                     "frac": alg_flops / s / 1e12 / useful_cap})
     if cfg is not None and cfg.algo in PRODUCTS:
         products = PRODUCTS[cfg.algo]
-        tensor_peak = pk["bf16_tflops_sustained"]
         roof["tensor_pipe_frac"] = alg_flops * products / s / 1e12 / tensor_peak
         roof["tensor_products_per_mac"] = products
-        useful_cap = tensor_peak / products  # TFLOP/s of useful work at the tensor peak
-        hbm_time = alg_bytes / (pk["hbm_gbs"] * 1e9)
-        tensor_time = alg_flops / (useful_cap * 1e12)
-        if tensor_time > hbm_time:
-            roof.update({"bound": "tensor", "achieved": alg_flops / s / 1e12, "peak": useful_cap,
-                         "unit": "TFLOP/s (useful 2MNK; peak = sustained BF16 / products)",
-                         "frac": alg_flops / s / 1e12 / useful_cap})
     if cfg is not None and cfg.algo == 1:
         roof["simt_fp32_tflops"] = alg_flops / s / 1e12
         roof["simt_fp32_peak_nominal"] = SIMT_PEAK_NOMINAL
@@ -625,7 +631,7 @@ def run_ours(args):
     from hiperml_b200.dist import max_over_ranks
 
     ctx = Ctx()
-    algo = {"auto": None, "simt": 1, "bf16x3": 2, "bf16x6": 3, "tf32x3": 4}[args.algo]
+    algo = ALGO_CODES[args.algo]
     problems = workload_problems(args.workload, args.rows, args.only_n)
     clocks = ClockSampler(ctx.local)
     r = measure_gemms(ctx, problems, algo, args.dist, args.steps, args.warmup,

@@ -7,7 +7,7 @@ fallback for any entry point.
 """
 from ._lib import HmlError, SgemmConfig, lib  # noqa: F401  (loads the .so)
 from .api import (  # noqa: F401
-    ALGO_AUTO, ALGO_BF16X3, ALGO_BF16X6, ALGO_SIMT, ALGO_TF32X3, COL_MAJOR, OP_N, OP_T, ROW_MAJOR,
+    ALGO_AUTO, ALGO_BF16X3, ALGO_BF16X6, ALGO_FP16X3, ALGO_SIMT, ALGO_TF32X3, COL_MAJOR, OP_N, OP_T, ROW_MAJOR,
     check_wait_limit, config_check, configs, device_error, error_fp64, fill_random, hmlSgemm,
     hmlSgemmBasic,
     hmlSgemmKernelConfig, hmlSgemv, hmlSgemvBasic, hmlSgemvKernelConfig, select, select_algo, sgemm,

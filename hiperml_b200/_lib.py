@@ -33,7 +33,7 @@ class SgemmConfig(ctypes.Structure):
         return (self.algo, self.tile_m, self.tile_n, self.split_k, self.stages, self.variant)
 
     def __repr__(self):
-        names = {0: "AUTO", 1: "SIMT", 2: "BF16X3", 3: "BF16X6", 4: "TF32X3"}
+        names = {0: "AUTO", 1: "SIMT", 2: "BF16X3", 3: "BF16X6", 4: "TF32X3", 5: "FP16X3"}
         return (f"SgemmConfig({names.get(self.algo, self.algo)}, {self.tile_m}x{self.tile_n}, "
                 f"split_k={self.split_k}, stages={self.stages}, variant={self.variant})")
 

@@ -22,7 +22,7 @@ from ._lib import GemmDesc, SgemmConfig, SgemvTuneEntry, TuneEntry, check, lib
 
 COL_MAJOR, ROW_MAJOR = 0, 1
 OP_N, OP_T = 0, 1
-ALGO_AUTO, ALGO_SIMT, ALGO_BF16X3, ALGO_BF16X6, ALGO_TF32X3 = 0, 1, 2, 3, 4
+ALGO_AUTO, ALGO_SIMT, ALGO_BF16X3, ALGO_BF16X6, ALGO_TF32X3, ALGO_FP16X3 = 0, 1, 2, 3, 4, 5
 
 
 def _ptr(x) -> Optional[int]:

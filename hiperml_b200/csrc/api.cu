@@ -155,7 +155,8 @@ hml_status run(const GemmProblem &p, const hml_sgemm_config &c, cudaStream_t s) 
     case HML_ALGO_SIMT: return launch_simt(p, c, s);
     case HML_ALGO_BF16X3:
     case HML_ALGO_BF16X6:
-    case HML_ALGO_TF32X3: return launch_tc(p, c, s);
+    case HML_ALGO_TF32X3:
+    case HML_ALGO_FP16X3: return launch_tc(p, c, s);
     default: return HML_STATUS_INVALID_VALUE;
   }
 }
@@ -179,7 +180,8 @@ hml_status check_config(const GemmProblem &p, const hml_sgemm_config &c) {
     case HML_ALGO_SIMT: return check_simt(p, c);
     case HML_ALGO_BF16X3:
     case HML_ALGO_BF16X6:
-    case HML_ALGO_TF32X3: return check_tc(p, c);
+    case HML_ALGO_TF32X3:
+    case HML_ALGO_FP16X3: return check_tc(p, c);
     default: return HML_STATUS_INVALID_VALUE;
   }
 }
@@ -269,7 +271,7 @@ hml_status hml_sgemm_select_algo(hml_order order, hml_op transA, hml_op transB, 
   if (!config) return HML_STATUS_INVALID_VALUE;
   if (algo == HML_ALGO_AUTO) return hml_sgemm_select(order, transA, transB, M, N, K, config);
   if (algo != HML_ALGO_SIMT && algo != HML_ALGO_BF16X3 && algo != HML_ALGO_BF16X6 &&
-      algo != HML_ALGO_TF32X3)
+      algo != HML_ALGO_TF32X3 && algo != HML_ALGO_FP16X3)
     return HML_STATUS_INVALID_VALUE;
   GemmProblem p;
   const bool cm = order == HML_COL_MAJOR;

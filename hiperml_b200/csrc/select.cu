@@ -43,7 +43,8 @@ int choose_split(int64_t tiles, int K, int ctas_per_sm, int min_k) {
 
 hml_sgemm_config heuristic_config(const GemmProblem &p, int algo) {
   hml_sgemm_config c = {};
-  if (algo == HML_ALGO_BF16X3 || algo == HML_ALGO_BF16X6 || algo == HML_ALGO_TF32X3) {
+  if (algo == HML_ALGO_BF16X3 || algo == HML_ALGO_BF16X6 || algo == HML_ALGO_TF32X3 ||
+      algo == HML_ALGO_FP16X3) {
     int best = -1;
     // the narrowest single-CTA (128-row) tile that holds N
     for (int v = 0; v < tc_num_shapes(); ++v) {

@@ -28,8 +28,13 @@
 //     CTA's slot of a per-stream workspace; the CTA of the strip that
 //     arrives last (a per-strip counter, which it resets) sums the slots in
 //     CTA order and writes C.  Results are deterministic.  This epilogue
-//     is inlined: built as a separate, non-inlined function it gave wrong
-//     results on B200 in testing (cause not found), so it is not.
+//     is inlined.  Built as a separate __noinline__ function (the same code,
+//     with the named barrier in its non-aligned form) it gives wrong and
+//     run-to-run different results on B200 in 3 of the 18 stream-kernel
+//     tests, while the inlined build passes all of them bitwise-repeatably;
+//     the cause was not found by reading (barrier participation, the reuse
+//     of `red` and `s_last` across strips and the workspace hand-off check
+//     out), so the function stays inlined.
 //
 // Measured on B200 (M = 65536, K = 4096, column-major A, 4 stages): N = 8
 // 180 us with N-contiguous B (6.0 TB/s of A), and 194 us streaming a
@@ -116,8 +121,13 @@ __device__ __forceinline__ void loads_consumed(const float2 (&acc)[4][NB / 2]) {
     for (int h = 0; h < NB / 2; ++h) asm volatile("" ::"f"(acc[j][h].x), "f"(acc[j][h].y));
 }
 
+// Named barrier 1 over the 8 consumer warps.  The non-aligned form:
+// barrier.sync.aligned (what bar.sync means) requires every thread of a warp
+// to execute the same barrier instruction together, which the epilogue's
+// one-thread branches (tid == 0) do not promise by themselves; the
+// non-aligned form is defined for threads that arrive separately.
 __device__ __forceinline__ void consumers_sync() {
-  asm volatile("bar.sync 1, %0;" ::"n"(kSPhases * 32) : "memory");
+  asm volatile("barrier.sync 1, %0;" ::"n"(kSPhases * 32) : "memory");
 }
 
 // End of this CTA's segment of `strip`, after every warp has stashed its

@@ -6,6 +6,10 @@
 // in FP32:
 //   BF16X3: a0*b0 + a0*b1 + a1*b0                          (2 planes, 3 MMAs)
 //   BF16X6: a0*b0 + a0*b1 + a1*b0 + a0*b2 + a1*b1 + a2*b0  (3 planes, 6 MMAs)
+// and two explicit forms with 11-bit planes: TF32X3 (kind::tf32) and FP16X3
+// (FP16 hi/lo planes of operands scaled by powers of two: per row of each
+// 32-deep block of A, per column of B; each block is accumulated in TMEM on
+// its own and rescaled by the drain).
 // The result is C = alpha * A * B + beta * C in FP32, the reference's
 // hmlSgemm contract (src/hml_sgemm.cu:120-211) on a different machine.
 //
@@ -40,6 +44,7 @@
 // word is set, the CTA skips ahead, waits for its issued MMAs, frees its TMEM
 // and returns.
 #include <cuda_bf16.h>
+#include <cuda_fp16.h>
 
 #include <algorithm>
 #include <cstring>
@@ -86,8 +91,11 @@ constexpr int kNumTcShapes = sizeof(kTcShapes) / sizeof(kTcShapes[0]);
 // and so A stages (NS x 16 columns each, two BF16 per 32-bit column).
 __host__ __device__ constexpr int tc_groups() { return 2; }
 __host__ __device__ constexpr int tc_drain_groups(int bn) { return bn > 64 ? 2 : 1; }
+// BF16-plane equivalents of a form's operand planes: NS = 2 and 3 (BF16X3,
+// BF16X6), 4 (TF32X3: two 32-bit planes), 5 (FP16X3: two FP16 planes).
+__host__ __device__ constexpr int tc_geom(int ns) { return ns == 5 ? 2 : ns; }
 // TMEM columns of one converted A block: NS planes x 32 BF16 (2 per column).
-__host__ __device__ constexpr int tc_stage_cols(int ns) { return ns * kBK / 2; }
+__host__ __device__ constexpr int tc_stage_cols(int ns) { return tc_geom(ns) * kBK / 2; }
 // Operand stages (B slot + A TMEM stage) with ni issuers: a multiple of
 // 2 * ni (blocks per chunk x issuers), so that every stage is only ever used
 // by one issuer and, as 2 * ni is even, by one converter group; at most 8.
@@ -258,6 +266,12 @@ __host__ __device__ constexpr uint32_t idesc_bf16(int bn, int bm = kBM) {
          (static_cast<uint32_t>(bm >> 4) << 24);
 }
 
+// The same for FP16 x FP16 -> F32 (kind::f16; A and B format code 0).
+__host__ __device__ constexpr uint32_t idesc_f16(int bn, int bm = kBM) {
+  return (1u << 4) | (static_cast<uint32_t>(bn >> 3) << 17) |
+         (static_cast<uint32_t>(bm >> 4) << 24);
+}
+
 // The same for TF32 x TF32 -> F32 (kind::tf32; A and B format code 2).
 __host__ __device__ constexpr uint32_t idesc_tf32(int bn, int bm = kBM) {
   return (1u << 4) | (2u << 7) | (2u << 10) | (static_cast<uint32_t>(bn >> 3) << 17) |
@@ -337,6 +351,72 @@ __device__ __forceinline__ void split_plane32(float (&x)[32], uint32_t (&w)[16])
   }
 }
 
+// ------------------------------------------------------- FP16X3 split
+// FP16 keeps 11 significant bits but only 5 exponent bits, so each FP32 row
+// block of A (and each column of B) is first scaled by a power of two 2^S
+// that brings its largest magnitude into [2^14, 2^15): then x*2^S = hi + lo
+// with hi = fp16(x*2^S) and lo = fp16(x*2^S - hi) keeps 22 significant bits
+// of every element within 2^-17 of the largest (the scaling is exact), and
+// hi*hi + hi*lo + lo*hi (3 products) carries FP32-level information.  The
+// biased exponent of the scale is clamped to [1, 253] so that both 2^S and
+// 2^-S are normal floats; an all-zero or denormal block gets 2^126.
+__device__ __forceinline__ int fh_scale_biased(float maxabs) {
+  const int e = __float_as_int(maxabs) >> 23;  // biased exponent (maxabs >= 0)
+  return min(max(268 - e, 1), 253);            // 127 + (14 - (e - 127))
+}
+
+// Two FP32 values rounded to FP16 (nearest even), packed: lo in the low half.
+__device__ __forceinline__ uint32_t f16x2_rn(float lo, float hi) {
+  uint32_t r;
+  asm("cvt.rn.f16x2.f32 %0, %1, %2;" : "=r"(r) : "f"(hi), "f"(lo));
+  return r;
+}
+
+__device__ __forceinline__ float2 f16x2_to_f32(uint32_t h) {
+  return __half22float2(*reinterpret_cast<const __half2 *>(&h));
+}
+
+// The hi and lo FP16 planes of 32 scaled values of one row: word j holds
+// elements 2j and 2j+1; hi = fp16(v), lo = fp16(v - hi) with v = x * s, the
+// residual exact in FP32 (hi is converted back to FP32 to form it).
+__device__ __forceinline__ void split_fh32(const float (&x)[32], float s, uint32_t (&wh)[16],
+                                           uint32_t (&wl)[16]) {
+#pragma unroll
+  for (int j = 0; j < 16; ++j) {
+    const float a = __fmul_rn(x[2 * j], s), b = __fmul_rn(x[2 * j + 1], s);
+    const uint32_t h = f16x2_rn(a, b);
+    const float2 hf = f16x2_to_f32(h);
+    wh[j] = h;
+    wl[j] = f16x2_rn(__fsub_rn(a, hf.x), __fsub_rn(b, hf.y));
+  }
+}
+
+// Largest magnitude of 32 values (a tree of maxima of absolute values).
+__device__ __forceinline__ float maxabs32(const float (&x)[32]) {
+  float m[16];
+#pragma unroll
+  for (int j = 0; j < 16; ++j) m[j] = fmaxf(fabsf(x[2 * j]), fabsf(x[2 * j + 1]));
+#pragma unroll
+  for (int w = 8; w >= 1; w >>= 1)
+#pragma unroll
+    for (int j = 0; j < w; ++j) m[j] = fmaxf(m[j], m[j + w]);
+  return m[0];
+}
+
+// 2^e as a float for e in [-149, 127] (denormal below -126), 0 below.
+__device__ __forceinline__ float exp2_int(int e) {
+  if (e >= -126) return __int_as_float((min(e, 127) + 127) << 23);
+  if (e >= -149) return __int_as_float(1 << (e + 149));
+  return 0.0f;
+}
+
+// x * 2^e for an integer e, exact unless the result leaves the float range.
+__device__ __forceinline__ float scale_pow2(float x, int e) {
+  while (e > 126) { x *= 0x1p126f; e -= 126; }
+  while (e < -126) { x *= 0x1p-126f; e += 126; }
+  return x * __int_as_float((e + 127) << 23);
+}
+
 struct TcArgs {
   GemmProblem p;
   int split;       // CTAs per cluster along K
@@ -344,6 +424,7 @@ struct TcArgs {
   int sa, so;      // A ring and operand-stage depths
   int n_pad;       // rows of one B plane in the workspace
   int *err;
+  const int *bexp;  // FP16X3: per column of B, the scale exponent S_n of its planes
 };
 
 // ------------------------------------------------------------ B planes
@@ -395,6 +476,52 @@ __global__ void split_b_kernel(const float *B, int64_t sbk, int64_t sbn, int K, 
   }
 }
 
+// FP16X3 planes of B: column n is scaled by 2^S_n, which brings its largest
+// magnitude over K into [2^14, 2^15), and split into planes[0][n][k] =
+// fp16(b * 2^S_n) and planes[1][n][k] = fp16(b * 2^S_n - hi); S_n goes to
+// bexp[n].  Padding columns (n >= N) get zero planes and kNoColumn.  One
+// warp per column: the column's maximum, then its conversion, 8 values a
+// lane at a time (16-byte stores).
+constexpr int kNoColumn = -100000;
+
+__global__ void split_b_fh_kernel(const float *B, int64_t sbk, int64_t sbn, int K, int N,
+                                  uint32_t *planes, int *bexp, int k_pad, int n_pad) {
+  allow_dependent_launch();
+  const int wpb = blockDim.x >> 5, lane = threadIdx.x & 31;
+  for (int n = blockIdx.x * wpb + (threadIdx.x >> 5); n < n_pad; n += gridDim.x * wpb) {
+    const float *col = B + static_cast<int64_t>(n) * sbn;
+    float mx = 0.0f;
+    if (n < N)
+      for (int k = lane; k < K; k += 32) mx = fmaxf(mx, fabsf(col[static_cast<int64_t>(k) * sbk]));
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    const int sb = fh_scale_biased(mx);
+    const float sc = __int_as_float(sb << 23);
+    if (lane == 0) bexp[n] = n < N ? sb - 127 : kNoColumn;
+    // planes as 32-bit words: two FP16 per word, k_pad / 2 words per row
+    uint32_t *ph = planes + static_cast<int64_t>(n) * (k_pad / 2);
+    uint32_t *pl = planes + (static_cast<int64_t>(n_pad) + n) * (k_pad / 2);
+    for (int k0 = lane * 8; k0 < k_pad; k0 += 256) {
+      float x[8];
+#pragma unroll
+      for (int j = 0; j < 8; ++j) {
+        const int k = k0 + j;
+        x[j] = (n < N && k < K) ? col[static_cast<int64_t>(k) * sbk] : 0.0f;
+      }
+      uint32_t h[4], l[4];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const float a = x[2 * j] * sc, b = x[2 * j + 1] * sc;
+        h[j] = f16x2_rn(a, b);
+        const float2 hf = f16x2_to_f32(h[j]);  // hi exactly as stored
+        l[j] = f16x2_rn(a - hf.x, b - hf.y);
+      }
+      *reinterpret_cast<uint4 *>(ph + k0 / 2) = make_uint4(h[0], h[1], h[2], h[3]);
+      *reinterpret_cast<uint4 *>(pl + k0 / 2) = make_uint4(l[0], l[1], l[2], l[3]);
+    }
+  }
+}
+
 // ------------------------------------------------------------- kernel
 // Shared-memory plan of one CTA (tiles 1024-byte aligned):
 //   A ring    sa slots of the FP32 A tile (16 KB), filled by TMA, released
@@ -411,11 +538,15 @@ struct TcPlan {
 
 __host__ __device__ constexpr size_t tc_a_bytes() { return static_cast<size_t>(kBM) * kBK * 4; }
 __host__ __device__ constexpr size_t tc_b_bytes(int bn, int ns) {
-  return static_cast<size_t>(ns) * bn * kBK * 2;
+  return static_cast<size_t>(tc_geom(ns)) * bn * kBK * 2;
 }
+// FP16X3: the ring of per-row scale exponents the converters hand to the
+// drain warps, one entry per K block in flight (2 x the operand stages).
+__host__ __device__ constexpr int tc_fh_ring(int so) { return 2 * so; }
 size_t tc_plan_bytes(int bn, int ns, const TcPlan &pl) {
+  const size_t ring = ns == 5 ? static_cast<size_t>(tc_fh_ring(pl.so)) * (8 + kBM * 4) : 0;
   return 1024 + pl.sa * tc_a_bytes() + pl.so * tc_b_bytes(bn, ns) +
-         8 * (2 * pl.sa + 2 * pl.so + 2 * 4 + 1) + 16;
+         8 * (2 * pl.sa + 2 * pl.so + 2 * 4 + 1) + 16 + ring + 16;
 }
 
 // The deepest operand-stage ring that fits TMEM and shared memory next to
@@ -455,8 +586,12 @@ __global__ void __launch_bounds__(tc_warps(BN, NS) * 32, 1)
   // NS = 4 is the TF32 form: 2 planes of 32-bit TF32 (hi, lo), the TMEM and
   // shared-memory footprint of 4 BF16 planes
   constexpr bool TF = NS == 4;
-  static_assert(!(PAIR && TF), "CTA pairs run the BF16 forms only");
-  constexpr int PL = TF ? 2 : NS;                            // planes
+  // NS = 5 is the FP16X3 form: 2 FP16 planes of scaled values (the footprint
+  // of 2 BF16 planes), a power-of-two scale per row and 32-deep block of A
+  // and per column of B, each block accumulated and drained on its own
+  constexpr bool FH = NS == 5;
+  static_assert(!(PAIR && (TF || FH)), "CTA pairs run the BF16 forms only");
+  constexpr int PL = TF ? 2 : tc_geom(NS);                   // planes
   constexpr int PLC = TF ? kBK : kBK / 2;                    // TMEM columns of a plane
   constexpr int KMMA = TF ? 8 : 16;                          // K of one MMA
   constexpr int G = tc_groups();
@@ -471,8 +606,10 @@ __global__ void __launch_bounds__(tc_warps(BN, NS) * 32, 1)
   constexpr int BSLOT = PL * BPL_BYTES;                      // one B slot
   constexpr int SC = tc_stage_cols(NS);                      // TMEM columns of an A stage
   static_assert(SC == PL * PLC, "stage columns");
-  constexpr uint32_t IDESC = TF ? idesc_tf32(BN) : idesc_bf16(BN, PAIR ? 2 * kBM : kBM);
-  constexpr int P = kChunkK / kBK;                           // blocks per TMEM chunk
+  constexpr uint32_t IDESC =
+      TF ? idesc_tf32(BN) : FH ? idesc_f16(BN) : idesc_bf16(BN, PAIR ? 2 * kBM : kBM);
+  // blocks per TMEM chunk (FP16X3: one, the row scales change every block)
+  constexpr int P = FH ? 1 : kChunkK / kBK;
 
   extern __shared__ uint8_t smem_raw[];
   uint8_t *smem = reinterpret_cast<uint8_t *>(
@@ -488,8 +625,16 @@ __global__ void __launch_bounds__(tc_warps(BN, NS) * 32, 1)
   uint64_t *accfull = opempty + SO;   // [NI] accumulator holds a finished chunk
   uint64_t *accempty = accfull + NI;  // [NI] accumulator drained
   uint64_t *mmadone = accempty + NI;  // every issued MMA has completed
-  uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(mmadone + 1);
+  // FP16X3: ring of R entries, one per K block in flight, each the 128 row
+  // scale exponents of a block (sexp) and the barrier the converters arrive
+  // on once they are written (sfull)
+  const int R = FH ? tc_fh_ring(SO) : 0;
+  uint64_t *sfull = mmadone + 1;      // [R]
+  uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(sfull + R);
   int *bad_flag = reinterpret_cast<int *>(tmem_slot + 1);
+  int *tmax_sh = bad_flag + 1;        // FP16X3: the largest column scale exponent of the tile
+  int *sexp = reinterpret_cast<int *>((reinterpret_cast<uintptr_t>(tmax_sh + 1) + 15) &
+                                      ~static_cast<uintptr_t>(15));  // [R][kBM]
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int split = args.split;
@@ -520,6 +665,7 @@ __global__ void __launch_bounds__(tc_warps(BN, NS) * 32, 1)
       mbar_init(&accempty[b], PAIR ? 2 * 4 * D : 4 * D);
     }
     mbar_init(mmadone, NI);  // one commit per MMA issuer
+    for (int r = 0; r < R; ++r) mbar_init(&sfull[r], 4);  // the converter group's warps
     *bad_flag = 0;
     fence_mbar_init();
   }
@@ -696,12 +842,20 @@ __global__ void __launch_bounds__(tc_warps(BN, NS) * 32, 1)
       // __syncwarp alone does not wait for the other lanes' shared-memory
       // loads to return
       uint32_t wv[16];
+      [[maybe_unused]] uint32_t wl[16];
+      [[maybe_unused]] int sexp_m = 0;
       if constexpr (TF) {
         // hi of the first 16 values; the other 16 only need to have arrived
 #pragma unroll
         for (int k = 0; k < 16; ++k) wv[k] = tf32_rna(x[k]);
 #pragma unroll
         for (int k = 16; k < 32; ++k) asm volatile("" ::"f"(x[k]));
+      } else if constexpr (FH) {
+        // the row's scale for this block from its largest magnitude, then
+        // both planes
+        const int sb = fh_scale_biased(maxabs32(x));
+        sexp_m = sb - 127;
+        split_fh32(x, __int_as_float(sb << 23), wv, wl);
       } else {
         split_plane32<NS == 1>(x, wv);
       }
@@ -714,6 +868,14 @@ __global__ void __launch_bounds__(tc_warps(BN, NS) * 32, 1)
         break;
       }
       tc_fence_after();
+      if constexpr (FH) {
+        // the drain of this block reads the row's scale exponent (the entry
+        // is free: the drain of block kb - R finished before the MMAs of
+        // block kb - SO, which released this operand stage)
+        sexp[(kb % R) * kBM + m] = sexp_m;
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&sfull[kb % R]);
+      }
       const uint32_t dst = tA + lanes + static_cast<uint32_t>(o * SC);
       if constexpr (TF) {
         // one TF32 per column: plane hi in columns 0..31 (k), lo in 32..63;
@@ -732,6 +894,9 @@ __global__ void __launch_bounds__(tc_warps(BN, NS) * 32, 1)
 #pragma unroll
         for (int k = 0; k < 16; ++k) wv[k] = tf32_rna(x[16 + k]);
         tmem_st16(dst + 48u, wv);
+      } else if constexpr (FH) {
+        tmem_st16(dst, wv);
+        tmem_st16(dst + 16u, wl);
       } else {
         tmem_st16(dst, wv);
         split_plane32<NS == 2>(x, wv);
@@ -755,19 +920,79 @@ __global__ void __launch_bounds__(tc_warps(BN, NS) * 32, 1)
     // ------------------------------------------ drain (D groups)
     const int d = (warp - kDrainWarp0) >> 2;
     const uint32_t lanes = static_cast<uint32_t>((warp & 3) * 32) << 16;
+    const int mrow = tid & (kBM - 1);
     float sums[DC];  // FP32 running sums of row m, DC columns
 #pragma unroll
     for (int i = 0; i < DC; ++i) sums[i] = 0.0f;
+    [[maybe_unused]] int tmax = kNoColumn;
+    if constexpr (FH) {
+      // the tile's largest column scale exponent: the running sums hold
+      // C(m, n) * 2^(S_n - tmax), never above |C(m, n)| (the column scales
+      // come from the B-splitting kernel launched just before this one)
+      wait_prior_grid();
+      for (int c = lane; c < BN; c += 32)
+        if (n0 + c < p.N) tmax = max(tmax, args.bexp[n0 + c]);
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) tmax = max(tmax, __shfl_xor_sync(0xffffffffu, tmax, o));
+      if (tid == kDrainWarp0 * 32) *tmax_sh = tmax;
+    }
     for (int q = 0; q < nchunks; ++q) {
       const int b = q % NI;
       bool w = mbar_wait(&accfull[b], (q / NI) & 1, args.err, kDevErrMmaBarrier);
+      [[maybe_unused]] float mult = 1.0f, mult2 = 1.0f;
+      [[maybe_unused]] bool twostep = false;
+      if constexpr (FH) {
+        // block q's partial of row m is scaled by 2^(S_m,q + S_n): undo the
+        // row's scale and the tile's largest column scale, 2^e.  Outside
+        // the normal range the factor is applied in two exact steps
+        // (2^(e -+ 126), then 2^(+-126)), so no contribution is lost or
+        // clamped that FP32 itself would represent.
+        if (w) w = mbar_wait(&sfull[q % R], (q / R) & 1, args.err, kDevErrFullBarrier);
+        if (w) {
+          const int e = -sexp[(q % R) * kBM + mrow] - tmax;
+          twostep = e < -126 || e > 127;
+          mult = exp2_int(e < -126 ? e + 126 : e > 127 ? e - 126 : e);
+          mult2 = e < -126 ? 0x1p-126f : 0x1p126f;
+        }
+      }
       if (!__all_sync(0xffffffffu, w)) {  // tcgen05.ld is warp-collective
         *bad_flag = 1;
         break;
       }
       tc_fence_after();
       const uint32_t src = tacc + lanes + static_cast<uint32_t>(b * BN + d * DC);
-      if constexpr (DC >= 16) {
+      if constexpr (FH && DC >= 16) {
+        // up to 32 columns loaded before one wait (16 when the running sums
+        // take 64 registers); packed FP32x2 FMAs
+        constexpr int W = DC >= 64 ? 16 : DC >= 32 ? 32 : DC;
+        const float2 m2 = make_float2(mult, mult), m22 = make_float2(mult2, mult2);
+#pragma unroll
+        for (int c = 0; c < DC; c += W) {
+          uint32_t r0[W];
+#pragma unroll
+          for (int h = 0; h < W; h += 16)
+            tmem_ld16(src + c + h, *reinterpret_cast<uint32_t(*)[16]>(r0 + h));
+          tmem_wait_ld();
+          if (!twostep) {
+#pragma unroll
+            for (int i = 0; i < W; i += 2) {
+              const float2 r = make_float2(__uint_as_float(r0[i]), __uint_as_float(r0[i + 1]));
+              const float2 t = __ffma2_rn(r, m2, make_float2(sums[c + i], sums[c + i + 1]));
+              sums[c + i] = t.x;
+              sums[c + i + 1] = t.y;
+            }
+          } else {
+#pragma unroll
+            for (int i = 0; i < W; i += 2) {
+              const float2 r = make_float2(__uint_as_float(r0[i]), __uint_as_float(r0[i + 1]));
+              const float2 t = __ffma2_rn(__fmul2_rn(r, m2), m22,
+                                          make_float2(sums[c + i], sums[c + i + 1]));
+              sums[c + i] = t.x;
+              sums[c + i + 1] = t.y;
+            }
+          }
+        }
+      } else if constexpr (DC >= 16) {
 #pragma unroll
         for (int c = 0; c < DC; c += 16) {
           uint32_t r0[16];
@@ -781,8 +1006,19 @@ __global__ void __launch_bounds__(tc_warps(BN, NS) * 32, 1)
         uint32_t r0[8];
         tmem_ld8(src, r0);
         tmem_wait_ld();
+        if constexpr (FH) {
+          if (!twostep) {
 #pragma unroll
-        for (int i = 0; i < 8; ++i) sums[i] += __uint_as_float(r0[i]);
+            for (int i = 0; i < 8; ++i) sums[i] = __fmaf_rn(__uint_as_float(r0[i]), mult, sums[i]);
+          } else {
+#pragma unroll
+            for (int i = 0; i < 8; ++i)
+              sums[i] = __fmaf_rn(__fmul_rn(__uint_as_float(r0[i]), mult), mult2, sums[i]);
+          }
+        } else {
+#pragma unroll
+          for (int i = 0; i < 8; ++i) sums[i] += __uint_as_float(r0[i]);
+        }
       }
       tc_fence_before();
       __syncwarp();
@@ -814,13 +1050,20 @@ __global__ void __launch_bounds__(tc_warps(BN, NS) * 32, 1)
         const int gn = n0 + d * DC + i;
         if (gn < p.N) {
           float *cp = p.C + gm * p.scm + static_cast<int64_t>(gn) * p.scn;
-          *cp = axpby(p.alpha, sums[i], p.beta, cp);
+          float v = sums[i];
+          if constexpr (FH) v = scale_pow2(v, tmax - args.bexp[gn]);
+          *cp = axpby(p.alpha, v, p.beta, cp);
         }
       }
     }
   }
   if (warp < kDrainWarp0) __syncthreads();
   if (split > 1) {
+    [[maybe_unused]] int tmax_all = 0;
+    if constexpr (FH) {
+      wait_prior_grid();  // the column scale exponents below
+      tmax_all = *tmax_sh;
+    }
     cluster_sync();
     const float *red = reinterpret_cast<const float *>(smem);
     constexpr int E = kBM * BN;
@@ -841,7 +1084,9 @@ __global__ void __launch_bounds__(tc_warps(BN, NS) * 32, 1)
         const int gn = n0 + nn;
         if (gm < p.M && gn < p.N) {
           float *cp = p.C + gm * p.scm + static_cast<int64_t>(gn) * p.scn;
-          *cp = axpby(p.alpha, sv[qq], p.beta, cp);
+          float v = sv[qq];
+          if constexpr (FH) v = scale_pow2(v, tmax_all - args.bexp[gn]);
+          *cp = axpby(p.alpha, v, p.beta, cp);
         }
       }
     }
@@ -881,10 +1126,11 @@ namespace {
 template <int BN, int NS, bool AK>
 hml_status launch_tc_planes(const GemmProblem &p, const hml_sgemm_config &c,
                             const __nv_bfloat16 *planes, int k_pad, int n_pad, int *err,
-                            cudaStream_t s) {
+                            cudaStream_t s, const int *bexp = nullptr) {
   // a 256-row configuration runs on CTA pairs (clusters of two)
   const bool pair = c.tile_m == 2 * kBM;
-  if (pair && (BN < 32 || c.split_k != 1 || NS == 4)) return HML_STATUS_INVALID_VALUE;
+  if (pair && (BN < 32 || c.split_k != 1 || NS >= 4)) return HML_STATUS_INVALID_VALUE;
+  if (NS == 5 && !bexp) return HML_STATUS_INVALID_VALUE;
   CUtensorMap ta, tb;
   memset(&ta, 0, sizeof ta);
   memset(&tb, 0, sizeof tb);
@@ -900,10 +1146,11 @@ hml_status launch_tc_planes(const GemmProblem &p, const hml_sgemm_config &c,
       ok = tensor_map_2d(&tb, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, planes, k_pad,
                          static_cast<uint64_t>(2) * n_pad, static_cast<uint64_t>(k_pad) * 4, kBK,
                          BN, CU_TENSOR_MAP_SWIZZLE_128B);
-    else
+    else  // 16-bit planes (BF16, or FP16 for NS = 5: TMA only moves the bytes)
       ok = tensor_map_2d(&tb, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, planes, k_pad,
-                         static_cast<uint64_t>(NS) * n_pad, static_cast<uint64_t>(k_pad) * 2, kBK,
-                         pair ? BN / 2 : BN, CU_TENSOR_MAP_SWIZZLE_64B);
+                         static_cast<uint64_t>(tc_geom(NS)) * n_pad,
+                         static_cast<uint64_t>(k_pad) * 2, kBK, pair ? BN / 2 : BN,
+                         CU_TENSOR_MAP_SWIZZLE_64B);
   }
   if (!ok) return HML_STATUS_CUDA_ERROR;
   TcArgs args;
@@ -917,9 +1164,10 @@ hml_status launch_tc_planes(const GemmProblem &p, const hml_sgemm_config &c,
   args.so = plan.so;
   args.n_pad = n_pad;
   args.err = err;
+  args.bexp = bexp;
   const size_t smem = tc_plan_bytes(BN, NS, plan);
   void (*kern)(CUtensorMap, CUtensorMap, TcArgs) = tc_kernel<BN, NS, AK, false>;
-  if constexpr (BN >= 32 && NS != 4) {
+  if constexpr (BN >= 32 && NS < 4) {
     if (pair) kern = tc_kernel<BN, NS, AK, true>;
   }
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -959,19 +1207,46 @@ hml_status split_b(const GemmProblem &p, __nv_bfloat16 *planes, int k_pad, int n
   return HML_STATUS_SUCCESS;
 }
 
+// B -> the two FP16 planes of the FP16X3 form and the column scale
+// exponents (bexp, n_pad ints).
+hml_status split_b_fh(const GemmProblem &p, void *planes, int *bexp, int k_pad, int n_pad,
+                      cudaStream_t s) {
+  const int blocks = std::min(std::max(1, (n_pad + 7) / 8), 4 * sm_count());
+  count_launch();
+  split_b_fh_kernel<<<blocks, 256, 0, s>>>(p.B, p.sbk, p.sbn, p.K, p.N,
+                                           static_cast<uint32_t *>(planes), bexp, k_pad, n_pad);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) {
+    note_cuda_error(e, "split_b_fh");
+    return HML_STATUS_CUDA_ERROR;
+  }
+  return HML_STATUS_SUCCESS;
+}
+
 template <int BN, int NS, bool AK>
 hml_status run_tc(const GemmProblem &p, const hml_sgemm_config &c, cudaStream_t s) {
   const int k_pad = ((p.K + kChunkK - 1) / kChunkK) * kChunkK;
   const int n_pad = ((p.N + BN - 1) / BN) * BN;
-  // B planes in the stream's workspace
+  // B planes in the stream's workspace (FP16X3: then the column exponents)
   const size_t plane_bytes = static_cast<size_t>(n_pad) * k_pad * 2;
+  const size_t planes_total = tc_geom(NS) * plane_bytes;
+  const size_t extra = NS == 5 ? static_cast<size_t>(n_pad) * sizeof(int) : 0;
   void *ws = nullptr;
-  hml_status st = workspace(NS * plane_bytes, s, &ws);
+  hml_status st = workspace(planes_total + extra, s, &ws);
   if (st != HML_STATUS_SUCCESS) return st;
   auto *planes = static_cast<__nv_bfloat16 *>(ws);
-  st = split_b<NS>(p, planes, k_pad, n_pad, s);
-  if (st != HML_STATUS_SUCCESS) return st;
-  return launch_tc_planes<BN, NS, AK>(p, c, planes, k_pad, n_pad, device_error_word(), s);
+  if constexpr (NS == 5) {
+    // planes_total is a multiple of 128 bytes (k_pad a multiple of 64)
+    int *bexp = reinterpret_cast<int *>(static_cast<uint8_t *>(ws) + planes_total);
+    st = split_b_fh(p, ws, bexp, k_pad, n_pad, s);
+    if (st != HML_STATUS_SUCCESS) return st;
+    return launch_tc_planes<BN, NS, AK>(p, c, planes, k_pad, n_pad, device_error_word(), s,
+                                        bexp);
+  } else {
+    st = split_b<NS>(p, planes, k_pad, n_pad, s);
+    if (st != HML_STATUS_SUCCESS) return st;
+    return launch_tc_planes<BN, NS, AK>(p, c, planes, k_pad, n_pad, device_error_word(), s);
+  }
 }
 
 template <int BN, int NS>
@@ -1002,16 +1277,24 @@ void tc_shape(int v, int *bm, int *bn) {
 
 // Planes of a split-precision family, in units of BF16 planes: TF32X3's two
 // 32-bit planes take the room of four (its kernels are instantiated NS = 4).
-int tc_ns(int algo) { return algo == HML_ALGO_BF16X3 ? 2 : algo == HML_ALGO_BF16X6 ? 3 : 4; }
+// (FP16X3 is instantiated NS = 5: two 16-bit planes, the room of two BF16 ones)
+int tc_ns(int algo) {
+  return algo == HML_ALGO_BF16X3   ? 2
+         : algo == HML_ALGO_BF16X6 ? 3
+         : algo == HML_ALGO_FP16X3 ? 5
+                                   : 4;
+}
 
 hml_status check_tc(const GemmProblem &p, const hml_sgemm_config &c) {
-  if (c.algo != HML_ALGO_BF16X3 && c.algo != HML_ALGO_BF16X6 && c.algo != HML_ALGO_TF32X3)
+  if (c.algo != HML_ALGO_BF16X3 && c.algo != HML_ALGO_BF16X6 && c.algo != HML_ALGO_TF32X3 &&
+      c.algo != HML_ALGO_FP16X3)
     return HML_STATUS_INVALID_VALUE;
   if (c.variant < 0 || c.variant >= kNumTcShapes) return HML_STATUS_INVALID_VALUE;
   if (c.tile_m != kTcShapes[c.variant].bm || c.tile_n != kTcShapes[c.variant].bn)
     return HML_STATUS_INVALID_VALUE;
   // a CTA pair is one cluster: no cluster split-K on top of it
-  if (c.tile_m == 2 * kBM && (c.split_k != 1 || c.algo == HML_ALGO_TF32X3))
+  if (c.tile_m == 2 * kBM &&
+      (c.split_k != 1 || c.algo == HML_ALGO_TF32X3 || c.algo == HML_ALGO_FP16X3))
     return HML_STATUS_INVALID_VALUE;
   if (c.split_k < 1 || c.split_k > 16 || (c.split_k & (c.split_k - 1)) != 0)
     return HML_STATUS_INVALID_VALUE;
@@ -1035,6 +1318,7 @@ hml_status launch_tc(const GemmProblem &p, const hml_sgemm_config &c, cudaStream
   switch (c.algo) {
     case HML_ALGO_BF16X3: return run_tc_ns<2>(p, c, s);
     case HML_ALGO_BF16X6: return run_tc_ns<3>(p, c, s);
+    case HML_ALGO_FP16X3: return run_tc_ns<5>(p, c, s);
     default: return run_tc_ns<4>(p, c, s);
   }
 }

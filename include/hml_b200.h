@@ -52,9 +52,18 @@ typedef enum hml_algo {
   HML_ALGO_SIMT = 1,   /* plain FP32 FMA on CUDA cores                     */
   HML_ALGO_BF16X3 = 2, /* tcgen05: hi/lo BF16 split, 3 products (hh,hl,lh) */
   HML_ALGO_BF16X6 = 3, /* tcgen05: hi/mid/lo split, 6 products            */
-  HML_ALGO_TF32X3 = 4  /* tcgen05 kind::tf32: hi/lo TF32 split, 3 products
+  HML_ALGO_TF32X3 = 4, /* tcgen05 kind::tf32: hi/lo TF32 split, 3 products
                           (FP32-level accuracy like BF16X6; explicit
                           configurations only, 128-row tiles)           */
+  HML_ALGO_FP16X3 = 5  /* tcgen05 kind::f16 with FP16 operands: each row of
+                          a 32-deep block of A and each column of B scaled
+                          by a power of two into FP16's range, hi/lo FP16
+                          split (22 significant bits), 3 products;
+                          FP32-level accuracy; 128-row tiles.  Range: the
+                          running sums of a tile hold C scaled by a power
+                          of two <= 1, so a result overflows only where
+                          |alpha| sum_k |A(m,k)| |B(k,n)| itself exceeds
+                          the FP32 range */
 } hml_algo;
 
 /* Accuracy policy of hml_sgemm_ex's automatic choice. */

@@ -1,11 +1,12 @@
-"""Split-precision tcgen05 SGEMM (BF16X3, BF16X6, TF32X3) against the FP64
-oracle and the reference fixtures (GPU).
+"""Split-precision tcgen05 SGEMM (BF16X3, BF16X6, TF32X3, FP16X3) against the
+FP64 oracle and the reference fixtures (GPU).
 
 Tolerances (normwise = max|dC| / max|C64|, componentwise = max |dC| /
 (|alpha||A||B| + |beta||C|)):
-  BF16X6, TF32X3  normwise <= 2e-6 and componentwise <= 2 gamma_{K+2} (the
-          FP32 bound; TF32X3's hi + lo keep 22 significant bits of each
-          operand, the one product it drops, lo x lo, is below 2**-22)
+  BF16X6, TF32X3, FP16X3  normwise <= 2e-6 and componentwise <= 2 gamma_{K+2}
+          (the FP32 bound; TF32X3's and FP16X3's hi + lo keep 22 significant
+          bits of each operand, the one product they drop, lo x lo, is below
+          2**-22)
   BF16X3  normwise <= 1e-5 and componentwise <= 2**-16 + 2 gamma_{K+2}
           (the two-term split keeps ~16 significant bits of each operand)
 """
@@ -23,8 +24,8 @@ from tests.test_sgemm_gpu import fetch, store
 pytestmark = pytest.mark.gpu
 META, ARR = load()
 
-X3, X6, TF = hml.ALGO_BF16X3, hml.ALGO_BF16X6, hml.ALGO_TF32X3
-FP32_LEVEL = (X6, TF)
+X3, X6, TF, FH = hml.ALGO_BF16X3, hml.ALGO_BF16X6, hml.ALGO_TF32X3, hml.ALGO_FP16X3
+FP32_LEVEL = (X6, TF, FH)
 VAR = {16: 0, 32: 1, 64: 2, 128: 3}
 PAIR_VAR = {32: 4, 64: 5, 128: 6}  # 256-row tiles on a CTA pair
 
@@ -58,7 +59,7 @@ def run_tc(M, N, K, algo, bn, split=1, stages=4, order=0, ta=0, tb=0, alpha=1.0,
     return got, D, absD
 
 
-@pytest.mark.parametrize("algo", [X3, X6, TF])
+@pytest.mark.parametrize("algo", [X3, X6, TF, FH])
 @pytest.mark.parametrize("bn", [16, 32, 64, 128])
 @pytest.mark.parametrize("layout", [(0, 0, 0), (0, 1, 0), (0, 0, 1), (1, 0, 0), (1, 1, 1)])
 def test_tc_tiles_and_layouts(cuda, algo, bn, layout):
@@ -68,7 +69,7 @@ def test_tc_tiles_and_layouts(cuda, algo, bn, layout):
         check_tol(algo, got, D, absD, K, what=f"{algo} {bn} {layout} {(M, N, K)}")
 
 
-@pytest.mark.parametrize("algo", [X3, X6, TF])
+@pytest.mark.parametrize("algo", [X3, X6, TF, FH])
 @pytest.mark.parametrize("split", [2, 4, 8, 16])
 def test_tc_cluster_split_k(cuda, algo, split):
     for K in (64, 1000, 4096):
@@ -78,7 +79,7 @@ def test_tc_cluster_split_k(cuda, algo, split):
 
 @pytest.mark.parametrize("stages", [2, 4, 6, 8])
 def test_tc_ring_depths(cuda, stages):
-    for algo, bn in ((X3, 128), (X6, 64), (TF, 32), (TF, 128)):
+    for algo, bn in ((X3, 128), (X6, 64), (TF, 32), (TF, 128), (FH, 16), (FH, 64), (FH, 128)):
         cfg = SgemmConfig(algo, 128, bn, 1, stages, VAR[bn])
         if hml.config_check(0, 0, 0, 500, bn, 800, 500, 800, 500, cfg) != 0:
             continue
@@ -105,7 +106,7 @@ def test_tc_beta_zero_does_not_read_c(cuda):
     assert torch.isfinite(C).all()
 
 
-@pytest.mark.parametrize("algo", [X3, X6, TF])
+@pytest.mark.parametrize("algo", [X3, X6, TF, FH])
 @pytest.mark.parametrize("case", [c for c in META["sgemm"] if (c["K"] * 4) % 16 == 0],
                          ids=lambda c: c["name"])
 def test_tc_matches_reference_golden(cuda, algo, case):
@@ -133,7 +134,7 @@ def test_tc_matches_reference_golden(cuda, algo, case):
     assert np.all(np.abs(ref - D) <= 2 * gamma(K + 2) * absD + 1e-37)
 
 
-@pytest.mark.parametrize("algo", [X3, X6, TF])
+@pytest.mark.parametrize("algo", [X3, X6, TF, FH])
 def test_tc_c1_full_size_against_reference_golden(cuda, algo):
     import torch
     M, N, K = 4096, 16, 4096
@@ -154,7 +155,7 @@ def test_tc_c1_full_size_against_reference_golden(cuda, algo):
     assert np.max(np.abs(got - ref)) / np.max(np.abs(ref)) <= tol + 4 * 2.0 ** -24 * 64
 
 
-@pytest.mark.parametrize("algo", [X3, X6, TF])
+@pytest.mark.parametrize("algo", [X3, X6, TF, FH])
 @pytest.mark.parametrize("N", [8, 32, 64, 128])
 def test_tc_precision_sweep_full_size(cuda, algo, N):
     """M = 65536, K = 4096, uniform and log-uniform (1e-3..1e3) inputs,
@@ -188,7 +189,7 @@ def test_tc_square_8192_full_size(cuda, dist):
     C = torch.zeros(M * N, device="cuda")
     hml.fill_random(A, 4, 0, dist)
     hml.fill_random(B, 4, 1, dist)
-    for cfg in (None, hml.select_algo(0, 0, 0, M, N, K, X6)):
+    for cfg in (None, hml.select_algo(0, 0, 0, M, N, K, X6), hml.select_algo(0, 0, 0, M, N, K, FH)):
         C.zero_()
         hml.sgemm_ex(0, 0, 0, M, N, K, 1.0, A, M, B, K, 0.0, C, M, config=cfg)
         err = hml.error_fp64(0, 0, 0, M, N, K, 1.0, A, M, B, K, 0.0, None, C, M)
