@@ -624,6 +624,119 @@ def predictor_entry(ctx, live_shapes=4, live_reps=3):
             "seconds": time.perf_counter() - t0}
 
 
+def reference_gpu_entry(ctx, reps=3):
+    """The reference's own GPU kernels (its kernel repositories and selectors
+    compiled from its sources into oracle/_ref, K40 rules loaded) against
+    this library on the same row-major problems, kernel time only (CUDA
+    events, operands on the device; L2 flushed before each launch of the
+    4096 x 16 x 4096 problem, whose A fits in it).  The reference's
+    host-pointer API refuses problems with M*K or N*K >= 2^27 (its texture
+    limit, src/hml_sgemm.cu:146-149, src/hml_sgemv.cu:150); its kernels run
+    them here through the texture stand-in, and such shapes are marked."""
+    import tempfile
+
+    import numpy as np
+    import torch
+
+    import hiperml_b200 as hml
+    import oracle
+    from hiperml_b200 import datagen as dg
+    if not oracle.ref_gpu_available():
+        return {"workload": "reference_gpu",
+                "unavailable": "oracle/_ref GPU libraries not built (make -C oracle refgpu)"}
+    rules = dict(np.load(os.path.join(ROOT, "tests", "golden", "cfg_rules.npz")))
+    with tempfile.TemporaryDirectory() as d:
+        for kind in ("sgemm", "sgemv"):
+            rows = rules[f"hml_{kind}_k40"]
+            path = os.path.join(d, f"{kind}.cfg")
+            with open(path, "w") as f:
+                f.write(f"#{kind.upper()} smart kernel config file v1.0\n")
+                for r in rows:
+                    f.write((f"{r[0]} {r[1]} : {r[2]} {r[3]}\n" if kind == "sgemm"
+                             else f"{r[0]} : {r[1]} {r[2]} {r[3]}\n"))
+            oracle.ref_gpu_load_rules(kind, path)
+    dev, stream = ctx.dev, ctx.stream
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)
+    out = []
+
+    def ours_ms(fn, n, flush_l2):
+        evs = []
+        for _ in range(n + 1):
+            if flush_l2:
+                flush.fill_(1.0)
+            a = torch.cuda.Event(enable_timing=True)
+            b = torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            fn()
+            b.record(stream)
+            evs.append((a, b))
+        torch.cuda.synchronize()
+        return statistics.median(a.elapsed_time(b) for a, b in evs[1:])
+
+    def ref_ms(fn, n, flush_l2):
+        times = []
+        for _ in range(n + 1):
+            if flush_l2:
+                flush.fill_(1.0)
+                torch.cuda.synchronize()
+            times.append(fn())
+        return statistics.median(times[1:])
+
+    for (M, N, K) in [(4096, 16, 4096)] + [(SWEEP_M, n, SWEEP_K) for n in SWEEP_N]:
+        A = torch.empty(M * K, device=dev)
+        B = torch.empty(K * N, device=dev)
+        hml.fill_random(A, 0, 0, dg.UNIFORM)
+        hml.fill_random(B, 0, 1, dg.UNIFORM)
+        Cr = torch.zeros(M * N, device=dev)
+        Co = torch.zeros(M * N, device=dev)
+        fl = M * K * 4 < 126e6
+        t_ref = ref_ms(lambda: oracle.ref_gpu_sgemm(Cr.data_ptr(), A.data_ptr(), B.data_ptr(), M, N,
+                                                    K, 1.0, 0.0, 1), reps, fl)
+        t_ours = ours_ms(lambda: hml.sgemm_ex(hml.ROW_MAJOR, 0, 0, M, N, K, 1.0, A, K, B, N, 0.0,
+                                              Co, N, stream=stream), reps, fl)
+        torch.cuda.synchronize()
+        diff = float((Cr - Co).abs().max() / Co.abs().max())
+        err_ref = hml.error_fp64(hml.ROW_MAJOR, 0, 0, M, N, K, 1.0, A, K, B, N, 0.0, None, Cr, N)
+        err_ours = hml.error_fp64(hml.ROW_MAJOR, 0, 0, M, N, K, 1.0, A, K, B, N, 0.0, None, Co, N)
+        is_const, grid, block = oracle.ref_gpu_select("sgemm", M, N, K)
+        out.append({"kind": "sgemm", "M": M, "N": N, "K": K, "layout": "row-major NN",
+                    "reference_ms": t_ref, "ours_ms": t_ours, "speedup": t_ref / t_ours,
+                    "reference_tflops": flops_of("sgemm", M, N, K) / (t_ref * 1e-3) / 1e12,
+                    "reference_kernel": {"const_k": is_const, "grid": grid, "block": block},
+                    "beyond_reference_texture_limit": M * K >= 1 << 27,
+                    "max_rel_diff": diff, "reference_max_rel_err_fp64": err_ref[0],
+                    "ours_max_rel_err_fp64": err_ours[0], "l2_flushed": fl})
+        del A, B, Cr, Co
+    for (M, N, form) in ((32768, 4096, "y = A x"), (4096, 32768, "y = A^T x")):
+        # row-major M x N: the two forms of the 32768 x 4096 column-major GEMV
+        A = torch.empty(M * N, device=dev)
+        x = torch.empty(N, device=dev)
+        hml.fill_random(A, 1, 0, dg.NORMAL)
+        hml.fill_random(x, 1, 1, dg.NORMAL)
+        yr = torch.zeros(M, device=dev)
+        yo = torch.zeros(M, device=dev)
+        t_ref = ref_ms(lambda: oracle.ref_gpu_sgemv(yr.data_ptr(), A.data_ptr(), x.data_ptr(), M, N,
+                                                    1.0, 0.0, 1), reps, False)
+        t_ours = ours_ms(lambda: hml.sgemv_ex(hml.ROW_MAJOR, hml.OP_N, M, N, 1.0, A, N, x, 0.0, yo,
+                                              stream=stream), reps, False)
+        torch.cuda.synchronize()
+        diff = float((yr - yo).abs().max() / yo.abs().max())
+        # y = A x as an M x 1 x N GEMM, row-major
+        err_ref = hml.error_fp64(hml.ROW_MAJOR, 0, 0, M, 1, N, 1.0, A, N, x, 1, 0.0, None, yr, 1)
+        err_ours = hml.error_fp64(hml.ROW_MAJOR, 0, 0, M, 1, N, 1.0, A, N, x, 1, 0.0, None, yo, 1)
+        out.append({"kind": "sgemv", "M": M, "N": N, "form": form, "layout": "row-major",
+                    "reference_max_rel_err_fp64": err_ref[0], "ours_max_rel_err_fp64": err_ours[0],
+                    "reference_kernel": "basic (N > 1024): its unsynchronised warp reduction "
+                                        "gives wrong sums on B200",
+                    "reference_ms": t_ref, "ours_ms": t_ours, "speedup": t_ref / t_ours,
+                    "reference_gbs": bytes_of("gemv_n", M, 1, N) / (t_ref * 1e-3) / 1e9,
+                    "beyond_reference_texture_limit": M * N >= 1 << 27, "max_rel_diff": diff})
+        del A, x, yr, yo
+    return {"workload": "reference_gpu", "rules": "shipped K40 .cfg (config/hml_sgemm_k40.cfg, "
+                                                   "config/hml_sgemv_k40.cfg)",
+            "shapes": out}
+
+
 def run_ours(args):
     import torch
 
@@ -707,6 +820,7 @@ def run_ours(args):
         torch.cuda.empty_cache()
         if ctx.rank == 0:
             workloads.append(predictor_entry(ctx))
+            workloads.append(reference_gpu_entry(ctx))
 
     if ctx.rank == 0:
         line = {

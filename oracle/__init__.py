@@ -14,6 +14,10 @@ Two native libraries back it (built by ``oracle/Makefile``):
 * ``_ref/libhml_ref_cpu.so`` -- the reference's own ``hmlSgemmCpu`` /
   ``hmlSgemvCpu`` / ``hmlComputeCsum`` / ``hmlComputeYsum`` compiled from its
   unmodified sources.  It pins the restatement bit for bit.
+* ``_ref/libhml_ref_gpu_{sgemm,sgemv}.so`` -- the reference's own GPU kernel
+  repositories and selectors, compiled from its unmodified sources with the
+  texture stand-in of ``ref_gpu_compat.h`` (``make -C oracle refgpu``): the
+  GPU baseline and a second parity target.
 """
 from __future__ import annotations
 
@@ -90,6 +94,78 @@ def ref():
         R.sgemm_cpu, R.sgemv_cpu, R.csum, R.ysum = f, g, cs, ys
         _ref = R
     return _ref
+
+
+_ref_gpu = {}
+
+
+def ref_gpu_available() -> bool:
+    return all(os.path.exists(os.path.join(_HERE, "_ref", f"libhml_ref_gpu_{k}.so"))
+               for k in ("sgemm", "sgemv"))
+
+
+def ref_gpu(kind):
+    """The reference's own GPU kernels and selectors (kind 'sgemm' or
+    'sgemv'), built from its sources by `make -C oracle refgpu`; entry points
+    of oracle/ref_gpu_harness.cu on device pointers (ints)."""
+    if kind not in _ref_gpu:
+        L = _load(os.path.join(_HERE, "_ref", f"libhml_ref_gpu_{kind}.so"))
+        vp, i, f = ctypes.c_void_p, ctypes.c_int, ctypes.c_float
+        ip = ctypes.POINTER(ctypes.c_int)
+        if kind == "sgemm":
+            L.ref_gpu_sgemm_config.argtypes = [ctypes.c_char_p]
+            L.ref_gpu_sgemm_select.argtypes = [i, i, i, ip, ip, ip]
+            L.ref_gpu_sgemm.argtypes = [vp, vp, vp, i, i, i, f, f, i, ctypes.POINTER(f)]
+        else:
+            L.ref_gpu_sgemv_config.argtypes = [ctypes.c_char_p]
+            L.ref_gpu_sgemv_select.argtypes = [i, i, ip, ip, ip]
+            L.ref_gpu_sgemv.argtypes = [vp, vp, vp, i, i, f, f, i, ctypes.POINTER(f)]
+        _ref_gpu[kind] = L
+    return _ref_gpu[kind]
+
+
+def ref_gpu_sgemm(C, A, B, M, N, K, alpha, beta, reps=1):
+    """hmlSgemm's kernel on device pointers (row-major); returns ms per launch."""
+    ms = ctypes.c_float()
+    with _QuietStderr():
+        rc = ref_gpu("sgemm").ref_gpu_sgemm(C, A, B, M, N, K, alpha, beta, reps, ctypes.byref(ms))
+    if rc != 0:
+        raise RuntimeError(f"reference SGEMM kernel: CUDA status {rc}")
+    return ms.value
+
+
+def ref_gpu_sgemv(y, A, x, M, N, alpha, beta, reps=1):
+    """hmlSgemv's kernel on device pointers (A row-major M x N)."""
+    ms = ctypes.c_float()
+    with _QuietStderr():
+        rc = ref_gpu("sgemv").ref_gpu_sgemv(y, A, x, M, N, alpha, beta, reps, ctypes.byref(ms))
+    if rc != 0:
+        raise RuntimeError(f"reference SGEMV kernel: CUDA status {rc}")
+    return ms.value
+
+
+def ref_gpu_select(kind, *shape):
+    """(is_const, grid, block) of the kernel the loaded rules pick."""
+    c = ctypes.c_int()
+    g = (ctypes.c_int * 3)()
+    b = (ctypes.c_int * 3)()
+    fn = ref_gpu(kind).ref_gpu_sgemm_select if kind == "sgemm" else \
+        ref_gpu(kind).ref_gpu_sgemv_select
+    with _QuietStderr():
+        rc = fn(*shape, ctypes.byref(c), g, b)
+    if rc != 0:
+        raise RuntimeError("reference selector: no rules loaded")
+    return bool(c.value), tuple(g), tuple(b)
+
+
+def ref_gpu_load_rules(kind, path):
+    """hmlSgemmKernelConfigReadFile / hmlSgemvKernelConfigReadFile."""
+    fn = ref_gpu(kind).ref_gpu_sgemm_config if kind == "sgemm" else \
+        ref_gpu(kind).ref_gpu_sgemv_config
+    with _QuietStderr():
+        rc = fn(str(path).encode())
+    if rc != 0:
+        raise RuntimeError(f"reference {kind} rules not loaded from {path}")
 
 
 def _fp(a):
