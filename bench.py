@@ -737,6 +737,55 @@ def reference_gpu_entry(ctx, reps=3):
             "shapes": out}
 
 
+def kmeans_entry(ctx, reps=5):
+    """The k-means assignment step (hml_kmeans_assign: one skinny SGEMM and
+    an exact argmin) against the reference's own assignment kernel
+    hmlKmeansAssignCtrdSmem (oracle/_ref), 1M points, N(0,1), kernel time
+    with CUDA events, and whether the two index arrays are equal."""
+    import torch
+
+    import hiperml_b200 as hml
+    import oracle
+    from hiperml_b200 import datagen as dg
+    out = []
+    for (n, d, k) in ((1 << 20, 32, 64), (1 << 20, 32, 256), (1 << 20, 64, 128)):
+        P = torch.empty(n * d, device=ctx.dev)
+        C = torch.empty(k * d, device=ctx.dev)
+        hml.fill_random(P, 11, 0, dg.NORMAL)
+        hml.fill_random(C, 11, 1, dg.NORMAL)
+        P, C = P.view(n, d), C.view(k, d)
+        got = torch.empty(n, dtype=torch.int32, device=ctx.dev)
+        evs = []
+        for i in range(reps + 2):
+            a = torch.cuda.Event(enable_timing=True)
+            b = torch.cuda.Event(enable_timing=True)
+            a.record(ctx.stream)
+            hml.kmeans_assign(P, C, out=got, stream=ctx.stream)
+            b.record(ctx.stream)
+            evs.append((a, b))
+        torch.cuda.synchronize()
+        t_ours = statistics.median(a.elapsed_time(b) for a, b in evs[2:])
+        entry = {"points": n, "dims": d, "clusters": k, "ours_ms": t_ours,
+                 "ours_points_per_s": n / (t_ours * 1e-3),
+                 "gemm_tflops": 2.0 * n * d * k / (t_ours * 1e-3) / 1e12}
+        _, exact = hml.kmeans_assign(P, C, count_exact=True)
+        entry["points_resolved_exactly"] = exact
+        if oracle.ref_gpu_kmeans_available():
+            ref = torch.zeros(n, dtype=torch.int32, device=ctx.dev)
+            oracle.ref_gpu_kmeans_assign(ref.data_ptr(), P.data_ptr(), n, C.data_ptr(), k, d, 1)
+            t_ref = oracle.ref_gpu_kmeans_assign(ref.data_ptr(), P.data_ptr(), n, C.data_ptr(), k,
+                                                 d, reps)
+            torch.cuda.synchronize()
+            entry.update({"reference_ms": t_ref, "speedup": t_ref / t_ours,
+                          "indices_equal": bool(torch.equal(got, ref))})
+        out.append(entry)
+        del P, C, got
+    return {"workload": "kmeans_assign",
+            "config": {"data": "points and centroids N(0,1), seed 11", "layout": "row-major",
+                       "reference": "hmlKmeansAssignCtrdSmem built from the reference's header"},
+            "shapes": out}
+
+
 def run_ours(args):
     import torch
 
@@ -821,6 +870,7 @@ def run_ours(args):
         if ctx.rank == 0:
             workloads.append(predictor_entry(ctx))
             workloads.append(reference_gpu_entry(ctx))
+            workloads.append(kmeans_entry(ctx))
 
     if ctx.rank == 0:
         line = {

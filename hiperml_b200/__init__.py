@@ -12,6 +12,7 @@ from .api import (  # noqa: F401
     hmlSgemmBasic,
     hmlSgemmKernelConfig, hmlSgemv, hmlSgemvBasic, hmlSgemvKernelConfig, select, select_algo, sgemm,
     sgemm_ex, sgemv_ex, autotune, autotune_sgemv, sgemv_select, tune_save, tune_load, tune_clear,
-    set_math_mode, MATH_FP32, MATH_FAST, BatchPlan, gemm_descs, sgemm_batched, batch_problem_config)
+    set_math_mode, MATH_FP32, MATH_FAST, BatchPlan, gemm_descs, sgemm_batched, batch_problem_config,
+    kmeans_assign)
 
 __version__ = lib.hml_version().decode()

@@ -218,6 +218,31 @@ def error_fp64(order, transA, transB, M, N, K, alpha, A, lda, B, ldb, beta, C0, 
     return tuple(err)
 
 
+def kmeans_assign(points, centroids, out=None, stream=None, count_exact=False):
+    """Nearest-centroid index of every point (``hml_kmeans_assign``): points
+    (n x d) and centroids (k x d) are row-major float32 CUDA tensors; returns
+    an int32 tensor of n indices (the reference kernel's, bit for bit), and
+    with ``count_exact`` also the number of points whose candidates were
+    resolved with the reference's own arithmetic."""
+    import torch
+    n, d = points.shape
+    k, d2 = centroids.shape
+    if d != d2:
+        raise ValueError("points and centroids differ in dimension")
+    if not (points.is_contiguous() and centroids.is_contiguous()):
+        raise ValueError("points and centroids must be row-major contiguous")
+    if out is None:
+        out = torch.empty(n, dtype=torch.int32, device=points.device)
+    if count_exact:
+        cnt = torch.zeros(1, dtype=torch.int32, device=points.device)
+        check(lib.hml_kmeans_assign_stats(_ptr(points), n, d, _ptr(centroids), k, _ptr(out),
+                                          _ptr(cnt), _stream(stream)), "hml_kmeans_assign")
+        return out, int(cnt.item())
+    check(lib.hml_kmeans_assign(_ptr(points), n, d, _ptr(centroids), k, _ptr(out),
+                                _stream(stream)), "hml_kmeans_assign")
+    return out
+
+
 def device_error() -> int:
     code = ctypes.c_int()
     check(lib.hml_device_error(ctypes.byref(code)), "hml_device_error")

@@ -161,6 +161,8 @@ hml_status run(const GemmProblem &p, const hml_sgemm_config &c, cudaStream_t s) 
   }
 }
 
+}  // namespace
+
 // N == 1 is a GEMV: route it to the GEMV kernels.
 bool as_gemv(const GemmProblem &p, GemvProblem *g) {
   if (p.N != 1) return false;
@@ -170,8 +172,6 @@ bool as_gemv(const GemmProblem &p, GemvProblem *g) {
   g->y = p.C; g->incy = p.scm;
   return true;
 }
-
-}  // namespace
 
 const std::vector<hml_sgemm_config> &config_space() { return space(); }
 

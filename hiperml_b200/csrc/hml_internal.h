@@ -59,6 +59,8 @@ hml_status gemv_from_blas(hml_order order, hml_op trans, int M, int N, float alp
 constexpr int kGemvTuned = -1;
 constexpr int kGemvMaxColSplit = 256;
 hml_status launch_gemv(const GemvProblem &p, int variant, cudaStream_t s);
+// A GEMM with N == 1 as the GEMV it is (false when N != 1; api.cu).
+bool as_gemv(const GemmProblem &p, GemvProblem *g);
 // Which GEMV kernel serves p: the row kernel (rows of A contiguous) or the
 // column kernel.
 inline bool gemv_rows_layout(const GemvProblem &p) {
@@ -106,6 +108,9 @@ int *device_error_word_if_any();  // nullptr when not allocated yet (allocates n
 // Reads and clears the allocation-free entry point's error word (sgemm_tc.cu).
 hml_status noalloc_take_error(int *code);
 hml_status workspace(size_t bytes, cudaStream_t s, void **ptr);
+// The same for a second, independent buffer per (device, stream): slot 1 holds
+// data that outlives a library call made in between (which uses slot 0).
+hml_status workspace_slot(int slot, size_t bytes, cudaStream_t s, void **ptr);
 // n zero-initialised counters private to (device, stream).  Kernels that use
 // them leave every counter at zero again when they finish.
 hml_status tile_counters(size_t n, cudaStream_t s, unsigned **ptr);

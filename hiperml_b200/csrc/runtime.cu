@@ -21,6 +21,7 @@ struct Ws {
   size_t bytes = 0;
 };
 std::map<std::pair<int, cudaStream_t>, Ws> g_ws;
+std::map<std::pair<int, cudaStream_t>, Ws> g_ws1;  // a second buffer per stream (slot 1)
 std::map<std::pair<int, cudaStream_t>, Ws> g_counters;
 std::map<int, int> g_sms;
 thread_local std::string t_last_error;
@@ -86,10 +87,12 @@ int *device_error_word() {
   return w;
 }
 
-hml_status workspace(size_t bytes, cudaStream_t s, void **ptr) {
+hml_status workspace(size_t bytes, cudaStream_t s, void **ptr) { return workspace_slot(0, bytes, s, ptr); }
+
+hml_status workspace_slot(int slot, size_t bytes, cudaStream_t s, void **ptr) {
   const int d = current_device();
   std::lock_guard<std::mutex> lk(g_mu);
-  Ws &w = g_ws[std::make_pair(d, s)];
+  Ws &w = (slot == 0 ? g_ws : g_ws1)[std::make_pair(d, s)];
   if (w.bytes < bytes) {
     if (w.ptr) {
       // earlier work on this stream may still use the old buffer
@@ -182,6 +185,9 @@ hml_status release_all() {
   for (auto &kv : g_ws)
     if (kv.second.ptr) cudaFree(kv.second.ptr);
   g_ws.clear();
+  for (auto &kv : g_ws1)
+    if (kv.second.ptr) cudaFree(kv.second.ptr);
+  g_ws1.clear();
   for (auto &kv : g_counters)
     if (kv.second.ptr) cudaFree(kv.second.ptr);
   g_counters.clear();

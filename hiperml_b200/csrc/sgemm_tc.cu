@@ -1329,16 +1329,20 @@ hml_status launch_tc(const GemmProblem &p, const hml_sgemm_config &c, cudaStream
 //
 // The batched plan (batched.cu) hands the problems it routes to the tensor
 // cores to tc_batch_create.  Each tile width class (BN = 32, 64, 128) gets one
-// persistent launch of tc_batch_kernel with one CTA per SM; every CTA works
-// through its own list of (problem, 128-row tile, BN-column tile) items,
-// assigned on the host longest-first to the least-loaded CTA, so CTAs never
-// share state and never wait for each other.  The pipeline inside a CTA is
-// the single-problem kernel's (TMA warps, converter groups, MMA issuers with
-// one TMEM accumulator each, drain warps) walking the 64-deep chunks of its
-// items in order; the TMA descriptors of every problem sit in device memory.
-// A tile's arithmetic is the single-problem kernel's with split_k = 1, so
-// each result equals hml_sgemm_ex_config's for the same tile width, bit for
-// bit.
+// persistent launch of tc_batch_kernel with one CTA per SM.  The class's
+// (problem, 128-row tile, BN-column tile) items sit in device memory longest
+// first, and a device-side work queue hands them out: the CTA's TMA-A thread
+// takes the next item with an atomic on the class's queue head and publishes
+// it to the CTA's other roles through a ring of item slots in shared memory
+// (one mbarrier each way per slot), so every SM keeps pulling work until the
+// queue is empty.  The pipeline inside a CTA is the single-problem kernel's
+// (TMA warps, converter groups, MMA issuers with one TMEM accumulator each,
+// drain warps) walking the 64-deep chunks of its items in the order taken;
+// the TMA descriptors of every problem sit in device memory.  The last CTA
+// to finish resets the queue, so a graph replays the launch as it is.  A
+// tile's arithmetic is the single-problem kernel's with split_k = 1, so each
+// result equals hml_sgemm_ex_config's for the same tile width, bit for bit,
+// whichever CTA took it.
 namespace hml {
 namespace {
 
@@ -1361,31 +1365,56 @@ struct TcBatchArgs {
   const CUtensorMap *tmA;       // [problems], 64-byte aligned
   const CUtensorMap *tmB;       // [problems]
   const TcBatchProblem *probs;  // [problems]
-  const TcBatchItem *items;     // this class's items, grouped by CTA
-  const int2 *cta;              // [grid]: first item of the CTA, its number of chunks
+  const TcBatchItem *items;     // this class's items, longest first
+  int nitems;
+  unsigned *queue;              // [2]: queue head, CTAs finished (zero between launches)
   int sa, so;
   int *err;
 };
 
-// Walks the chunks of a CTA's item list in order.  next() is called before
-// every chunk but the first, so it never reads past the CTA's last item.
-struct ItemCursor {
+// Item slots between the CTA's TMA-A thread (which takes items from the
+// queue) and its other roles.  More than the items a CTA can have in flight:
+// an item is at least one chunk, and the pipeline holds at most
+// sa + so blocks (<= 16) plus NI chunks (<= 4).
+constexpr int kItemRing = 32;
+constexpr int kNoItem = -1;  // the sentinel published once the queue is empty
+
+// A role's walk through the items its CTA takes, in the order taken: item j
+// of the sequence is read from ring slot j % kItemRing once published, and
+// the slot is released right after the read (every role reads every item:
+// the roles count chunks across item boundaries).
+struct QueueCursor {
   TcBatchItem it;
   const TcBatchProblem *pr;
-  int item, c;
-  __device__ __forceinline__ void start(const TcBatchArgs &a, int i0) {
-    item = i0;
-    c = 0;
-    it = a.items[item];
-    pr = a.probs + it.prob;
-  }
-  __device__ __forceinline__ void next(const TcBatchArgs &a) {
-    if (++c == pr->cpt) {
-      c = 0;
-      ++item;
-      it = a.items[item];
-      pr = a.probs + it.prob;
+  int j = 0, c = 0;
+  bool end = false;
+  // Reads item j; false when the wait for it expired.  `warp_role`: every
+  // lane of the warp calls this, lane 0 releases the slot for the warp.
+  __device__ __forceinline__ bool fetch(const TcBatchArgs &a, uint64_t *ifull, uint64_t *iempty,
+                                        const TcBatchItem *ring, bool warp_role, int lane) {
+    const int r = j % kItemRing;
+    bool w = mbar_wait(&ifull[r], (j / kItemRing) & 1, a.err, kDevErrFullBarrier);
+    if (warp_role) w = __all_sync(0xffffffffu, w);
+    if (!w) return false;
+    it = ring[r];
+    if (warp_role) {
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&iempty[r]);
+    } else {
+      mbar_arrive(&iempty[r]);
     }
+    end = it.prob == kNoItem;
+    if (!end) pr = a.probs + it.prob;
+    c = 0;
+    return true;
+  }
+  // Advances past the current chunk, reading the next item at an item
+  // boundary; false when a wait expired.
+  __device__ __forceinline__ bool next(const TcBatchArgs &a, uint64_t *ifull, uint64_t *iempty,
+                                       const TcBatchItem *ring, bool warp_role, int lane) {
+    if (++c < pr->cpt) return true;
+    ++j;
+    return fetch(a, ifull, iempty, ring, warp_role, lane);
   }
 };
 
@@ -1426,10 +1455,14 @@ __global__ void __launch_bounds__(tcb_warps(BN, NS) * 32, 1) tc_batch_kernel(TcB
   uint64_t *accempty = accfull + NI;
   uint64_t *mmadone = accempty + NI;
   uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(mmadone + 1);
+  // item ring: slot published (producer) / slot read by every role
+  uint64_t *ifull = reinterpret_cast<uint64_t *>(tmem_slot + 2);
+  uint64_t *iempty = ifull + kItemRing;
+  TcBatchItem *iring = reinterpret_cast<TcBatchItem *>(iempty + kItemRing);
+  // readers of every item: the B loader, NI issuers, the converter and drain warps
+  constexpr int kItemReaders = 1 + NI + 4 * G + 4 * D;
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const int2 work = args.cta[blockIdx.x];
-  const int i0 = work.x, nch = work.y, nblk = nch * P;
   const uint32_t tmem_cols = tc_tmem_alloc_cols(BN, NS, SO);
 
   if (tid == 0) {
@@ -1446,6 +1479,10 @@ __global__ void __launch_bounds__(tcb_warps(BN, NS) * 32, 1) tc_batch_kernel(TcB
       mbar_init(&accempty[b], 4 * D);
     }
     mbar_init(mmadone, NI);
+    for (int r = 0; r < kItemRing; ++r) {
+      mbar_init(&ifull[r], 1);
+      mbar_init(&iempty[r], kItemReaders);
+    }
     fence_mbar_init();
   }
   if (warp == 2) tmem_alloc(tmem_slot, tmem_cols);
@@ -1457,87 +1494,116 @@ __global__ void __launch_bounds__(tcb_warps(BN, NS) * 32, 1) tc_batch_kernel(TcB
   const uint32_t tA = tmem + NI * BN;
 
   if (warp == 0) {
-    // -------------------------------------------------------- TMA, A
-    if (lane == 0 && nch > 0) {
-      ItemCursor cur;
-      cur.start(args, i0);
-      for (int blk = 0; blk < nblk; ++blk) {
-        if (blk > 0 && blk % P == 0) cur.next(args);
-        const CUtensorMap *tm = args.tmA + cur.it.prob;
-        const int m0 = cur.it.tm * kBM;
-        const int k0 = (cur.c * P + blk % P) * kBK;
-        const int s = blk % SA;
-        if (!mbar_wait(&aempty[s], ((blk / SA) & 1) ^ 1, args.err, kDevErrEmptyBarrier)) break;
-        mbar_arrive_expect_tx(&afull[s], A32_BYTES);
-        // k beyond K (the last chunk of a problem) reads TMA's zero fill
-        if (cur.pr->akc)
-          tma_load_2d(aring + s * A32_BYTES, tm, &afull[s], k0, m0);
-        else
-          tma_load_2d(aring + s * A32_BYTES, tm, &afull[s], m0, k0);
+    // ------------------------------------------- queue + TMA, A
+    // takes items from the class's queue, publishes each to the ring, then
+    // loads its A blocks; a sentinel ends every role's walk
+    if (lane == 0) {
+      int blk = 0;
+      // the index of the next item is taken one item ahead, so the atomic's
+      // round trip overlaps the current item's loads
+      unsigned idx = atomicAdd(&args.queue[0], 1u);
+      for (int j = 0;; ++j) {
+        const int r = j % kItemRing;
+        if (!mbar_wait(&iempty[r], ((j / kItemRing) & 1) ^ 1, args.err, kDevErrEmptyBarrier))
+          break;
+        TcBatchItem it = {kNoItem, 0, 0, 0};
+        if (idx < static_cast<unsigned>(args.nitems)) it = args.items[idx];
+        iring[r] = it;
+        mbar_arrive(&ifull[r]);  // release: the slot's item is visible to the waiters
+        if (it.prob == kNoItem) break;
+        idx = atomicAdd(&args.queue[0], 1u);
+        const TcBatchProblem &pr = args.probs[it.prob];
+        const CUtensorMap *tm = args.tmA + it.prob;
+        const int m0 = it.tm * kBM;
+        bool ok = true;
+        for (int kq = 0; kq < pr.cpt * P && ok; ++kq, ++blk) {
+          const int k0 = kq * kBK;
+          const int s = blk % SA;
+          if (!mbar_wait(&aempty[s], ((blk / SA) & 1) ^ 1, args.err, kDevErrEmptyBarrier)) {
+            ok = false;
+            break;
+          }
+          mbar_arrive_expect_tx(&afull[s], A32_BYTES);
+          // k beyond K (the last chunk of a problem) reads TMA's zero fill
+          if (pr.akc)
+            tma_load_2d(aring + s * A32_BYTES, tm, &afull[s], k0, m0);
+          else
+            tma_load_2d(aring + s * A32_BYTES, tm, &afull[s], m0, k0);
+        }
+        if (!ok) break;
       }
     }
   } else if (warp == 1) {
     // -------------------------------------------------------- TMA, B
-    if (lane == 0 && nch > 0) {
+    if (lane == 0) {
       // launched as a programmatic dependent of the previous kernel of the
       // plan: the B planes are complete once that kernel is (the kernel
       // before a tile kernel is the splitting kernel or another tile
       // kernel, itself complete only after the splitting kernel)
       wait_prior_grid();
-      ItemCursor cur;
-      cur.start(args, i0);
-      for (int blk = 0; blk < nblk; ++blk) {
-        if (blk > 0 && blk % P == 0) cur.next(args);
+      QueueCursor cur;
+      bool ok = cur.fetch(args, ifull, iempty, iring, false, lane);
+      for (int blk = 0; ok && !cur.end;) {
         const CUtensorMap *tm = args.tmB + cur.it.prob;
         const int n0 = cur.it.tn * BN;
-        const int k0 = (cur.c * P + blk % P) * kBK;
         const int np = cur.pr->n_pad;
-        const int o = blk % SO;
-        if (!mbar_wait(&opempty[o], ((blk / SO) & 1) ^ 1, args.err, kDevErrEmptyBarrier)) break;
-        uint8_t *dst = bring + o * BSLOT;
-        mbar_arrive_expect_tx(&opfull[o], BSLOT);
+        for (int kb = 0; kb < P; ++kb, ++blk) {
+          const int k0 = (cur.c * P + kb) * kBK;
+          const int o = blk % SO;
+          if (!mbar_wait(&opempty[o], ((blk / SO) & 1) ^ 1, args.err, kDevErrEmptyBarrier)) {
+            ok = false;
+            break;
+          }
+          uint8_t *dst = bring + o * BSLOT;
+          mbar_arrive_expect_tx(&opfull[o], BSLOT);
 #pragma unroll
-        for (int i = 0; i < NS; ++i)
-          tma_load_2d(dst + i * BPL_BYTES, tm, &opfull[o], k0, i * np + n0);
+          for (int i = 0; i < NS; ++i)
+            tma_load_2d(dst + i * BPL_BYTES, tm, &opfull[o], k0, i * np + n0);
+        }
+        if (ok) ok = cur.next(args, ifull, iempty, iring, false, lane);
       }
     }
   } else if (warp >= 2 && warp < 2 + NI) {
     // ---------------------------------------------------------- MMA
+    // issuer b takes the chunks q = b, b + NI, ... of the CTA's sequence
     if (lane == 0) {
       const int b = warp - 2;
       const uint32_t dacc = tacc + static_cast<uint32_t>(b * BN);
-      bool ok = true;
-      for (int j = b; j < nch && ok; j += NI) {
-        if (!mbar_wait(&accempty[b], ((j / NI) & 1) ^ 1, args.err, kDevErrEmptyBarrier)) {
-          ok = false;
-          break;
-        }
-        for (int kb = 0; kb < P; ++kb) {
-          const int blk = j * P + kb;
-          const int o = blk % SO;
-          if (!mbar_wait(&opfull[o], (blk / SO) & 1, args.err, kDevErrFullBarrier)) {
-            ok = false;
-            break;
+      QueueCursor cur;
+      bool ok = cur.fetch(args, ifull, iempty, iring, false, lane);
+      for (int q = 0; ok && !cur.end; ++q) {
+        if (q % NI == b) {
+          const int jq = q / NI;
+          if (!mbar_wait(&accempty[b], (jq & 1) ^ 1, args.err, kDevErrEmptyBarrier)) break;
+          for (int kb = 0; kb < P; ++kb) {
+            const int blk = q * P + kb;
+            const int o = blk % SO;
+            if (!mbar_wait(&opfull[o], (blk / SO) & 1, args.err, kDevErrFullBarrier)) {
+              ok = false;
+              break;
+            }
+            tc_fence_after();
+            const uint32_t astage = tA + static_cast<uint32_t>(o * SC);
+            const uint64_t b_desc = sw64_desc(smem_u32(bring + o * BSLOT));
+#pragma unroll
+            for (int kk = 0; kk < kBK / 16; ++kk) {
+#pragma unroll
+              for (int i = 0; i < NS; ++i)
+#pragma unroll
+                for (int jj = 0; jj < NS - i; ++jj) {
+                  const uint32_t at = astage + static_cast<uint32_t>(i * 16 + kk * 8);
+                  const uint64_t bd =
+                      b_desc + static_cast<uint64_t>((jj * BPL_BYTES + kk * 32) >> 4);
+                  const uint32_t acc = (kb > 0 || kk > 0 || i > 0 || jj > 0) ? 1u : 0u;
+                  mma_bf16_ts(dacc, at, bd, IDESC, acc);
+                }
+            }
+            mma_commit(&opempty[o]);
           }
-          tc_fence_after();
-          const uint32_t astage = tA + static_cast<uint32_t>(o * SC);
-          const uint64_t b_desc = sw64_desc(smem_u32(bring + o * BSLOT));
-#pragma unroll
-          for (int kk = 0; kk < kBK / 16; ++kk) {
-#pragma unroll
-            for (int i = 0; i < NS; ++i)
-#pragma unroll
-              for (int jj = 0; jj < NS - i; ++jj) {
-                const uint32_t at = astage + static_cast<uint32_t>(i * 16 + kk * 8);
-                const uint64_t bd =
-                    b_desc + static_cast<uint64_t>((jj * BPL_BYTES + kk * 32) >> 4);
-                const uint32_t acc = (kb > 0 || kk > 0 || i > 0 || jj > 0) ? 1u : 0u;
-                mma_bf16_ts(dacc, at, bd, IDESC, acc);
-              }
-          }
-          mma_commit(&opempty[o]);
+          if (!ok) break;
+          mma_commit(&accfull[b]);
         }
-        if (ok) mma_commit(&accfull[b]);
+        ok = cur.next(args, ifull, iempty, iring, false, lane);
       }
       mma_commit(mmadone);
     }
@@ -1547,11 +1613,10 @@ __global__ void __launch_bounds__(tcb_warps(BN, NS) * 32, 1) tc_batch_kernel(TcB
     const int g = (warp - kConvWarp0) >> 2;
     const int m = tid & (kBM - 1);
     const uint32_t lanes = static_cast<uint32_t>((warp & 3) * 32) << 16;
-    ItemCursor cur;
-    if (nch > 0) cur.start(args, i0);
-    for (int j = 0; j < nch; ++j) {
-      if (j > 0) cur.next(args);
-      const int blk = j * P + g;
+    QueueCursor cur;
+    bool ok = cur.fetch(args, ifull, iempty, iring, true, lane);
+    for (int q = 0; ok && !cur.end; ++q) {
+      const int blk = q * P + g;
       const int s = blk % SA, o = blk % SO;
       bool w = mbar_wait(&afull[s], (blk / SA) & 1, args.err, kDevErrFullBarrier);
       if (!__all_sync(0xffffffffu, w)) break;
@@ -1587,6 +1652,7 @@ __global__ void __launch_bounds__(tcb_warps(BN, NS) * 32, 1) tc_batch_kernel(TcB
       tc_fence_before();
       __syncwarp();
       if (lane == 0) mbar_arrive(&opfull[o]);
+      ok = cur.next(args, ifull, iempty, iring, true, lane);
     }
   } else if (warp >= kDrainWarp0) {
     // ------------------------------------------ drain (D groups)
@@ -1596,12 +1662,11 @@ __global__ void __launch_bounds__(tcb_warps(BN, NS) * 32, 1) tc_batch_kernel(TcB
     float sums[DC];
 #pragma unroll
     for (int i = 0; i < DC; ++i) sums[i] = 0.0f;
-    ItemCursor cur;
-    if (nch > 0) cur.start(args, i0);
-    for (int j = 0; j < nch; ++j) {
-      if (j > 0) cur.next(args);
-      const int b = j % NI;
-      const bool w = mbar_wait(&accfull[b], (j / NI) & 1, args.err, kDevErrMmaBarrier);
+    QueueCursor cur;
+    bool ok = cur.fetch(args, ifull, iempty, iring, true, lane);
+    for (int q = 0; ok && !cur.end; ++q) {
+      const int b = q % NI;
+      const bool w = mbar_wait(&accfull[b], (q / NI) & 1, args.err, kDevErrMmaBarrier);
       if (!__all_sync(0xffffffffu, w)) break;
       tc_fence_after();
       const uint32_t src = tacc + lanes + static_cast<uint32_t>(b * BN + d * DC);
@@ -1642,6 +1707,7 @@ __global__ void __launch_bounds__(tcb_warps(BN, NS) * 32, 1) tc_batch_kernel(TcB
 #pragma unroll
         for (int i = 0; i < DC; ++i) sums[i] = 0.0f;
       }
+      ok = cur.next(args, ifull, iempty, iring, true, lane);
     }
   }
   tc_fence_before();
@@ -1653,6 +1719,16 @@ __global__ void __launch_bounds__(tcb_warps(BN, NS) * 32, 1) tc_batch_kernel(TcB
     (void)w;
     tc_fence_after();
     tmem_dealloc(tmem, tmem_cols);
+  }
+  if (tid == 0) {
+    // the last CTA out resets the queue for the next launch (every CTA's
+    // last atomic on the head came before its own increment here)
+    __threadfence();
+    if (atomicAdd(&args.queue[1], 1u) == gridDim.x - 1) {
+      args.queue[0] = 0u;
+      args.queue[1] = 0u;
+      __threadfence();
+    }
   }
 }
 
@@ -1730,15 +1806,20 @@ namespace {
 
 size_t up256(size_t b) { return (b + 255) & ~static_cast<size_t>(255); }
 
+// Shared memory of the item ring: slots plus their two barriers.
+constexpr size_t kItemRingBytes = kItemRing * (sizeof(TcBatchItem) + 2 * sizeof(uint64_t)) + 16;
+
 template <int BN>
 hml_status tc_batch_class_setup(TcBatch::Class &c) {
   TcPlan plan;
   int sa = 8;
-  while (sa >= 2 && !tc_plan(BN, kBatchTcNS, sa, &plan)) sa -= 2;
+  while (sa >= 2 && !(tc_plan(BN, kBatchTcNS, sa, &plan) &&
+                      tc_plan_bytes(BN, kBatchTcNS, plan) + kItemRingBytes <= 227 * 1024))
+    sa -= 2;
   if (sa < 2) return HML_STATUS_NOT_SUPPORTED;
   c.args.sa = plan.sa;
   c.args.so = plan.so;
-  c.smem = tc_plan_bytes(BN, kBatchTcNS, plan);
+  c.smem = tc_plan_bytes(BN, kBatchTcNS, plan) + kItemRingBytes;
   const cudaError_t e = cudaFuncSetAttribute(tc_batch_kernel<BN, kBatchTcNS>,
                                              cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              static_cast<int>(c.smem));
@@ -1779,60 +1860,32 @@ hml_status tc_batch_create(const GemmProblem *probs, int count, cudaStream_t str
         items[cls[i]].push_back({k_pad[i] / kChunkK, TcBatchItem{i, static_cast<int>(x),
                                                                  static_cast<int>(y), 0}});
   }
-  // longest-processing-time assignment per class: items longest first, each
-  // to the CTA with the least work so far; then grouped by CTA
+  // per class: the items longest first, the order the queue hands them out
+  // (each CTA takes the next when it can: longest-processing-time first)
   std::vector<TcBatchItem> cls_items[3];
-  std::vector<int2> cls_cta[3];
   size_t total_items = 0;
   for (int c = 0; c < 3; ++c) {
     auto &v = items[c];
     if (v.empty()) continue;
+    if (v.size() > 0x7fffffffu) return HML_STATUS_NOT_SUPPORTED;
     std::stable_sort(v.begin(), v.end(),
                      [](const std::pair<int, TcBatchItem> &a, const std::pair<int, TcBatchItem> &b) {
                        return a.first > b.first;
                      });
-    const int grid = static_cast<int>(std::min<size_t>(v.size(), static_cast<size_t>(sms)));
-    std::vector<std::vector<TcBatchItem>> per(grid);
-    std::vector<int64_t> load(grid, 0);
-    // (load, cta) min-heap
-    std::vector<std::pair<int64_t, int>> heap;
-    for (int g = 0; g < grid; ++g) heap.push_back({0, g});
-    auto cmp = [](const std::pair<int64_t, int> &a, const std::pair<int64_t, int> &b) {
-      return a.first != b.first ? a.first > b.first : a.second > b.second;
-    };
-    std::make_heap(heap.begin(), heap.end(), cmp);
-    for (const auto &e : v) {
-      std::pop_heap(heap.begin(), heap.end(), cmp);
-      auto &top = heap.back();
-      per[top.second].push_back(e.second);
-      top.first += e.first;
-      load[top.second] = top.first;
-      std::push_heap(heap.begin(), heap.end(), cmp);
-    }
-    for (int g = 0; g < grid; ++g) {
-      const int first = static_cast<int>(cls_items[c].size());
-      int64_t chunks = 0;
-      for (const auto &it : per[g]) {
-        cls_items[c].push_back(it);
-        chunks += k_pad[it.prob] / kChunkK;
-      }
-      if (chunks > 0x7fffffff / kChunkK) return HML_STATUS_NOT_SUPPORTED;
-      cls_cta[c].push_back(make_int2(first, static_cast<int>(chunks)));
-    }
+    for (const auto &e : v) cls_items[c].push_back(e.second);
     total_items += v.size();
   }
-  // device layout: tensor maps | problems | split descriptors | per class
-  // items and CTA table | planes
+  // device layout: tensor maps | problems | split descriptors | queues |
+  // per class items | planes
   const size_t o_tmA = 0, o_tmB = up256(count * sizeof(CUtensorMap));
   const size_t o_prob = o_tmB + up256(count * sizeof(CUtensorMap));
   const size_t o_split = o_prob + up256(count * sizeof(TcBatchProblem));
-  size_t o = o_split + up256(count * sizeof(TcSplitDesc));
-  size_t o_items[3], o_cta[3];
+  const size_t o_queue = o_split + up256(count * sizeof(TcSplitDesc));
+  size_t o = o_queue + up256(3 * 2 * sizeof(unsigned));
+  size_t o_items[3];
   for (int c = 0; c < 3; ++c) {
     o_items[c] = o;
     o += up256(cls_items[c].size() * sizeof(TcBatchItem));
-    o_cta[c] = o;
-    o += up256(cls_cta[c].size() * sizeof(int2));
   }
   const size_t o_planes = o;
   const size_t total = o_planes + planes_bytes;
@@ -1894,17 +1947,17 @@ hml_status tc_batch_create(const GemmProblem *probs, int count, cudaStream_t str
     upload(o_tmB, tmB.data(), count * sizeof(CUtensorMap));
     upload(o_prob, hp.data(), count * sizeof(TcBatchProblem));
     upload(o_split, hs.data(), count * sizeof(TcSplitDesc));
-    for (int c = 0; c < 3; ++c) {
+    for (int c = 0; c < 3; ++c)
       upload(o_items[c], cls_items[c].data(), cls_items[c].size() * sizeof(TcBatchItem));
-      upload(o_cta[c], cls_cta[c].data(), cls_cta[c].size() * sizeof(int2));
-    }
+    const unsigned zeros[6] = {0u, 0u, 0u, 0u, 0u, 0u};  // queue heads and finished counts
+    upload(o_queue, zeros, sizeof zeros);
     // pageable sources: a synchronous copy has consumed them on return; the
     // stream-ordered ones have been staged by the driver before returning
   }
   hml_status st = ok ? cuda_status(e) : HML_STATUS_CUDA_ERROR;
   for (int c = 0; c < 3 && st == HML_STATUS_SUCCESS; ++c) {
     TcBatch::Class &k = b->cls[c];
-    k.grid = static_cast<int>(cls_cta[c].size());
+    k.grid = static_cast<int>(std::min<size_t>(cls_items[c].size(), static_cast<size_t>(sms)));
     if (k.grid == 0) continue;
     st = c == 0   ? tc_batch_class_setup<32>(k)
          : c == 1 ? tc_batch_class_setup<64>(k)
@@ -1913,7 +1966,8 @@ hml_status tc_batch_create(const GemmProblem *probs, int count, cudaStream_t str
     k.args.tmB = reinterpret_cast<const CUtensorMap *>(base + o_tmB);
     k.args.probs = reinterpret_cast<const TcBatchProblem *>(base + o_prob);
     k.args.items = reinterpret_cast<const TcBatchItem *>(base + o_items[c]);
-    k.args.cta = reinterpret_cast<const int2 *>(base + o_cta[c]);
+    k.args.nitems = static_cast<int>(cls_items[c].size());
+    k.args.queue = reinterpret_cast<unsigned *>(base + o_queue) + 2 * c;
     k.args.err = device_error_word();
     b->ctas = std::max(b->ctas, k.grid);
   }

@@ -157,18 +157,10 @@ struct SimtTile {
             b[4 * j + 0] = v.x; b[4 * j + 1] = v.y; b[4 * j + 2] = v.z; b[4 * j + 3] = v.w;
           }
         }
-        // packed FP32x2 FMAs (fma.rn.f32x2): each half rounds exactly as the
-        // scalar fmaf, so the sums are bitwise those of scalar FMAs in the
-        // same order, with half the FMA instructions issued
 #pragma unroll
         for (int i = 0; i < TM; ++i)
 #pragma unroll
-          for (int j = 0; j < TN; j += 2) {
-            const float2 t = __ffma2_rn(make_float2(a[i], a[i]), make_float2(b[j], b[j + 1]),
-                                        make_float2(acc[i][j], acc[i][j + 1]));
-            acc[i][j] = t.x;
-            acc[i][j + 1] = t.y;
-          }
+          for (int j = 0; j < TN; ++j) acc[i][j] = fmaf(a[i], b[j], acc[i][j]);
       }
     }
   }

@@ -432,6 +432,28 @@ hml_status hml_cfg_v1_save(int kind, const char *path);
  * library's own selection). */
 hml_status hml_sgemm_v1_config(int M, int N, int K, hml_sgemm_config *config);
 
+/* --------------------------------------------------- k-means assignment */
+
+/* assignments[p] = argmin_k sum_d (points[p][d] - centroids[k][d])^2, the
+ * assignment step of HiperML's k-means (hmlKmeansAssignCtrdSmem,
+ * include/hml_kmeans_kernel_template.h:19-90): device pointers, points
+ * row-major [num_points][dims], centroids row-major [num_clusters][dims],
+ * assignments uint32 [num_points].  Computed as ||c||^2 - 2 x.c with the
+ * skinny SGEMM (FP32-accurate configuration) and made exact: every point
+ * gets the index the reference kernel gives (its FP32 sums, the first k on
+ * ties).  Uses the stream's second workspace (num_points x num_clusters
+ * floats).  Stream ordered. */
+hml_status hml_kmeans_assign(const float *points, int num_points, int dims,
+                             const float *centroids, int num_clusters,
+                             uint32_t *assignments, void *stream);
+
+/* The same, adding to *exact_count (a device counter) the number of points
+ * whose candidates had to be compared with the reference's own arithmetic. */
+hml_status hml_kmeans_assign_stats(const float *points, int num_points,
+                                   int dims, const float *centroids,
+                                   int num_clusters, uint32_t *assignments,
+                                   unsigned *exact_count, void *stream);
+
 /* ------------------------------------------------------------ utilities */
 
 /* Text of the last CUDA error seen by this thread inside the library. */

@@ -64,6 +64,9 @@ def lib():
                                            _c_float_p, i64, i64, _c_double_p,
                                            _c_double_p, ctypes.c_int]
         L.oracle_dgemm_strided.restype = ctypes.c_int
+        L.oracle_kmeans_assign.argtypes = [_c_float_p, ctypes.c_int64, ctypes.c_int, _c_float_p,
+                                           ctypes.c_int, ctypes.POINTER(ctypes.c_uint32)]
+        L.oracle_kmeans_assign.restype = None
         _lib = L
     return _lib
 
@@ -286,6 +289,38 @@ def ref_csum(C):
     if C.ndim == 1:
         return ref().ysum(_fp(C), C.shape[0])
     return ref().csum(_fp(C), C.shape[0], C.shape[1])
+
+
+def kmeans_assign(points, centroids):
+    """Nearest-centroid index per point with the reference kernel's
+    arithmetic (hml_oracle.c: oracle_kmeans_assign)."""
+    P = np.ascontiguousarray(points, np.float32)
+    C = np.ascontiguousarray(centroids, np.float32)
+    out = np.zeros(P.shape[0], np.uint32)
+    lib().oracle_kmeans_assign(_fp(P), P.shape[0], P.shape[1], _fp(C), C.shape[0],
+                               out.ctypes.data_as(ctypes.POINTER(ctypes.c_uint32)))
+    return out
+
+
+def ref_gpu_kmeans_available() -> bool:
+    return os.path.exists(os.path.join(_HERE, "_ref", "libhml_ref_gpu_kmeans.so"))
+
+
+def ref_gpu_kmeans_assign(asg, rows, n, ctrds, k, d, reps=1):
+    """The reference's hmlKmeansAssignCtrdSmem on device pointers (ints);
+    returns ms per launch."""
+    if "kmeans" not in _ref_gpu:
+        L = _load(os.path.join(_HERE, "_ref", "libhml_ref_gpu_kmeans.so"))
+        vp, u = ctypes.c_void_p, ctypes.c_uint32
+        L.ref_gpu_kmeans_assign.argtypes = [vp, vp, u, vp, u, u, ctypes.c_int,
+                                            ctypes.POINTER(ctypes.c_float)]
+        _ref_gpu["kmeans"] = L
+    ms = ctypes.c_float()
+    rc = _ref_gpu["kmeans"].ref_gpu_kmeans_assign(asg, rows, n, ctrds, k, d, reps,
+                                                  ctypes.byref(ms))
+    if rc != 0:
+        raise RuntimeError(f"reference k-means kernel: CUDA status {rc}")
+    return ms.value
 
 
 def rel_errors(approx, exact, absbound=None):

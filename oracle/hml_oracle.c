@@ -28,6 +28,8 @@
  * them into oracle/_ref) and against the committed fixtures that those loops
  * produced (tests/golden/).
  */
+#include <float.h>
+#include <math.h>
 #include <pthread.h>
 #include <stdint.h>
 #include <stdlib.h>
@@ -202,4 +204,32 @@ int oracle_sgemm_rm_f32_mt(float *C, const float *A, const float *B, int M,
   sgemm_worker(&jobs[0]);
   for (int t = 1; t < threads; ++t) pthread_join(tid[t], NULL);
   return 0;
+}
+
+/* k-means assignment with the arithmetic of the reference's GPU kernel
+ * hmlKmeansAssignCtrdSmem (include/hml_kmeans_kernel_template.h:19-90):
+ * dist = sum over d, in order, of delta * delta with delta = x - c, each step
+ * one fused multiply-add (what nvcc makes of `dist += delta * delta`), from
+ * 0; the first k whose dist is below the running minimum (from FLT_MAX)
+ * wins.  points [n][d], centroids [k][d], row-major. */
+void oracle_kmeans_assign(const float *points, int64_t n, int d, const float *ctrds, int k,
+                          uint32_t *out) {
+  for (int64_t p = 0; p < n; ++p) {
+    const float *x = points + p * d;
+    float min_dist = FLT_MAX;
+    uint32_t min_k = 0;
+    for (int c = 0; c < k; ++c) {
+      const float *cc = ctrds + (int64_t)c * d;
+      float dist = 0.0f;
+      for (int j = 0; j < d; ++j) {
+        const float delta = x[j] - cc[j];
+        dist = fmaf(delta, delta, dist);
+      }
+      if (dist < min_dist) {
+        min_dist = dist;
+        min_k = (uint32_t)c;
+      }
+    }
+    out[p] = min_k;
+  }
 }

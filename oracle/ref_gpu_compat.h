@@ -16,8 +16,9 @@
  *   - cudaBindTexture / cudaUnbindTexture record the bound (pointer, length)
  *     in a small __device__ table of every translation unit of the library;
  *   - tex1Dfetch(t, i) reads element i of the range bound to t, 0 outside it.
- * One library is built per reference API (HML_REF_SGEMM or HML_REF_SGEMV),
- * because both define a texture named texFloatA.
+ * One library is built per reference API (HML_REF_SGEMM, HML_REF_SGEMV or
+ * HML_REF_KMEANS), because the SGEMM and SGEMV sources both define a texture
+ * named texFloatA.
  */
 #ifndef HML_ORACLE_REF_GPU_COMPAT_H_
 #define HML_ORACLE_REF_GPU_COMPAT_H_
@@ -39,10 +40,15 @@ void hml_ref_register_texture(const void *host_obj, int id);
 void hml_ref_register_table(cudaError_t (*update)(int id, const void *ptr, size_t n));
 cudaError_t hml_ref_bind(const void *host_obj, const void *ptr, size_t n);
 
-enum { hml_ref_tex_texFloatA = 0, hml_ref_tex_texFloatB = 1, hml_ref_tex_texFloatx = 2 };
+enum {
+  hml_ref_tex_texFloatA = 0,
+  hml_ref_tex_texFloatB = 1,
+  hml_ref_tex_texFloatx = 2,
+  hml_ref_tex_texData1 = 3
+};
 
 /* this translation unit's table, and its update hook */
-static __device__ HmlRefTexRange hml_ref_tex_table[3];
+static __device__ HmlRefTexRange hml_ref_tex_table[4];
 static cudaError_t hml_ref_update_table(int id, const void *ptr, size_t n) {
   HmlRefTexRange r;
   r.ptr = ptr;

@@ -1,0 +1,111 @@
+"""The k-means assignment step on the skinny SGEMM (GPU).
+
+hml_kmeans_assign computes argmin_k ||c_k||^2 - 2 x.c_k from one GEMM and
+resolves every close call with the reference kernel's own arithmetic, so its
+indices must equal, bit for bit, those of
+  * the C restatement of the reference kernel (oracle.kmeans_assign), and
+  * the reference's own GPU kernel hmlKmeansAssignCtrdSmem
+    (include/hml_kmeans_kernel_template.h:19-90, built into oracle/_ref),
+on random data, on data built to be close to ties (centroid pairs a few ulps
+apart, duplicated centroids, points on the perpendicular bisector), on points
+far from the origin (where ||x||^2 - 2 x.c cancels) and on a large case.
+"""
+import numpy as np
+import pytest
+
+import hiperml_b200 as hml
+import oracle
+
+pytestmark = pytest.mark.gpu
+
+
+def dev(a):
+    import torch
+    return torch.from_numpy(np.ascontiguousarray(a, np.float32)).cuda()
+
+
+def ours(P, C):
+    out, exact = hml.kmeans_assign(dev(P), dev(C), count_exact=True)
+    return out.cpu().numpy().astype(np.uint32), exact
+
+
+def clustered(rng, n, d, k, spread=0.3):
+    C = rng.standard_normal((k, d)).astype(np.float32)
+    lab = rng.integers(0, k, n)
+    P = (C[lab] + spread * rng.standard_normal((n, d))).astype(np.float32)
+    return P, C
+
+
+@pytest.mark.parametrize("d", [1, 3, 8, 16, 32, 64, 100])
+@pytest.mark.parametrize("k", [1, 2, 16, 130])
+def test_matches_reference_arithmetic(cuda, d, k):
+    rng = np.random.default_rng(d * 1000 + k)
+    P, C = clustered(rng, 3000, d, k)
+    got, _ = ours(P, C)
+    np.testing.assert_array_equal(got, oracle.kmeans_assign(P, C))
+
+
+def test_near_ties_duplicates_and_bisectors(cuda):
+    rng = np.random.default_rng(7)
+    d = 16
+    base = rng.standard_normal((20, d)).astype(np.float32)
+    # pairs a few ulps apart, exact duplicates, and the rest
+    near = np.nextafter(base[:10], np.float32(np.inf)).astype(np.float32)
+    C = np.concatenate([base, near, base[10:15]]).astype(np.float32)
+    # points: on centroids, on bisectors of close pairs, and random
+    mid = ((base[:10].astype(np.float64) + near.astype(np.float64)) / 2).astype(np.float32)
+    bis = ((base[:10].astype(np.float64) + base[10:20].astype(np.float64)) / 2).astype(np.float32)
+    P = np.concatenate([C, mid, bis, rng.standard_normal((4000, d)).astype(np.float32)])
+    got, exact = ours(P, C)
+    np.testing.assert_array_equal(got, oracle.kmeans_assign(P, C))
+    assert exact >= 20  # the close calls went through the reference's arithmetic
+
+
+def test_far_from_origin(cuda):
+    """A common offset of 1e3 makes ||x||^2 - 2 x.c cancel: most points need
+    the exact comparison, and still agree."""
+    rng = np.random.default_rng(8)
+    P, C = clustered(rng, 5000, 24, 40, spread=0.5)
+    P += np.float32(1e3)
+    C += np.float32(1e3)
+    got, exact = ours(P, C)
+    np.testing.assert_array_equal(got, oracle.kmeans_assign(P, C))
+    assert exact > 0
+
+
+@pytest.mark.skipif(not oracle.ref_gpu_kmeans_available(),
+                    reason="reference k-means kernel not built (make -C oracle refgpu)")
+@pytest.mark.parametrize("d", [8, 16, 32, 64])
+def test_matches_reference_gpu_kernel(cuda, d):
+    import torch
+    rng = np.random.default_rng(100 + d)
+    P, C = clustered(rng, 200000, d, 64, spread=0.8)
+    dP, dC = dev(P), dev(C)
+    ref = torch.zeros(P.shape[0], dtype=torch.int32, device="cuda")
+    oracle.ref_gpu_kmeans_assign(ref.data_ptr(), dP.data_ptr(), P.shape[0], dC.data_ptr(),
+                                 C.shape[0], d)
+    got, exact = hml.kmeans_assign(dP, dC, count_exact=True)
+    torch.cuda.synchronize()
+    assert torch.equal(got, ref), int((got != ref).sum())
+    np.testing.assert_array_equal(got.cpu().numpy().astype(np.uint32)[:20000],
+                                  oracle.kmeans_assign(P[:20000], C))
+
+
+@pytest.mark.skipif(not oracle.ref_gpu_kmeans_available(),
+                    reason="reference k-means kernel not built (make -C oracle refgpu)")
+def test_large_case_against_reference_gpu_kernel(cuda):
+    """1M points, 32 dims, 256 centroids."""
+    import torch
+    n, d, k = 1 << 20, 32, 256
+    P = torch.empty(n * d, device="cuda")
+    hml.fill_random(P, 9, 0, 1)
+    Cn = torch.empty(k * d, device="cuda")
+    hml.fill_random(Cn, 9, 1, 1)
+    P = P.view(n, d)
+    C = Cn.view(k, d)
+    ref = torch.zeros(n, dtype=torch.int32, device="cuda")
+    oracle.ref_gpu_kmeans_assign(ref.data_ptr(), P.data_ptr(), n, C.data_ptr(), k, d)
+    got = hml.kmeans_assign(P, C)
+    torch.cuda.synchronize()
+    assert torch.equal(got, ref), int((got != ref).sum())
+    assert hml.device_error() == 0
