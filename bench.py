@@ -738,51 +738,67 @@ def reference_gpu_entry(ctx, reps=3):
 
 
 def kmeans_entry(ctx, reps=5):
-    """The k-means assignment step (hml_kmeans_assign: one skinny SGEMM and
-    an exact argmin) against the reference's own assignment kernel
-    hmlKmeansAssignCtrdSmem (oracle/_ref), 1M points, N(0,1), kernel time
-    with CUDA events, and whether the two index arrays are equal."""
+    """The k-means assignment step (hml_kmeans_assign_ex: the dot products as
+    one skinny GEMM, an exact argmin) in both of its forms -- tiled (the
+    argmin fused into a register-tiled SIMT GEMM) and SGEMM (the products
+    through HBM, then a pick kernel) -- against the reference's own assignment
+    kernel hmlKmeansAssignCtrdSmem (oracle/_ref; up to 64 dimensions, as in
+    the reference), 1M points, N(0,1), kernel time with CUDA events, and
+    whether the index arrays are equal."""
     import torch
 
     import hiperml_b200 as hml
     import oracle
     from hiperml_b200 import datagen as dg
+
+    def timed(fn):
+        evs = []
+        for i in range(reps + 2):
+            a = torch.cuda.Event(enable_timing=True)
+            b = torch.cuda.Event(enable_timing=True)
+            a.record(ctx.stream)
+            fn()
+            b.record(ctx.stream)
+            evs.append((a, b))
+        torch.cuda.synchronize()
+        return statistics.median(a.elapsed_time(b) for a, b in evs[2:])
+
     out = []
-    for (n, d, k) in ((1 << 20, 32, 64), (1 << 20, 32, 256), (1 << 20, 64, 128)):
+    for (n, d, k) in ((1 << 20, 32, 64), (1 << 20, 32, 256), (1 << 20, 64, 128),
+                      (1 << 20, 128, 64), (1 << 20, 256, 64)):
         P = torch.empty(n * d, device=ctx.dev)
         C = torch.empty(k * d, device=ctx.dev)
         hml.fill_random(P, 11, 0, dg.NORMAL)
         hml.fill_random(C, 11, 1, dg.NORMAL)
         P, C = P.view(n, d), C.view(k, d)
         got = torch.empty(n, dtype=torch.int32, device=ctx.dev)
-        evs = []
-        for i in range(reps + 2):
-            a = torch.cuda.Event(enable_timing=True)
-            b = torch.cuda.Event(enable_timing=True)
-            a.record(ctx.stream)
-            hml.kmeans_assign(P, C, out=got, stream=ctx.stream)
-            b.record(ctx.stream)
-            evs.append((a, b))
-        torch.cuda.synchronize()
-        t_ours = statistics.median(a.elapsed_time(b) for a, b in evs[2:])
-        entry = {"points": n, "dims": d, "clusters": k, "ours_ms": t_ours,
-                 "ours_points_per_s": n / (t_ours * 1e-3),
-                 "gemm_tflops": 2.0 * n * d * k / (t_ours * 1e-3) / 1e12}
+        entry = {"points": n, "dims": d, "clusters": k}
+        results = {}
+        for name, method in (("tiled", hml.KMEANS_TILED), ("gemm", hml.KMEANS_GEMM),
+                             ("auto", hml.KMEANS_AUTO)):
+            t = timed(lambda: hml.kmeans_assign(P, C, out=got, stream=ctx.stream, method=method))
+            entry[f"{name}_ms"] = t
+            results[name] = got.clone()
+        t_ours = entry["auto_ms"]
+        entry.update({"ours_points_per_s": n / (t_ours * 1e-3),
+                      "gemm_tflops": 2.0 * n * d * k / (t_ours * 1e-3) / 1e12,
+                      "forms_equal": bool(torch.equal(results["tiled"], results["gemm"]))})
         _, exact = hml.kmeans_assign(P, C, count_exact=True)
         entry["points_resolved_exactly"] = exact
-        if oracle.ref_gpu_kmeans_available():
+        if oracle.ref_gpu_kmeans_available() and d in (4, 8, 16, 32, 64):
             ref = torch.zeros(n, dtype=torch.int32, device=ctx.dev)
             oracle.ref_gpu_kmeans_assign(ref.data_ptr(), P.data_ptr(), n, C.data_ptr(), k, d, 1)
             t_ref = oracle.ref_gpu_kmeans_assign(ref.data_ptr(), P.data_ptr(), n, C.data_ptr(), k,
                                                  d, reps)
             torch.cuda.synchronize()
             entry.update({"reference_ms": t_ref, "speedup": t_ref / t_ours,
-                          "indices_equal": bool(torch.equal(got, ref))})
+                          "indices_equal": bool(torch.equal(results["auto"], ref))})
         out.append(entry)
-        del P, C, got
+        del P, C, got, results
     return {"workload": "kmeans_assign",
             "config": {"data": "points and centroids N(0,1), seed 11", "layout": "row-major",
-                       "reference": "hmlKmeansAssignCtrdSmem built from the reference's header"},
+                       "reference": "hmlKmeansAssignCtrdSmem built from the reference's header "
+                                    "(dimensions up to 64, its limit)"},
             "shapes": out}
 
 

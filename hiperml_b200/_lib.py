@@ -100,8 +100,8 @@ _SIGS = {
     "hml_sgemm_v1_config": (c_int, [c_int, c_int, c_int, ctypes.POINTER(SgemmConfig)]),
     "hml_fill_random": (c_int, [c_void_p, c_size_t, c_uint64, c_uint64, c_int, c_void_p]),
     "hml_kmeans_assign": (c_int, [c_void_p, c_int, c_int, c_void_p, c_int, c_void_p, c_void_p]),
-    "hml_kmeans_assign_stats": (c_int, [c_void_p, c_int, c_int, c_void_p, c_int, c_void_p,
-                                        c_void_p, c_void_p]),
+    "hml_kmeans_assign_ex": (c_int, [c_void_p, c_int, c_int, c_void_p, c_int, c_void_p, c_int,
+                                     c_void_p, c_void_p]),
     "hml_sgemm_error_fp64": (c_int, [c_int, c_int, c_int, c_int, c_int, c_int, c_float, c_void_p,
                                      c_int, c_void_p, c_int, c_float, c_void_p, c_void_p, c_int,
                                      ctypes.POINTER(c_double), c_void_p]),

@@ -218,12 +218,18 @@ def error_fp64(order, transA, transB, M, N, K, alpha, A, lda, B, ldb, beta, C0, 
     return tuple(err)
 
 
-def kmeans_assign(points, centroids, out=None, stream=None, count_exact=False):
-    """Nearest-centroid index of every point (``hml_kmeans_assign``): points
-    (n x d) and centroids (k x d) are row-major float32 CUDA tensors; returns
-    an int32 tensor of n indices (the reference kernel's, bit for bit), and
-    with ``count_exact`` also the number of points whose candidates were
-    resolved with the reference's own arithmetic."""
+KMEANS_AUTO, KMEANS_TILED, KMEANS_GEMM = 0, 1, 2
+
+
+def kmeans_assign(points, centroids, out=None, stream=None, count_exact=False,
+                  method=KMEANS_AUTO):
+    """Nearest-centroid index of every point (``hml_kmeans_assign_ex``):
+    points (n x d) and centroids (k x d) are row-major float32 CUDA tensors;
+    returns an int32 tensor of n indices (the reference kernel's, bit for
+    bit), and with ``count_exact`` also the number of points whose candidates
+    were resolved with the reference's own arithmetic.  ``method``: 0 = the
+    library's choice, 1 = the tiled SIMT form with the argmin fused, 2 = the
+    SGEMM form (products through HBM)."""
     import torch
     n, d = points.shape
     k, d2 = centroids.shape
@@ -233,13 +239,12 @@ def kmeans_assign(points, centroids, out=None, stream=None, count_exact=False):
         raise ValueError("points and centroids must be row-major contiguous")
     if out is None:
         out = torch.empty(n, dtype=torch.int32, device=points.device)
+    cnt = torch.zeros(1, dtype=torch.int32, device=points.device) if count_exact else None
+    check(lib.hml_kmeans_assign_ex(_ptr(points), n, d, _ptr(centroids), k, _ptr(out), method,
+                                   _ptr(cnt) if cnt is not None else None, _stream(stream)),
+          "hml_kmeans_assign_ex")
     if count_exact:
-        cnt = torch.zeros(1, dtype=torch.int32, device=points.device)
-        check(lib.hml_kmeans_assign_stats(_ptr(points), n, d, _ptr(centroids), k, _ptr(out),
-                                          _ptr(cnt), _stream(stream)), "hml_kmeans_assign")
         return out, int(cnt.item())
-    check(lib.hml_kmeans_assign(_ptr(points), n, d, _ptr(centroids), k, _ptr(out),
-                                _stream(stream)), "hml_kmeans_assign")
     return out
 
 

@@ -44,7 +44,9 @@
 // cache (LDG broadcasts) instead of staging it in shared memory capped the
 // same structure at 5.0 TB/s with either B.  For 8 < N <= 16 the 64
 // accumulators a thread cost the second CTA on each SM, and the split-BF16
-// tensor-core kernel is faster there.
+// tensor-core kernel is faster there (an NB = 16 instantiation at one CTA
+// per SM, measured: 4096 x 16 x 4096 with L2 flushed 58 us against 29.7 us,
+// 65536 x 16 x 4096 320 us against 336 us, i.e. A at 3.4 TB/s).
 #include <algorithm>
 #include <cstring>
 

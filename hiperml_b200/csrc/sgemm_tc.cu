@@ -1378,6 +1378,7 @@ struct TcBatchArgs {
 // sa + so blocks (<= 16) plus NI chunks (<= 4).
 constexpr int kItemRing = 32;
 constexpr int kNoItem = -1;  // the sentinel published once the queue is empty
+constexpr int kQueueAhead = 4;  // queue indices a CTA's producer takes ahead
 
 // A role's walk through the items its CTA takes, in the order taken: item j
 // of the sequence is read from ring slot j % kItemRing once published, and
@@ -1499,19 +1500,31 @@ __global__ void __launch_bounds__(tcb_warps(BN, NS) * 32, 1) tc_batch_kernel(TcB
     // loads its A blocks; a sentinel ends every role's walk
     if (lane == 0) {
       int blk = 0;
-      // the index of the next item is taken one item ahead, so the atomic's
-      // round trip overlaps the current item's loads
-      unsigned idx = atomicAdd(&args.queue[0], 1u);
+      // the indices of the next kQueueAhead items are taken ahead and the
+      // record of the next one is loaded ahead, so the atomics' and the
+      // load's round trips overlap the current item's loads (a CTA holds at
+      // most kQueueAhead - 1 items it has not started: at the end of the
+      // longest-first queue, short ones)
+      unsigned q[kQueueAhead];
+#pragma unroll
+      for (int i = 0; i < kQueueAhead; ++i) q[i] = atomicAdd(&args.queue[0], 1u);
+      const unsigned nitems = static_cast<unsigned>(args.nitems);
+      TcBatchItem nxt = {kNoItem, 0, 0, 0};
+      if (q[0] < nitems) nxt = args.items[q[0]];
       for (int j = 0;; ++j) {
         const int r = j % kItemRing;
         if (!mbar_wait(&iempty[r], ((j / kItemRing) & 1) ^ 1, args.err, kDevErrEmptyBarrier))
           break;
-        TcBatchItem it = {kNoItem, 0, 0, 0};
-        if (idx < static_cast<unsigned>(args.nitems)) it = args.items[idx];
+        const TcBatchItem it = nxt;
         iring[r] = it;
         mbar_arrive(&ifull[r]);  // release: the slot's item is visible to the waiters
         if (it.prob == kNoItem) break;
-        idx = atomicAdd(&args.queue[0], 1u);
+        // slide the window: one more index taken, the next record loaded
+#pragma unroll
+        for (int i = 0; i + 1 < kQueueAhead; ++i) q[i] = q[i + 1];
+        q[kQueueAhead - 1] = atomicAdd(&args.queue[0], 1u);  // past the end: harmless
+        nxt = {kNoItem, 0, 0, 0};
+        if (q[0] < nitems) nxt = args.items[q[0]];
         const TcBatchProblem &pr = args.probs[it.prob];
         const CUtensorMap *tm = args.tmA + it.prob;
         const int m0 = it.tm * kBM;
@@ -1532,6 +1545,11 @@ __global__ void __launch_bounds__(tcb_warps(BN, NS) * 32, 1) tc_batch_kernel(TcB
         }
         if (!ok) break;
       }
+      // every atomic taken ahead has returned (its register is read) before
+      // this thread's arrival on the finish counter, so the last CTA's reset
+      // of the head comes after all of them
+#pragma unroll
+      for (int i = 0; i < kQueueAhead; ++i) asm volatile("" ::"r"(q[i]));
     }
   } else if (warp == 1) {
     // -------------------------------------------------------- TMA, B

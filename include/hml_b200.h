@@ -438,21 +438,25 @@ hml_status hml_sgemm_v1_config(int M, int N, int K, hml_sgemm_config *config);
  * assignment step of HiperML's k-means (hmlKmeansAssignCtrdSmem,
  * include/hml_kmeans_kernel_template.h:19-90): device pointers, points
  * row-major [num_points][dims], centroids row-major [num_clusters][dims],
- * assignments uint32 [num_points].  Computed as ||c||^2 - 2 x.c with the
- * skinny SGEMM (FP32-accurate configuration) and made exact: every point
- * gets the index the reference kernel gives (its FP32 sums, the first k on
- * ties).  Uses the stream's second workspace (num_points x num_clusters
- * floats).  Stream ordered. */
+ * assignments uint32 [num_points].  Computed as ||c||^2 - 2 x.c, the dot
+ * products a skinny GEMM, and made exact: every point gets the index the
+ * reference kernel gives (its FP32 sums, the first k on ties).  Uses the
+ * stream's second workspace.  Stream ordered. */
 hml_status hml_kmeans_assign(const float *points, int num_points, int dims,
                              const float *centroids, int num_clusters,
                              uint32_t *assignments, void *stream);
 
-/* The same, adding to *exact_count (a device counter) the number of points
- * whose candidates had to be compared with the reference's own arithmetic. */
-hml_status hml_kmeans_assign_stats(const float *points, int num_points,
-                                   int dims, const float *centroids,
-                                   int num_clusters, uint32_t *assignments,
-                                   unsigned *exact_count, void *stream);
+/* The same with the form chosen: method 0 = the library's choice (the tiled
+ * form up to 256 dimensions), 1 = the tiled form (a register-tiled FP32 SIMT
+ * GEMM with the argmin in its epilogue), 2 = the SGEMM form (the products
+ * through HBM, num_points x num_clusters floats of workspace, then a pick
+ * kernel; HML_STATUS_NOT_SUPPORTED above 51200 clusters).  When exact_count
+ * (a device counter) is not NULL, the number of points whose candidates had
+ * to be compared with the reference's own arithmetic is added to it. */
+hml_status hml_kmeans_assign_ex(const float *points, int num_points, int dims,
+                                const float *centroids, int num_clusters,
+                                uint32_t *assignments, int method,
+                                unsigned *exact_count, void *stream);
 
 /* ------------------------------------------------------------ utilities */
 

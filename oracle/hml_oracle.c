@@ -211,7 +211,10 @@ int oracle_sgemm_rm_f32_mt(float *C, const float *A, const float *B, int M,
  * dist = sum over d, in order, of delta * delta with delta = x - c, each step
  * one fused multiply-add (what nvcc makes of `dist += delta * delta`), from
  * 0; the first k whose dist is below the running minimum (from FLT_MAX)
- * wins.  points [n][d], centroids [k][d], row-major. */
+ * wins.  A point none of whose distances is below FLT_MAX (NaN or infinite
+ * ones) gets 0 here; the reference kernel leaves its minK unset for such a
+ * point (:30, :74), so its output there is whatever the register held.
+ * points [n][d], centroids [k][d], row-major. */
 void oracle_kmeans_assign(const float *points, int64_t n, int d, const float *ctrds, int k,
                           uint32_t *out) {
   for (int64_t p = 0; p < n; ++p) {
