@@ -739,9 +739,10 @@ def reference_gpu_entry(ctx, reps=3):
 
 def kmeans_entry(ctx, reps=5):
     """The k-means assignment step (hml_kmeans_assign_ex: the dot products as
-    one skinny GEMM, an exact argmin) in both of its forms -- tiled (the
-    argmin fused into a register-tiled SIMT GEMM) and SGEMM (the products
-    through HBM, then a pick kernel) -- against the reference's own assignment
+    one skinny GEMM, an exact argmin) in each of its forms -- tiled (the
+    argmin fused into a register-tiled SIMT GEMM), SGEMM (the products
+    through HBM, then a pick kernel) and tensor-core (TF32X3 products in
+    TMEM, the argmin read from the accumulator) -- against the reference's own assignment
     kernel hmlKmeansAssignCtrdSmem (oracle/_ref; up to 64 dimensions, as in
     the reference), 1M points, N(0,1), kernel time with CUDA events, and
     whether the index arrays are equal."""
@@ -774,15 +775,18 @@ def kmeans_entry(ctx, reps=5):
         got = torch.empty(n, dtype=torch.int32, device=ctx.dev)
         entry = {"points": n, "dims": d, "clusters": k}
         results = {}
-        for name, method in (("tiled", hml.KMEANS_TILED), ("gemm", hml.KMEANS_GEMM),
-                             ("auto", hml.KMEANS_AUTO)):
+        forms = [("tiled", hml.KMEANS_TILED), ("gemm", hml.KMEANS_GEMM)]
+        if d % 4 == 0 and d <= 64 and k <= 256:
+            forms.append(("tensor", hml.KMEANS_TENSOR))
+        for name, method in forms + [("auto", hml.KMEANS_AUTO)]:
             t = timed(lambda: hml.kmeans_assign(P, C, out=got, stream=ctx.stream, method=method))
             entry[f"{name}_ms"] = t
             results[name] = got.clone()
         t_ours = entry["auto_ms"]
         entry.update({"ours_points_per_s": n / (t_ours * 1e-3),
                       "gemm_tflops": 2.0 * n * d * k / (t_ours * 1e-3) / 1e12,
-                      "forms_equal": bool(torch.equal(results["tiled"], results["gemm"]))})
+                      "forms_equal": all(bool(torch.equal(results[f], results["tiled"]))
+                                         for f, _ in forms)})
         _, exact = hml.kmeans_assign(P, C, count_exact=True)
         entry["points_resolved_exactly"] = exact
         if oracle.ref_gpu_kmeans_available() and d in (4, 8, 16, 32, 64):

@@ -13,6 +13,6 @@ from .api import (  # noqa: F401
     hmlSgemmKernelConfig, hmlSgemv, hmlSgemvBasic, hmlSgemvKernelConfig, select, select_algo, sgemm,
     sgemm_ex, sgemv_ex, autotune, autotune_sgemv, sgemv_select, tune_save, tune_load, tune_clear,
     set_math_mode, MATH_FP32, MATH_FAST, BatchPlan, gemm_descs, sgemm_batched, batch_problem_config,
-    kmeans_assign, KMEANS_AUTO, KMEANS_TILED, KMEANS_GEMM)
+    kmeans_assign, KMEANS_AUTO, KMEANS_TILED, KMEANS_GEMM, KMEANS_TENSOR)
 
 __version__ = lib.hml_version().decode()

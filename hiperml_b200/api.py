@@ -218,7 +218,7 @@ def error_fp64(order, transA, transB, M, N, K, alpha, A, lda, B, ldb, beta, C0, 
     return tuple(err)
 
 
-KMEANS_AUTO, KMEANS_TILED, KMEANS_GEMM = 0, 1, 2
+KMEANS_AUTO, KMEANS_TILED, KMEANS_GEMM, KMEANS_TENSOR = 0, 1, 2, 3
 
 
 def kmeans_assign(points, centroids, out=None, stream=None, count_exact=False,
@@ -229,7 +229,9 @@ def kmeans_assign(points, centroids, out=None, stream=None, count_exact=False,
     bit), and with ``count_exact`` also the number of points whose candidates
     were resolved with the reference's own arithmetic.  ``method``: 0 = the
     library's choice, 1 = the tiled SIMT form with the argmin fused, 2 = the
-    SGEMM form (products through HBM)."""
+    SGEMM form (products through HBM), 3 = the tensor-core form (TF32X3
+    products in TMEM, the argmin read from the accumulator; 4 <= d <= 64 with
+    d a multiple of 4, at most 256 centroids)."""
     import torch
     n, d = points.shape
     k, d2 = centroids.shape

@@ -26,11 +26,14 @@
 // reference's own arithmetic, in increasing k with strict `<`.  So every
 // point gets the reference kernel's index, exact ties included.
 #include <cfloat>
+#include <cstring>
 
 #include "hml_device.cuh"
 #include "hml_internal.h"
 #include "hml_select.h"
 #include "hml_tune.h"
+#include "hml_tcgen05.cuh"
+#include "simt_tile.cuh"
 
 namespace hml {
 namespace {
@@ -41,9 +44,12 @@ constexpr int kNormWarps = 8;
 constexpr int kKmeansTiledMaxDims = 256;
 
 // ||c_k||^2 for every centroid, one warp per centroid (FP32; used only to
-// screen candidates).
-__global__ void centroid_norms_kernel(const float *cent, int k, int d, float *cnorm) {
+// screen candidates).  It runs first in every form, so it also empties the
+// close-call list of the call.
+__global__ void centroid_norms_kernel(const float *cent, int k, int d, float *cnorm,
+                                      unsigned *ccount) {
   const int lane = threadIdx.x & 31;
+  if (blockIdx.x == 0 && threadIdx.x == 0) *ccount = 0u;
   for (int c = blockIdx.x * kNormWarps + (threadIdx.x >> 5); c < k; c += gridDim.x * kNormWarps) {
     const float *row = cent + static_cast<int64_t>(c) * d;
     float s = 0.0f;
@@ -99,13 +105,46 @@ __device__ __noinline__ uint32_t exact_pick(const float *x, int d, const float *
   return bk < 0 ? 0u : static_cast<uint32_t>(bk);
 }
 
+// Close calls (a second smallest g within the bound of the smallest, or
+// non-finite values) are not settled where they are found: the screening
+// kernels append (point, bound) to a list, every lane of a warp calling this
+// together (one atomic per warp), and kmeans_settle_kernel settles the list
+// afterwards, a warp per point -- so a rare long settling never holds up the
+// screening of the other points.
+__device__ __forceinline__ void push_close(unsigned *ccount, uint2 *citems, int64_t p, float lim,
+                                           bool close) {
+  const unsigned m = __ballot_sync(0xffffffffu, close);
+  if (!m) return;
+  const int lane = threadIdx.x & 31, leader = __ffs(m) - 1;
+  unsigned base = 0;
+  if (lane == leader) base = atomicAdd(ccount, static_cast<unsigned>(__popc(m)));
+  base = __shfl_sync(0xffffffffu, base, leader);
+  if (close)
+    citems[base + __popc(m & ((1u << lane) - 1u))] =
+        make_uint2(static_cast<uint32_t>(p), __float_as_uint(lim));
+}
+
+__global__ void kmeans_settle_kernel(const float *points, int d, const float *cent, int k,
+                                     const float *cnorm, const unsigned *ccount,
+                                     const uint2 *citems, uint32_t *out, unsigned *exact) {
+  const unsigned n = *ccount;
+  if (exact && n && blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(exact, n);
+  const int lane = threadIdx.x & 31;
+  const unsigned warps = (gridDim.x * blockDim.x) >> 5;
+  for (unsigned w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; w < n; w += warps) {
+    const uint2 it = citems[w];
+    const uint32_t pick = exact_pick<32>(points + static_cast<int64_t>(it.x) * d, d, cent, k,
+                                         cnorm, __uint_as_float(it.y), 0xffffffffu, lane);
+    if (lane == 0) out[it.x] = pick;
+  }
+}
+
 // One thread per point: g_k = ||c_k||^2 - 2 S(p, k) (S column-major, ld lds),
-// the candidates within `margin` of the smallest, and, when there is more
-// than one, the reference's own pick among them.  `exact` counts the points
-// that needed it.
-__global__ void kmeans_pick_kernel(const float *points, int64_t np, int d, const float *cent,
-                                   int k, const float *S, int64_t lds, const float *cnorm,
-                                   uint32_t *out, unsigned *exact) {
+// the candidates within `margin` of the smallest; a point with more than
+// one goes to the close-call list.
+__global__ void kmeans_pick_kernel(const float *points, int64_t np, int d, int k, const float *S,
+                                   int64_t lds, const float *cnorm, uint32_t *out,
+                                   unsigned *ccount, uint2 *citems) {
   extern __shared__ float s_cnorm[];  // [k], then the block's max
   float cmax = 0.0f;
   for (int c = threadIdx.x; c < k; c += blockDim.x) {
@@ -126,10 +165,9 @@ __global__ void kmeans_pick_kernel(const float *points, int64_t np, int d, const
   // 16 gamma_{d+4}, rounded up (gamma_n = n u / (1 - n u), u = 2^-24)
   const double nu = (d + 4) * 0x1p-24;
   const float bound = static_cast<float>(16.0 * nu / (1.0 - nu) * 1.001);
-  unsigned my_exact = 0;
   const int lane = threadIdx.x & 31;
   // the warp walks 32 consecutive points at a time (every lane takes every
-  // step, so the warp can settle its close calls together)
+  // step, so the warp can list its close calls together)
   const int64_t wstride = static_cast<int64_t>(gridDim.x) * blockDim.x;
   for (int64_t p0 = blockIdx.x * static_cast<int64_t>(blockDim.x) + (threadIdx.x & ~31); p0 < np;
        p0 += wstride) {
@@ -157,21 +195,8 @@ __global__ void kmeans_pick_kernel(const float *points, int64_t np, int d, const
       close = cand != 1;
       if (!close) out[p] = static_cast<uint32_t>(kmin);
     }
-    // close calls (or non-finite values): the warp settles each with the
-    // reference's own arithmetic over the candidates
-    unsigned todo = __ballot_sync(0xffffffffu, close);
-    my_exact += __popc(todo) * (lane == 0);
-    while (todo) {
-      const int src = __ffs(todo) - 1;
-      todo &= todo - 1;
-      const int64_t q = p0 + src;
-      const float ql = __shfl_sync(0xffffffffu, lim, src);
-      const uint32_t pick = exact_pick<32>(points + q * d, d, cent, k, cnorm, ql, 0xffffffffu,
-                                           lane);
-      if (lane == 0) out[q] = pick;
-    }
+    push_close(ccount, citems, p, lim, close);
   }
-  if (exact && my_exact) atomicAdd(exact, my_exact);
 }
 
 // The tiled form: the dot products of 128 points with 64 centroids at a
@@ -220,9 +245,68 @@ __device__ __forceinline__ Best best_merge(const Best &a, const Best &b) {
   return {a.g1, a.k1, fminf(a.g2, b.g1)};
 }
 
+__device__ __forceinline__ Best shfl_best(unsigned mask, const Best &b, int o) {
+  return {__shfl_xor_sync(mask, b.g1, o), __shfl_xor_sync(mask, b.k1, o),
+          __shfl_xor_sync(mask, b.g2, o)};
+}
+
+// End of a tile for the 16 lanes of a point group (one half-warp, lane tx):
+// their states for the group's 8 points (thread-local point i = tile row
+// ty*4+i for i < 4, 64+ty*4+i-4 otherwise) are merged by a reduce-scatter --
+// at offsets 8, 4 and 2 a lane keeps half of the points it carries, merged
+// with its partner's half, and at offset 1 the pair merges its one point --
+// so lanes tx and tx^1 end with point 4*bit3 + 2*bit2 + bit1 of tx merged
+// over all 16.  The even lane writes a settled point or lists a close call
+// (all 32 lanes of the warp call this together).
+__device__ __forceinline__ void settle_group(Best (&best)[8], int64_t p0, int nb, int ty, int tx,
+                                             const float *s_xn, float cmax, float bound,
+                                             uint32_t *out, unsigned *ccount, uint2 *citems) {
+  const unsigned hmask = 0xFFFFu << (threadIdx.x & 16);
+  Best b4[4];
+  {
+    const bool up = tx & 8;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const Best keep = up ? best[4 + i] : best[i];
+      const Best send = up ? best[i] : best[4 + i];
+      b4[i] = best_merge(keep, shfl_best(hmask, send, 8));
+    }
+  }
+  Best b2[2];
+  {
+    const bool up = tx & 4;
+#pragma unroll
+    for (int i = 0; i < 2; ++i) {
+      const Best keep = up ? b4[2 + i] : b4[i];
+      const Best send = up ? b4[i] : b4[2 + i];
+      b2[i] = best_merge(keep, shfl_best(hmask, send, 4));
+    }
+  }
+  Best b;
+  {
+    const bool up = tx & 2;
+    const Best keep = up ? b2[1] : b2[0];
+    const Best send = up ? b2[0] : b2[1];
+    b = best_merge(keep, shfl_best(hmask, send, 2));
+  }
+  b = best_merge(b, shfl_best(hmask, b, 1));
+  const int i = ((tx >> 3) & 1) * 4 + ((tx >> 2) & 1) * 2 + ((tx >> 1) & 1);
+  const int pt = i < 4 ? ty * 4 + i : 64 + ty * 4 + (i - 4);
+  const bool mine = (tx & 1) == 0 && pt < nb;
+  float lim = 0.0f;
+  bool close = false;
+  if (mine) {
+    lim = b.g1 + bound * (s_xn[pt] + cmax) + 1e-37f;
+    close = !(b.g2 > lim);
+    if (!close) out[p0 + pt] = static_cast<uint32_t>(b.k1);
+  }
+  push_close(ccount, citems, p0 + pt, lim, close);
+}
+
 __global__ void __launch_bounds__(kTThreads, 2) kmeans_tile_kernel(
     const float *__restrict__ points, int np, int d, const float *__restrict__ cent, int k,
-    const float *__restrict__ cnorm, uint32_t *__restrict__ out, unsigned *exact) {
+    const float *__restrict__ cnorm, uint32_t *__restrict__ out, unsigned *ccount,
+    uint2 *citems) {
   __shared__ __align__(16) float xs[kTD][kXS];
   __shared__ __align__(16) float cs[kTD][kCS];
   __shared__ float s_cn[kTC];
@@ -311,62 +395,501 @@ __global__ void __launch_bounds__(kTThreads, 2) kmeans_tile_kernel(
   const double nu = (d + 4) * 0x1p-24;
   const float bound = static_cast<float>(16.0 * nu / (1.0 - nu) * 1.001);
 
-  // merge over the 16 threads of each point group (lanes of one half-warp)
-#pragma unroll
-  for (int i = 0; i < 8; ++i) {
-#pragma unroll
-    for (int o = 1; o < 16; o <<= 1) {
-      const Best other = {__shfl_xor_sync(0xffffffffu, best[i].g1, o),
-                          __shfl_xor_sync(0xffffffffu, best[i].k1, o),
-                          __shfl_xor_sync(0xffffffffu, best[i].g2, o)};
-      best[i] = best_merge(best[i], other);
+  settle_group(best, p0, nb, ty, tx, s_xn, cmax, bound, out, ccount, citems);
+}
+
+// The resident form of the tiled kernel, for centroids that fit in shared
+// memory (k and dims padded to kp = 64-multiple and dp = 4-multiple, dp <= 64
+// and kp * dp <= kResidentFloats, so two blocks fit on an SM): each block
+// stages the transposed centroids and their norms once and then walks
+// 128-point tiles (a persistent grid), the next
+// tile's rows copied by cp.async into the other of two row-major buffers
+// while the current tile is computed, so the loads' latency hides behind the
+// arithmetic.  A thread's 8 points are read as 16-byte row pieces (4
+// dimensions each), the centroids as 16-byte pieces of a dimension row; the
+// products, the running argmin, the merge and the settling of close calls
+// are the tiled kernel's.
+constexpr int kResidentFloats = 8192;
+
+__global__ void __launch_bounds__(kTThreads, 2) kmeans_resident_kernel(
+    const float *__restrict__ points, int np, int d, int dp, bool vec,
+    const float *__restrict__ cent, int k, int kp, const float *__restrict__ cnorm,
+    uint32_t *__restrict__ out, unsigned *ccount, uint2 *citems) {
+  extern __shared__ __align__(16) float sm[];
+  const int cst = kp + 4;                   // row stride of the transposed centroids
+  float *ct = sm;                           // [dp][cst]
+  float *cn = ct + dp * cst;                // [kp]
+  float *xr = cn + kp;                      // [2][kTP][dp]
+  float *s_xn = xr + 2 * kTP * dp;          // [kTP]
+  __shared__ float s_wmax[kTThreads / 32];
+  const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
+  const int64_t tiles = (static_cast<int64_t>(np) + kTP - 1) / kTP;
+
+  // the next tile's rows into buffer `buf` (zero past d and past np when
+  // copied element-wise)
+  auto issue = [&](int64_t t, int buf) {
+    const int64_t p0 = t * kTP;
+    const int nbt = static_cast<int>(min(static_cast<int64_t>(kTP), np - p0));
+    float *dst = xr + buf * kTP * dp;
+    if (vec) {
+      const int q = dp / 4;
+      for (int e = tid; e < nbt * q; e += kTThreads) {
+        const int pt = e / q, c4 = e - pt * q;
+        cp_async16(smem_u32(dst + pt * dp + c4 * 4), points + (p0 + pt) * d + c4 * 4, 16);
+      }
+    } else {
+      for (int e = tid; e < kTP * dp; e += kTThreads) {
+        const int pt = e / dp, j = e - pt * dp;
+        const bool v = pt < nbt && j < d;
+        cp_async4(smem_u32(dst + e), v ? points + (p0 + pt) * d + j : points, v);
+      }
     }
+    cp_async_commit();
+  };
+  int64_t t = blockIdx.x;
+  if (t < tiles) issue(t, 0);
+
+  // centroids (transposed, zero padded) and norms (NaN past k: never taken)
+  for (int e = tid; e < dp * kp; e += kTThreads) {
+    const int j = e / kp, c = e - j * kp;
+    ct[j * cst + c] = (c < k && j < d) ? cent[static_cast<int64_t>(c) * d + j] : 0.0f;
   }
-  // the group's 8 points: a settled one is written by lane tx == i; a close
-  // call (or non-finite values) is settled by the 16 lanes together with the
-  // reference's own arithmetic over the candidates
-  const unsigned hmask = 0xFFFFu << (threadIdx.x & 16);
+  float cmax = 0.0f;
+  for (int c = tid; c < kp; c += kTThreads) {
+    const float v = c < k ? cnorm[c] : __int_as_float(0x7fc00000);
+    cn[c] = v;
+    if (c < k) cmax = fmaxf(cmax, v);
+  }
 #pragma unroll
-  for (int i = 0; i < 8; ++i) {
-    const int pt = i < 4 ? ty * 4 + i : 64 + ty * 4 + (i - 4);
-    if (pt >= nb) continue;  // the same for the whole half-warp
-    const int64_t p = p0 + pt;
-    const float lim = best[i].g1 + bound * (s_xn[pt] + cmax) + 1e-37f;
-    if (best[i].g2 > lim) {
-      if (tx == i) out[p] = static_cast<uint32_t>(best[i].k1);
-      continue;
+  for (int o = 16; o > 0; o >>= 1) cmax = fmaxf(cmax, __shfl_xor_sync(0xffffffffu, cmax, o));
+  if ((tid & 31) == 0) s_wmax[tid >> 5] = cmax;
+  __syncthreads();
+  cmax = 0.0f;
+#pragma unroll
+  for (int w = 0; w < kTThreads / 32; ++w) cmax = fmaxf(cmax, s_wmax[w]);
+  const double nu = (d + 4) * 0x1p-24;
+  const float bound = static_cast<float>(16.0 * nu / (1.0 - nu) * 1.001);
+
+  for (int buf = 0; t < tiles; t += gridDim.x, buf ^= 1) {
+    const int64_t tn = t + gridDim.x;
+    if (tn < tiles) {
+      issue(tn, buf ^ 1);
+      asm volatile("cp.async.wait_group 1;" ::: "memory");
+    } else {
+      asm volatile("cp.async.wait_group 0;" ::: "memory");
     }
-    if (tx == 0 && exact) atomicAdd(exact, 1u);
-    const uint32_t pick = exact_pick<16>(points + p * d, d, cent, k, cnorm, lim, hmask, tx);
-    if (tx == 0) out[p] = pick;
+    __syncthreads();  // this tile's rows are in place
+    const float *x = xr + buf * kTP * dp;
+    const int64_t p0 = t * kTP;
+    const int nb = static_cast<int>(min(static_cast<int64_t>(kTP), np - p0));
+    if (tid < kTP) {
+      // ||x||^2 for the bound (the row's 16-byte pieces in a rotated order,
+      // so that the lanes of a warp read different banks)
+      const int q = dp / 4;
+      float xn = 0.0f;
+      for (int i = 0; i < q; ++i) {
+        const float4 v = lds128(x + tid * dp + ((i + tid) % q) * 4);
+        xn = fmaf(v.x, v.x, xn);
+        xn = fmaf(v.y, v.y, xn);
+        xn = fmaf(v.z, v.z, xn);
+        xn = fmaf(v.w, v.w, xn);
+      }
+      s_xn[tid] = xn;
+    }
+    Best best[8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) best[i] = {INFINITY, 0, INFINITY};
+    const float *xa = x + (ty * 4) * dp, *xb = x + (64 + ty * 4) * dp;
+    for (int c0 = 0; c0 < kp; c0 += kTC) {
+      float acc[8][4];
+#pragma unroll
+      for (int i = 0; i < 8; ++i)
+#pragma unroll
+        for (int q = 0; q < 4; ++q) acc[i][q] = 0.0f;
+      const float *cc = ct + c0 + tx * 4;
+      for (int j0 = 0; j0 < dp; j0 += 4) {
+        float4 xv[8];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+          xv[i] = lds128(xa + i * dp + j0);
+          xv[4 + i] = lds128(xb + i * dp + j0);
+        }
+#pragma unroll
+        for (int jj = 0; jj < 4; ++jj) {
+          const float4 cv = lds128(cc + (j0 + jj) * cst);
+          const float cw[4] = {cv.x, cv.y, cv.z, cv.w};
+#pragma unroll
+          for (int i = 0; i < 8; ++i) {
+            const float xi = jj == 0 ? xv[i].x : jj == 1 ? xv[i].y : jj == 2 ? xv[i].z : xv[i].w;
+#pragma unroll
+            for (int q = 0; q < 4; ++q) acc[i][q] = fmaf(xi, cw[q], acc[i][q]);
+          }
+        }
+      }
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const int c = tx * 4 + q;
+        const float cnv = cn[c0 + c];
+#pragma unroll
+        for (int i = 0; i < 8; ++i) best_add(best[i], fmaf(-2.0f, acc[i][q], cnv), c0 + c);
+      }
+    }
+    __syncthreads();  // s_xn is complete
+    settle_group(best, p0, nb, ty, tx, s_xn, cmax, bound, out, ccount, citems);
+    __syncthreads();  // the buffer and s_xn are free for the tile after next
   }
 }
 
-hml_status launch_norms(const float *cent, int k, int d, float *cnorm, cudaStream_t s) {
+// ------------------------------------------------ the tensor-core form
+// (method 3)  The dot products of a 128-point tile with all (up to 256)
+// centroids as TF32X3 products on the tensor cores: x = xh + xl and
+// c = ch + cl with xh = tf32(x), xl = tf32(x - xh) (22 significant bits
+// together), and x.c ~ xh.ch + xh.cl + xl.ch accumulated in FP32 in TMEM.
+// One CTA per SM walks the tiles of a persistent grid:
+//   * warp 0, one lane: TMA of the centroids' TF32 planes (split once by
+//     kmeans_tf32_planes_kernel, K-contiguous), resident in shared memory
+//     in the UMMA K-major layout (128-byte swizzle), then of each point tile
+//     (128 rows x 32 dimensions a box, 128-byte swizzle) into a ring;
+//   * W warpgroups take the CTA's tiles round-robin.  Thread m of a group
+//     owns point m of the tile, which is TMEM lane m: it reads the point's
+//     row, forms ||x||^2 (for the bound) and the TF32 planes, writes them
+//     into the group's TMEM A region with tcgen05.st; one elected thread
+//     then issues the group's tcgen05.mma chain (A in TMEM, B from shared
+//     memory, N = the padded number of centroids) into the group's TMEM
+//     accumulator and commits it to the group's mbarrier; the group reads
+//     its rows back with tcgen05.ld and takes the argmin of g_k =
+//     ||c_k||^2 - 2 x.c_k in increasing k -- the whole row of a point in
+//     one thread, so no merge.  W groups keep W tiles in flight, W issuing
+//     threads in parallel (one thread issues a tcgen05.mma only every ~130
+//     cycles).
+// Close calls go to the close-call list, the margin being twice the SIMT
+// forms' (32 gamma_{dims+4}), as the
+// products' error is up to about four times a direct FP32 sum's (the split
+// leaves 2^-22 per operand; the tensor core's accumulation truncates).
+constexpr int kTcMaxD = 64;    // dimensions (padded to 32)
+constexpr int kTcMaxK = 256;   // centroids (padded to 32): one MMA's N
+constexpr int kTcBox = kTP * 32 * 4;  // bytes of one 128 x 32 FP32 box
+
+struct KmTcArgs {
+  int np, d, k, dp, kp, sa;
+  const float *cnorm;
+  uint32_t *out;
+  unsigned *ccount;
+  uint2 *citems;
+  int *err;
+};
+
+// TF32 hi and lo planes of the centroids: planes[p][c][j] (j contiguous, zero
+// padded to kp x dp), hi = TF32(x), lo = TF32(x - hi) (the residual exact).
+__global__ void kmeans_tf32_planes_kernel(const float *cent, int k, int d, int kp, int dp,
+                                          uint32_t *planes) {
+  const int n = kp * dp;
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += gridDim.x * blockDim.x) {
+    const int c = e / dp, j = e - c * dp;
+    const float v = (c < k && j < d) ? cent[static_cast<int64_t>(c) * d + j] : 0.0f;
+    const uint32_t hi = tf32_rna(v);
+    planes[e] = hi;
+    planes[n + e] = tf32_rna(__fsub_rn(v, __uint_as_float(hi)));
+  }
+}
+
+// OR of `v` over the 128 threads of a warpgroup (named barrier `id`).
+__device__ __forceinline__ bool group_any(bool v, int id) {
+  uint32_t r;
+  asm volatile(
+      "{\n\t.reg .pred p, q;\n\t"
+      "setp.ne.u32 p, %1, 0;\n\t"
+      "barrier.cta.red.or.pred q, %2, 128, p;\n\t"
+      "selp.u32 %0, 1, 0, q;\n\t}"
+      : "=r"(r)
+      : "r"(static_cast<uint32_t>(v)), "r"(id)
+      : "memory");
+  return r != 0;
+}
+
+__device__ __forceinline__ void group_sync(int id) {
+  asm volatile("barrier.cta.sync.aligned %0, 128;" ::"r"(id) : "memory");
+}
+
+__host__ __device__ constexpr int km_tc_threads(int w) { return (4 + 4 * w) * 32; }
+
+template <int W>
+__global__ void __launch_bounds__(km_tc_threads(W), 1)
+    kmeans_tc_kernel(const __grid_constant__ CUtensorMap tmX,
+                     const __grid_constant__ CUtensorMap tmB, const __grid_constant__ KmTcArgs a) {
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t *smem = reinterpret_cast<uint8_t *>(
+      (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~static_cast<uintptr_t>(1023));
+  const int dp = a.dp, kp = a.kp, nkb = dp / 32, SA = a.sa;
+  const int slot = nkb * kTcBox;   // bytes of one point tile
+  const int btile = kp * 128;      // bytes of one (plane, 32-dim block) of the centroids
+  uint8_t *xring = smem;                                  // [SA][nkb][128 x 128 B]
+  uint8_t *bsm = xring + SA * slot;                       // [2][nkb][kp x 128 B]
+  float *cn = reinterpret_cast<float *>(bsm + 2 * nkb * btile);  // [kp]
+  uint64_t *afull = reinterpret_cast<uint64_t *>(cn + kp);
+  uint64_t *aempty = afull + SA;
+  uint64_t *accfull = aempty + SA;  // [W]
+  uint64_t *bfull = accfull + W;
+  uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(bfull + 1);
+  float *s_cmax = reinterpret_cast<float *>(tmem_slot + 1);
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int64_t tiles = (static_cast<int64_t>(a.np) + kTP - 1) / kTP;
+  const int my_tiles = static_cast<int>((tiles - blockIdx.x + gridDim.x - 1) / gridDim.x);
+
+  if (threadIdx.x == 0) {
+    for (int i = 0; i < SA; ++i) {
+      mbar_init(&afull[i], 1);
+      mbar_init(&aempty[i], 4);  // the 4 warps of the group that read the tile
+    }
+    for (int g = 0; g < W; ++g) mbar_init(&accfull[g], 1);
+    mbar_init(bfull, 1);
+    fence_mbar_init();
+    prefetch_tmap(&tmX);
+    prefetch_tmap(&tmB);
+  }
+  if (warp == 1) {
+    // ||c||^2 (+inf past k: never taken, and never the second smallest) and
+    // its maximum over the centroids
+    float cmax = 0.0f;
+    for (int c = lane; c < kp; c += 32) {
+      const float v = c < a.k ? a.cnorm[c] : INFINITY;
+      cn[c] = v;
+      if (c < a.k) cmax = fmaxf(cmax, v);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) cmax = fmaxf(cmax, __shfl_xor_sync(0xffffffffu, cmax, o));
+    if (lane == 0) *s_cmax = cmax;
+  }
+  if (warp == 2) tmem_alloc(tmem_slot, 512);
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tmem_slot;
+
+  if (warp == 0) {
+    // ------------------------------------------------------------ TMA
+    if (lane == 0) {
+      mbar_arrive_expect_tx(bfull, 2 * nkb * btile);
+      for (int pl = 0; pl < 2; ++pl)
+        for (int kb = 0; kb < nkb; ++kb)
+          tma_load_2d(bsm + (pl * nkb + kb) * btile, &tmB, bfull, kb * 32, pl * kp);
+      int j = 0;
+      for (; j < my_tiles; ++j) {
+        const int st = j % SA;
+        if (j >= SA && !mbar_wait(&aempty[st], ((j / SA) - 1) & 1, a.err, kDevErrEmptyBarrier))
+          break;
+        const int64_t t = blockIdx.x + static_cast<int64_t>(j) * gridDim.x;
+        mbar_arrive_expect_tx(&afull[st], slot);
+        for (int kb = 0; kb < nkb; ++kb)
+          tma_load_2d(xring + st * slot + kb * kTcBox, &tmX, &afull[st], kb * 32,
+                      static_cast<int>(t * kTP));
+      }
+      // every load issued has landed before the CTA may exit
+      for (int i = max(0, j - SA); i < j; ++i)
+        mbar_wait(&afull[i % SA], (i / SA) & 1, a.err, kDevErrFullBarrier);
+      mbar_wait(bfull, 0, a.err, kDevErrFullBarrier);
+    }
+  } else if (warp >= 4) {
+    // ------------------------------------------------- point groups
+    const int g = (warp - 4) >> 2, bar_id = 1 + g;
+    const int m = (warp & 3) * 32 + lane;  // tile row == TMEM lane
+    const uint32_t lanes = static_cast<uint32_t>((warp & 3) * 32) << 16;
+    const uint32_t tacc = tmem + static_cast<uint32_t>(g * (kp + 2 * dp));
+    const uint32_t tA = tacc + static_cast<uint32_t>(kp);  // hi plane dp columns, then lo
+    const bool issuer = warp == 4 + 4 * g && lane == 0;
+    const float cmax = *s_cmax;
+    const double nu = (a.d + 4) * 0x1p-24;
+    const float bound = static_cast<float>(32.0 * nu / (1.0 - nu) * 1.001);
+    const uint32_t idesc = idesc_tf32(kp);
+    int it = 0;
+    for (int j = g; j < my_tiles; j += W, ++it) {
+      const int st = j % SA;
+      const bool w = mbar_wait(&afull[st], (j / SA) & 1, a.err, kDevErrFullBarrier);
+      if (group_any(!w, bar_id)) break;
+      __syncwarp();  // tcgen05.st is warp-collective
+      // the point's row: ||x||^2 in dimension order, then its TF32 planes
+      const float *xs = reinterpret_cast<const float *>(xring + st * slot);
+      float xn = 0.0f;
+      for (int kb = 0; kb < nkb; ++kb) {
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          float x[16];
+#pragma unroll
+          for (int c = 0; c < 4; ++c) {
+            const float4 v = *reinterpret_cast<const float4 *>(
+                xs + kb * (kTcBox / 4) + m * 32 + (((4 * h + c) ^ (m & 7)) * 4));
+            x[4 * c] = v.x;
+            x[4 * c + 1] = v.y;
+            x[4 * c + 2] = v.z;
+            x[4 * c + 3] = v.w;
+          }
+          uint32_t hi[16], lo[16];
+#pragma unroll
+          for (int i = 0; i < 16; ++i) {
+            xn = fmaf(x[i], x[i], xn);
+            hi[i] = tf32_rna(x[i]);
+            lo[i] = tf32_rna(__fsub_rn(x[i], __uint_as_float(hi[i])));
+          }
+          const uint32_t col = static_cast<uint32_t>(kb * 32 + h * 16);
+          tmem_st16(tA + lanes + col, hi);
+          tmem_st16(tA + lanes + static_cast<uint32_t>(dp) + col, lo);
+        }
+      }
+      // the slot is consumed (every value above was used before this point)
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&aempty[st]);
+      __syncwarp();
+      tmem_wait_st();
+      tc_fence_before();
+      group_sync(bar_id);
+      if (issuer) {
+        tc_fence_after();
+        bool bok = true;
+        if (it == 0) bok = mbar_wait(bfull, 0, a.err, kDevErrFullBarrier);
+        if (bok) {
+          // products hh, hl, lh of every 8-deep step of every 32-dim block
+          for (int kb = 0; kb < nkb; ++kb)
+#pragma unroll
+            for (int kk = 0; kk < 4; ++kk)
+#pragma unroll
+              for (int pr = 0; pr < 3; ++pr) {
+                const int ia = pr == 2 ? 1 : 0, jb = pr == 1 ? 1 : 0;
+                const uint32_t at = tA + static_cast<uint32_t>(ia * dp + kb * 32 + kk * 8);
+                const uint64_t bd =
+                    sw128_desc(smem_u32(bsm + (jb * nkb + kb) * btile)) +
+                    static_cast<uint64_t>((kk * 32) >> 4);
+                mma_tf32_ts(tacc, at, bd, idesc, (kb | kk | pr) != 0 ? 1u : 0u);
+              }
+        }
+        mma_commit(&accfull[g]);  // arrives once the group's MMAs are done
+      }
+      const bool w2 = mbar_wait(&accfull[g], it & 1, a.err, kDevErrMmaBarrier);
+      if (group_any(!w2, bar_id)) break;
+      __syncwarp();  // tcgen05.ld is warp-collective
+      tc_fence_after();
+      // argmin of g_k over the point's row of the accumulator, without
+      // branches: g1 the smallest, k1 the first index reaching it, g2 the
+      // second smallest of the multiset (equal to g1 on a tie; a NaN g makes
+      // it g1 too, which only sends the point to the close-call list)
+      float g1 = INFINITY, g2 = INFINITY;
+      int k1 = 0;
+      for (int c0 = 0; c0 < kp; c0 += 16) {
+        uint32_t r[16];
+        tmem_ld16(tacc + lanes + static_cast<uint32_t>(c0), r);
+        float cv[16];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          const float4 v = *reinterpret_cast<const float4 *>(cn + c0 + 4 * q);
+          cv[4 * q] = v.x;
+          cv[4 * q + 1] = v.y;
+          cv[4 * q + 2] = v.z;
+          cv[4 * q + 3] = v.w;
+        }
+        tmem_wait_ld();
+#pragma unroll
+        for (int i = 0; i < 16; ++i) {
+          const float gv = fmaf(-2.0f, __uint_as_float(r[i]), cv[i]);
+          k1 = gv < g1 ? c0 + i : k1;
+          g2 = fminf(g2, fmaxf(g1, gv));
+          g1 = fminf(g1, gv);
+        }
+      }
+      tc_fence_before();  // the reads are done before the next tile's MMAs
+      const int64_t t = blockIdx.x + static_cast<int64_t>(j) * gridDim.x;
+      const int64_t p = t * kTP + m;
+      const bool live = p < a.np;
+      const float lim = g1 + bound * (xn + cmax) + 1e-37f;
+      const bool close = live && !(g2 > lim);
+      if (live && !close) a.out[p] = static_cast<uint32_t>(k1);
+      push_close(a.ccount, a.citems, p, lim, close);
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 2) {
+    tc_fence_after();
+    tmem_dealloc(tmem, 512);
+  }
+}
+
+// The call's workspace (the stream's second slot): `extra` bytes for the
+// form (the products or the centroid planes), ||c||^2, and the close-call
+// list (a count, then room for every point).
+struct KmWs {
+  uint8_t *extra;
+  float *cnorm;
+  unsigned *ccount;
+  uint2 *citems;
+};
+
+hml_status km_workspace(size_t extra, int np, int k, cudaStream_t s, KmWs *w) {
+  auto up = [](size_t b) { return (b + 255) & ~static_cast<size_t>(255); };
+  const size_t o_norm = up(extra), o_cnt = o_norm + up(static_cast<size_t>(k) * sizeof(float));
+  const size_t o_items = o_cnt + 256;
+  void *ws = nullptr;
+  hml_status st = workspace_slot(1, o_items + static_cast<size_t>(np) * sizeof(uint2), s, &ws);
+  if (st != HML_STATUS_SUCCESS) return st;
+  uint8_t *b = static_cast<uint8_t *>(ws);
+  w->extra = b;
+  w->cnorm = reinterpret_cast<float *>(b + o_norm);
+  w->ccount = reinterpret_cast<unsigned *>(b + o_cnt);
+  w->citems = reinterpret_cast<uint2 *>(b + o_items);
+  return HML_STATUS_SUCCESS;
+}
+
+// ||c||^2 and an empty close-call list; first in every form.
+hml_status launch_norms(const float *cent, int k, int d, const KmWs &w, cudaStream_t s) {
   count_launch();
   const int nb = std::min((k + kNormWarps - 1) / kNormWarps, 4 * sm_count());
-  centroid_norms_kernel<<<std::max(1, nb), 32 * kNormWarps, 0, s>>>(cent, k, d, cnorm);
+  centroid_norms_kernel<<<std::max(1, nb), 32 * kNormWarps, 0, s>>>(cent, k, d, w.cnorm,
+                                                                     w.ccount);
   cudaError_t e = cudaGetLastError();
   note_cuda_error(e, "kmeans norms");
+  return cuda_status(e);
+}
+
+// The close calls the screening kernel listed; last in every form.
+hml_status launch_settle(const float *points, int d, const float *cent, int k, const KmWs &w,
+                         uint32_t *out, unsigned *exact, cudaStream_t s) {
+  count_launch();
+  kmeans_settle_kernel<<<2 * sm_count(), 256, 0, s>>>(points, d, cent, k, w.cnorm, w.ccount,
+                                                      w.citems, out, exact);
+  cudaError_t e = cudaGetLastError();
+  note_cuda_error(e, "kmeans settle");
   return cuda_status(e);
 }
 
 // The tiled SIMT form (method 1).
 hml_status assign_tiled(const float *points, int np, int d, const float *cent, int k,
                         uint32_t *out, unsigned *exact, cudaStream_t s) {
-  void *ws = nullptr;
-  hml_status st = workspace_slot(1, static_cast<size_t>(k) * sizeof(float), s, &ws);
-  if (st != HML_STATUS_SUCCESS) return st;
-  float *cnorm = static_cast<float *>(ws);
-  st = launch_norms(cent, k, d, cnorm, s);
+  KmWs w;
+  hml_status st = km_workspace(0, np, k, s, &w);
+  if (st == HML_STATUS_SUCCESS) st = launch_norms(cent, k, d, w, s);
   if (st != HML_STATUS_SUCCESS) return st;
   const int64_t blocks = (static_cast<int64_t>(np) + kTP - 1) / kTP;
+  const int dp = (d + 3) & ~3, kp = (k + kTC - 1) / kTC * kTC;
+  cudaError_t e = cudaSuccess;
   count_launch();
-  kmeans_tile_kernel<<<static_cast<unsigned>(blocks), kTThreads, 0, s>>>(points, np, d, cent, k,
-                                                                        cnorm, out, exact);
-  cudaError_t e = cudaGetLastError();
+  if (d > 0 && dp <= 64 && static_cast<int64_t>(dp) * kp <= kResidentFloats) {
+    const size_t smem =
+        (static_cast<size_t>(dp) * (kp + 4) + kp + 2 * kTP * dp + kTP) * sizeof(float);
+    e = cudaFuncSetAttribute(kmeans_resident_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             static_cast<int>(smem));
+    // 16-byte row copies when every row starts on a 16-byte boundary
+    const bool vec = d % 4 == 0 && (reinterpret_cast<uintptr_t>(points) & 15u) == 0;
+    const int64_t grid = std::min<int64_t>(blocks, 2LL * sm_count());
+    if (e == cudaSuccess)
+      kmeans_resident_kernel<<<static_cast<unsigned>(grid), kTThreads, smem, s>>>(
+          points, np, d, dp, vec, cent, k, kp, w.cnorm, out, w.ccount, w.citems);
+  } else {
+    kmeans_tile_kernel<<<static_cast<unsigned>(blocks), kTThreads, 0, s>>>(
+        points, np, d, cent, k, w.cnorm, out, w.ccount, w.citems);
+  }
+  if (e == cudaSuccess) e = cudaGetLastError();
   note_cuda_error(e, "kmeans tiled");
-  return cuda_status(e);
+  if (e != cudaSuccess) return cuda_status(e);
+  return launch_settle(points, d, cent, k, w, out, exact, s);
 }
 
 // The GEMM form (method 2): S = X C^T through the library's SGEMM, then the
@@ -374,12 +897,10 @@ hml_status assign_tiled(const float *points, int np, int d, const float *cent, i
 hml_status assign_gemm(const float *points, int np, int d, const float *cent, int k,
                        uint32_t *out, unsigned *exact, cudaStream_t s) {
   const size_t s_bytes = static_cast<size_t>(np) * k * sizeof(float);
-  const size_t n_off = (s_bytes + 255) & ~static_cast<size_t>(255);
-  void *ws = nullptr;
-  hml_status st = workspace_slot(1, n_off + static_cast<size_t>(k) * sizeof(float), s, &ws);
+  KmWs w;
+  hml_status st = km_workspace(s_bytes, np, k, s, &w);
   if (st != HML_STATUS_SUCCESS) return st;
-  float *S = static_cast<float *>(ws);
-  float *cnorm = reinterpret_cast<float *>(static_cast<uint8_t *>(ws) + n_off);
+  float *S = reinterpret_cast<float *>(w.extra);
   // S (points x clusters, column-major) = X C^T: X is the row-major points
   // (column-major d x np, transposed), C^T the row-major centroids
   // (column-major d x k)
@@ -409,7 +930,7 @@ hml_status assign_gemm(const float *points, int np, int d, const float *cent, in
       return HML_STATUS_CUDA_ERROR;
     }
   }
-  st = launch_norms(cent, k, d, cnorm, s);
+  st = launch_norms(cent, k, d, w, s);
   if (st != HML_STATUS_SUCCESS) return st;
   count_launch();
   cudaError_t e = cudaSuccess;
@@ -421,27 +942,115 @@ hml_status assign_gemm(const float *points, int np, int d, const float *cent, in
   if (e == cudaSuccess) {
     const int64_t blocks = std::min<int64_t>((np + 255) / 256, 8LL * sm_count());
     kmeans_pick_kernel<<<static_cast<unsigned>(blocks), 256, smem, s>>>(
-        points, np, d, cent, k, S, np, cnorm, out, exact);
+        points, np, d, k, S, np, w.cnorm, out, w.ccount, w.citems);
     e = cudaGetLastError();
   }
   note_cuda_error(e, "kmeans assign");
+  if (e != cudaSuccess) return cuda_status(e);
+  return launch_settle(points, d, cent, k, w, out, exact, s);
+}
+
+// The tensor-core form applies to points with 4 <= dims <= 64 (a multiple of
+// 4, rows 16-byte aligned, for TMA) and at most 256 centroids.
+bool tc_form_applies(const float *points, int d, int k) {
+  return d >= 4 && d % 4 == 0 && (reinterpret_cast<uintptr_t>(points) & 15u) == 0 &&
+         ((d + 31) & ~31) <= kTcMaxD && ((k + 31) & ~31) <= kTcMaxK;
+}
+
+template <int W>
+hml_status launch_km_tc(const CUtensorMap &tx, const CUtensorMap &tb, const KmTcArgs &a,
+                        int grid, size_t smem, cudaStream_t s) {
+  auto kern = kmeans_tc_kernel<W>;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       static_cast<int>(smem));
+  if (e == cudaSuccess) {
+    kern<<<grid, km_tc_threads(W), smem, s>>>(tx, tb, a);
+    e = cudaGetLastError();
+  }
+  note_cuda_error(e, "kmeans tensor-core");
   return cuda_status(e);
+}
+
+// The tensor-core form (method 3): centroid norms and TF32 planes, then one
+// persistent launch.
+hml_status assign_tc(const float *points, int np, int d, const float *cent, int k,
+                     uint32_t *out, unsigned *exact, cudaStream_t s) {
+  const int dp = (d + 31) & ~31, kp = (k + 31) & ~31, nkb = dp / 32;
+  const int W = kp + 2 * dp <= 128 ? 4 : kp + 2 * dp <= 256 ? 2 : 1;
+  const size_t pbytes = static_cast<size_t>(2) * kp * dp * sizeof(uint32_t);
+  KmWs w;
+  hml_status st = km_workspace(pbytes, np, k, s, &w);
+  if (st == HML_STATUS_SUCCESS) st = launch_norms(cent, k, d, w, s);
+  if (st != HML_STATUS_SUCCESS) return st;
+  uint32_t *planes = reinterpret_cast<uint32_t *>(w.extra);
+  count_launch();
+  const int pblocks = std::min((kp * dp + 255) / 256, 4 * sm_count());
+  kmeans_tf32_planes_kernel<<<pblocks, 256, 0, s>>>(cent, k, d, kp, dp, planes);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) {
+    note_cuda_error(e, "kmeans planes");
+    return HML_STATUS_CUDA_ERROR;
+  }
+  CUtensorMap tx, tb;
+  memset(&tx, 0, sizeof(tx));
+  memset(&tb, 0, sizeof(tb));
+  if (!tensor_map_2d(&tx, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, points, d, np,
+                     static_cast<uint64_t>(d) * 4, 32, kTP, CU_TENSOR_MAP_SWIZZLE_128B) ||
+      !tensor_map_2d(&tb, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, planes, dp, 2 * kp,
+                     static_cast<uint64_t>(dp) * 4, 32, kp, CU_TENSOR_MAP_SWIZZLE_128B))
+    return HML_STATUS_CUDA_ERROR;
+  const size_t slot = static_cast<size_t>(nkb) * kTcBox;
+  const size_t bbytes = static_cast<size_t>(2) * nkb * kp * 128;
+  const int sa = static_cast<int>(std::min<size_t>(6, (200 * 1024 - bbytes) / slot));
+  if (sa < 2) return HML_STATUS_NOT_SUPPORTED;
+  size_t smem = 1024 + sa * slot + bbytes + static_cast<size_t>(kp) * 4 +
+                static_cast<size_t>(2 * sa + W + 1) * 8 + 16;
+  // one CTA per SM: each allocates all 512 TMEM columns
+  smem = std::max<size_t>(smem, 120 * 1024);
+  KmTcArgs a;
+  a.np = np;
+  a.d = d;
+  a.k = k;
+  a.dp = dp;
+  a.kp = kp;
+  a.sa = sa;
+  a.cnorm = w.cnorm;
+  a.out = out;
+  a.ccount = w.ccount;
+  a.citems = w.citems;
+  a.err = device_error_word();
+  const int64_t tiles = (static_cast<int64_t>(np) + kTP - 1) / kTP;
+  const int grid = static_cast<int>(std::min<int64_t>(tiles, sm_count()));
+  count_launch();
+  switch (W) {
+    case 4: st = launch_km_tc<4>(tx, tb, a, grid, smem, s); break;
+    case 2: st = launch_km_tc<2>(tx, tb, a, grid, smem, s); break;
+    default: st = launch_km_tc<1>(tx, tb, a, grid, smem, s); break;
+  }
+  if (st != HML_STATUS_SUCCESS) return st;
+  return launch_settle(points, d, cent, k, w, out, exact, s);
 }
 
 }  // namespace
 
 hml_status kmeans_assign(const float *points, int np, int d, const float *cent, int k,
                          uint32_t *out, int method, unsigned *exact, cudaStream_t s) {
-  if (np < 0 || d < 0 || k < 1 || method < 0 || method > 2) return HML_STATUS_INVALID_VALUE;
+  if (np < 0 || d < 0 || k < 1 || method < 0 || method > 3) return HML_STATUS_INVALID_VALUE;
   if (np == 0) return HML_STATUS_SUCCESS;
   if (!out || (d > 0 && (!points || !cent))) return HML_STATUS_INVALID_VALUE;
   // the pick kernel keeps ||c||^2 of every centroid in shared memory
   if (method == 2 && static_cast<size_t>(k) * sizeof(float) > 200 * 1024)
     return HML_STATUS_NOT_SUPPORTED;
-  if (method == 0) method = d <= kKmeansTiledMaxDims ? 1 : 2;
-  if (method == 2 && static_cast<size_t>(k) * sizeof(float) > 200 * 1024) method = 1;
-  return method == 1 ? assign_tiled(points, np, d, cent, k, out, exact, s)
-                     : assign_gemm(points, np, d, cent, k, out, exact, s);
+  if (method == 3 && !tc_form_applies(points, d, k)) return HML_STATUS_NOT_SUPPORTED;
+  if (method == 0) {
+    method = tc_form_applies(points, d, k) ? 3 : d <= kKmeansTiledMaxDims ? 1 : 2;
+    if (method == 2 && static_cast<size_t>(k) * sizeof(float) > 200 * 1024) method = 1;
+  }
+  switch (method) {
+    case 1: return assign_tiled(points, np, d, cent, k, out, exact, s);
+    case 2: return assign_gemm(points, np, d, cent, k, out, exact, s);
+    default: return assign_tc(points, np, d, cent, k, out, exact, s);
+  }
 }
 
 }  // namespace hml

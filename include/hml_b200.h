@@ -446,13 +446,18 @@ hml_status hml_kmeans_assign(const float *points, int num_points, int dims,
                              const float *centroids, int num_clusters,
                              uint32_t *assignments, void *stream);
 
-/* The same with the form chosen: method 0 = the library's choice (the tiled
- * form up to 256 dimensions), 1 = the tiled form (a register-tiled FP32 SIMT
- * GEMM with the argmin in its epilogue), 2 = the SGEMM form (the products
- * through HBM, num_points x num_clusters floats of workspace, then a pick
- * kernel; HML_STATUS_NOT_SUPPORTED above 51200 clusters).  When exact_count
- * (a device counter) is not NULL, the number of points whose candidates had
- * to be compared with the reference's own arithmetic is added to it. */
+/* The same with the form chosen: method 0 = the library's choice (the
+ * tensor-core form where it applies, else the tiled form up to 256
+ * dimensions, else the SGEMM form), 1 = the tiled form (a register-tiled FP32
+ * SIMT GEMM with the argmin in its epilogue), 2 = the SGEMM form (the
+ * products through HBM, num_points x num_clusters floats of workspace, then a
+ * pick kernel; HML_STATUS_NOT_SUPPORTED above 51200 clusters), 3 = the
+ * tensor-core form (TF32X3 products on tcgen05 into TMEM, the argmin read
+ * from the accumulator; HML_STATUS_NOT_SUPPORTED unless dims is a multiple
+ * of 4 in 4..64, points is 16-byte aligned and num_clusters <= 256).  When
+ * exact_count (a device counter) is not NULL, the number of points whose
+ * candidates had to be compared with the reference's own arithmetic is added
+ * to it. */
 hml_status hml_kmeans_assign_ex(const float *points, int num_points, int dims,
                                 const float *centroids, int num_clusters,
                                 uint32_t *assignments, int method,

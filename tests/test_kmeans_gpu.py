@@ -1,8 +1,10 @@
 """The k-means assignment step on the skinny SGEMM (GPU).
 
 hml_kmeans_assign computes argmin_k ||c_k||^2 - 2 x.c_k from one GEMM -- in
-the tiled form (a register-tiled SIMT GEMM with the argmin in its epilogue)
-or the SGEMM form (the products through HBM, then a pick kernel) -- and
+the tiled form (a register-tiled SIMT GEMM with the argmin in its epilogue),
+the SGEMM form (the products through HBM, then a pick kernel) or the
+tensor-core form (TF32X3 products in TMEM, the argmin read from the
+accumulator) -- and
 resolves every close call with the reference kernel's own arithmetic, so
 either form's indices must equal, bit for bit, those of
   * the C restatement of the reference kernel (oracle.kmeans_assign), and
@@ -26,7 +28,20 @@ def dev(a):
     return torch.from_numpy(np.ascontiguousarray(a, np.float32)).cuda()
 
 
-METHODS = [hml.KMEANS_TILED, hml.KMEANS_GEMM]
+METHODS = [hml.KMEANS_TILED, hml.KMEANS_GEMM, hml.KMEANS_TENSOR]
+
+
+def tensor_applies(d, k):
+    return d >= 4 and d % 4 == 0 and d <= 64 and k <= 256
+
+
+def skip_unless_applies(method, d, k):
+    """The tensor-core form refuses shapes outside its range (checked here)."""
+    if method == hml.KMEANS_TENSOR and not tensor_applies(d, k):
+        with pytest.raises(hml.HmlError):
+            hml.kmeans_assign(dev(np.zeros((4, d), np.float32)), dev(np.zeros((k, d), np.float32)),
+                              method=method)
+        pytest.skip("outside the tensor-core form's range (refusal checked)")
 
 
 def ours(P, C, method=hml.KMEANS_AUTO):
@@ -48,6 +63,7 @@ def test_matches_reference_arithmetic(cuda, method, d, k):
     """Dimensions around the tiled form's 32-wide stages, centroid counts
     around its 64-wide passes, point counts not a multiple of its 128-point
     blocks."""
+    skip_unless_applies(method, d, k)
     rng = np.random.default_rng(d * 1000 + k)
     P, C = clustered(rng, 3001, d, k)
     got, _ = ours(P, C, method)
@@ -62,18 +78,29 @@ def test_automatic_choice_and_edge_cases(cuda):
         got, _ = ours(P, C)
         np.testing.assert_array_equal(got, oracle.kmeans_assign(P, C))
     # zero dimensions: every distance is 0, the first centroid wins
-    for method in METHODS:
+    for method in METHODS[:2]:
         out = hml.kmeans_assign(torch.zeros((50, 0), device="cuda"),
                                 torch.zeros((7, 0), device="cuda"), method=method)
         assert int(out.abs().sum()) == 0
     # one point; no points
-    P, C = clustered(rng, 1, 5, 9)
+    P, C = clustered(rng, 1, 8, 9)
     for method in METHODS:
         np.testing.assert_array_equal(ours(P, C, method)[0], oracle.kmeans_assign(P, C))
-        assert hml.kmeans_assign(torch.zeros((0, 5), device="cuda"), dev(C),
+        assert hml.kmeans_assign(torch.zeros((0, 8), device="cuda"), dev(C),
                                  method=method).numel() == 0
     with pytest.raises(hml.HmlError):
-        hml.kmeans_assign(dev(P), dev(C), method=3)
+        hml.kmeans_assign(dev(P), dev(C), method=4)
+    # the tensor-core form: 257 centroids, 68 dimensions, unaligned rows
+    for shape in ((10, 8, 257), (10, 68, 9), (10, 6, 9)):
+        with pytest.raises(hml.HmlError):
+            hml.kmeans_assign(dev(np.zeros(shape[:2], np.float32)),
+                              dev(np.zeros(shape[2:] + shape[1:2], np.float32)),
+                              method=hml.KMEANS_TENSOR)
+    import torch
+    buf = torch.zeros(1 + 100 * 8, device="cuda")
+    with pytest.raises(hml.HmlError):
+        hml.kmeans_assign(buf[1:].view(100, 8), dev(np.zeros((9, 8), np.float32)),
+                          method=hml.KMEANS_TENSOR)
 
 
 @pytest.mark.parametrize("method", METHODS)
@@ -81,7 +108,7 @@ def test_non_finite_values(cuda, method):
     """NaN and infinite coordinates: the reference skips a NaN distance
     (`dist < minDist` is false) and keeps the first of equal ones."""
     rng = np.random.default_rng(4)
-    P, C = clustered(rng, 2000, 12, 30)
+    P, C = clustered(rng, 2000, 12, 30)  # 12 dimensions: every form applies
     P[5, 3] = np.nan
     P[6, :] = np.inf
     P[7, 0] = -np.inf
