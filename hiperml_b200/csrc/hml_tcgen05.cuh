@@ -192,4 +192,16 @@ __device__ __forceinline__ uint32_t tf32_rna(float x) {
   return r;
 }
 
+// D (TMEM) (+)= A (shared memory descriptor, 128 rows x 8 TF32) * B (shared
+// memory descriptor, 8 TF32 deep), kind::tf32 with an FP32 accumulator.
+__device__ __forceinline__ void mma_tf32_ss(uint32_t dtmem, uint64_t adesc, uint64_t bdesc,
+                                            uint32_t idesc, uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}" ::"r"(dtmem),
+      "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
+      : "memory");
+}
+
 }  // namespace hml

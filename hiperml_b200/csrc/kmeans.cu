@@ -127,6 +127,7 @@ __device__ __forceinline__ void push_close(unsigned *ccount, uint2 *citems, int6
 __global__ void kmeans_settle_kernel(const float *points, int d, const float *cent, int k,
                                      const float *cnorm, const unsigned *ccount,
                                      const uint2 *citems, uint32_t *out, unsigned *exact) {
+  wait_prior_grid();  // launched as a programmatic dependent of the screening kernel
   const unsigned n = *ccount;
   if (exact && n && blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(exact, n);
   const int lane = threadIdx.x & 31;
@@ -572,26 +573,13 @@ constexpr int kTcBox = kTP * 32 * 4;  // bytes of one 128 x 32 FP32 box
 
 struct KmTcArgs {
   int np, d, k, dp, kp, sa;
+  int nc, passes;  // centroids per pass (a multiple of 32) and passes per tile
   const float *cnorm;
   uint32_t *out;
   unsigned *ccount;
   uint2 *citems;
   int *err;
 };
-
-// TF32 hi and lo planes of the centroids: planes[p][c][j] (j contiguous, zero
-// padded to kp x dp), hi = TF32(x), lo = TF32(x - hi) (the residual exact).
-__global__ void kmeans_tf32_planes_kernel(const float *cent, int k, int d, int kp, int dp,
-                                          uint32_t *planes) {
-  const int n = kp * dp;
-  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += gridDim.x * blockDim.x) {
-    const int c = e / dp, j = e - c * dp;
-    const float v = (c < k && j < d) ? cent[static_cast<int64_t>(c) * d + j] : 0.0f;
-    const uint32_t hi = tf32_rna(v);
-    planes[e] = hi;
-    planes[n + e] = tf32_rna(__fsub_rn(v, __uint_as_float(hi)));
-  }
-}
 
 // OR of `v` over the 128 threads of a warpgroup (named barrier `id`).
 __device__ __forceinline__ bool group_any(bool v, int id) {
@@ -648,6 +636,8 @@ __global__ void __launch_bounds__(km_tc_threads(W), 1)
     prefetch_tmap(&tmX);
     prefetch_tmap(&tmB);
   }
+  // the planes and norms come from the prep kernel launched just before
+  wait_prior_grid();
   if (warp == 1) {
     // ||c||^2 (+inf past k: never taken, and never the second smallest) and
     // its maximum over the centroids
@@ -695,14 +685,15 @@ __global__ void __launch_bounds__(km_tc_threads(W), 1)
     const int g = (warp - 4) >> 2, bar_id = 1 + g;
     const int m = (warp & 3) * 32 + lane;  // tile row == TMEM lane
     const uint32_t lanes = static_cast<uint32_t>((warp & 3) * 32) << 16;
-    const uint32_t tacc = tmem + static_cast<uint32_t>(g * (kp + 2 * dp));
-    const uint32_t tA = tacc + static_cast<uint32_t>(kp);  // hi plane dp columns, then lo
+    const int nc = a.nc, P = a.passes;
+    const uint32_t tacc = tmem + static_cast<uint32_t>(g * (nc + 2 * dp));
+    const uint32_t tA = tacc + static_cast<uint32_t>(nc);  // hi plane dp columns, then lo
     const bool issuer = warp == 4 + 4 * g && lane == 0;
     const float cmax = *s_cmax;
     const double nu = (a.d + 4) * 0x1p-24;
     const float bound = static_cast<float>(32.0 * nu / (1.0 - nu) * 1.001);
-    const uint32_t idesc = idesc_tf32(kp);
-    int it = 0;
+    const uint32_t idesc = idesc_tf32(nc);
+    int it = 0, ph = 0;  // tiles done, phases of accfull[g] done
     for (int j = g; j < my_tiles; j += W, ++it) {
       const int st = j % SA;
       const bool w = mbar_wait(&afull[st], (j / SA) & 1, a.err, kDevErrFullBarrier);
@@ -743,59 +734,70 @@ __global__ void __launch_bounds__(km_tc_threads(W), 1)
       tmem_wait_st();
       tc_fence_before();
       group_sync(bar_id);
-      if (issuer) {
-        tc_fence_after();
-        bool bok = true;
-        if (it == 0) bok = mbar_wait(bfull, 0, a.err, kDevErrFullBarrier);
-        if (bok) {
-          // products hh, hl, lh of every 8-deep step of every 32-dim block
-          for (int kb = 0; kb < nkb; ++kb)
-#pragma unroll
-            for (int kk = 0; kk < 4; ++kk)
-#pragma unroll
-              for (int pr = 0; pr < 3; ++pr) {
-                const int ia = pr == 2 ? 1 : 0, jb = pr == 1 ? 1 : 0;
-                const uint32_t at = tA + static_cast<uint32_t>(ia * dp + kb * 32 + kk * 8);
-                const uint64_t bd =
-                    sw128_desc(smem_u32(bsm + (jb * nkb + kb) * btile)) +
-                    static_cast<uint64_t>((kk * 32) >> 4);
-                mma_tf32_ts(tacc, at, bd, idesc, (kb | kk | pr) != 0 ? 1u : 0u);
-              }
-        }
-        mma_commit(&accfull[g]);  // arrives once the group's MMAs are done
-      }
-      const bool w2 = mbar_wait(&accfull[g], it & 1, a.err, kDevErrMmaBarrier);
-      if (group_any(!w2, bar_id)) break;
-      __syncwarp();  // tcgen05.ld is warp-collective
-      tc_fence_after();
-      // argmin of g_k over the point's row of the accumulator, without
-      // branches: g1 the smallest, k1 the first index reaching it, g2 the
-      // second smallest of the multiset (equal to g1 on a tie; a NaN g makes
-      // it g1 too, which only sends the point to the close-call list)
+      // the centroids in P passes of nc (the accumulator holds one pass):
+      // argmin of g_k over the point's row, without branches -- g1 the
+      // smallest, k1 the first index reaching it, g2 the second smallest of
+      // the multiset (equal to g1 on a tie; a NaN g makes it g1 too, which
+      // only sends the point to the close-call list)
       float g1 = INFINITY, g2 = INFINITY;
       int k1 = 0;
-      for (int c0 = 0; c0 < kp; c0 += 16) {
-        uint32_t r[16];
-        tmem_ld16(tacc + lanes + static_cast<uint32_t>(c0), r);
-        float cv[16];
+      bool bad = false;
+      for (int q = 0; q < P; ++q) {
+        if (issuer) {
+          tc_fence_after();
+          bool bok = true;
+          if (it == 0 && q == 0) bok = mbar_wait(bfull, 0, a.err, kDevErrFullBarrier);
+          if (bok) {
+            // products hh, hl, lh of every 8-deep step of every 32-dim block,
+            // against centroids q*nc .. q*nc+nc-1 (rows of the B tiles)
+            for (int kb = 0; kb < nkb; ++kb)
 #pragma unroll
-        for (int q = 0; q < 4; ++q) {
-          const float4 v = *reinterpret_cast<const float4 *>(cn + c0 + 4 * q);
-          cv[4 * q] = v.x;
-          cv[4 * q + 1] = v.y;
-          cv[4 * q + 2] = v.z;
-          cv[4 * q + 3] = v.w;
-        }
-        tmem_wait_ld();
+              for (int kk = 0; kk < 4; ++kk)
 #pragma unroll
-        for (int i = 0; i < 16; ++i) {
-          const float gv = fmaf(-2.0f, __uint_as_float(r[i]), cv[i]);
-          k1 = gv < g1 ? c0 + i : k1;
-          g2 = fminf(g2, fmaxf(g1, gv));
-          g1 = fminf(g1, gv);
+                for (int pr = 0; pr < 3; ++pr) {
+                  const int ia = pr == 2 ? 1 : 0, jb = pr == 1 ? 1 : 0;
+                  const uint32_t at = tA + static_cast<uint32_t>(ia * dp + kb * 32 + kk * 8);
+                  const uint64_t bd =
+                      sw128_desc(smem_u32(bsm + (jb * nkb + kb) * btile + q * nc * 128)) +
+                      static_cast<uint64_t>((kk * 32) >> 4);
+                  mma_tf32_ts(tacc, at, bd, idesc, (kb | kk | pr) != 0 ? 1u : 0u);
+                }
+          }
+          mma_commit(&accfull[g]);  // arrives once the group's MMAs are done
         }
+        const bool w2 = mbar_wait(&accfull[g], ph & 1, a.err, kDevErrMmaBarrier);
+        ++ph;
+        if (group_any(!w2, bar_id)) {
+          bad = true;
+          break;
+        }
+        __syncwarp();  // tcgen05.ld is warp-collective
+        tc_fence_after();
+        for (int c0 = 0; c0 < nc; c0 += 16) {
+          uint32_t r[16];
+          tmem_ld16(tacc + lanes + static_cast<uint32_t>(c0), r);
+          float cv[16];
+#pragma unroll
+          for (int qq = 0; qq < 4; ++qq) {
+            const float4 v = *reinterpret_cast<const float4 *>(cn + q * nc + c0 + 4 * qq);
+            cv[4 * qq] = v.x;
+            cv[4 * qq + 1] = v.y;
+            cv[4 * qq + 2] = v.z;
+            cv[4 * qq + 3] = v.w;
+          }
+          tmem_wait_ld();
+#pragma unroll
+          for (int i = 0; i < 16; ++i) {
+            const float gv = fmaf(-2.0f, __uint_as_float(r[i]), cv[i]);
+            k1 = gv < g1 ? q * nc + c0 + i : k1;
+            g2 = fminf(g2, fmaxf(g1, gv));
+            g1 = fminf(g1, gv);
+          }
+        }
+        tc_fence_before();  // the reads are done before the next MMAs
+        if (q + 1 < P) group_sync(bar_id);
       }
-      tc_fence_before();  // the reads are done before the next tile's MMAs
+      if (bad) break;
       const int64_t t = blockIdx.x + static_cast<int64_t>(j) * gridDim.x;
       const int64_t p = t * kTP + m;
       const bool live = p < a.np;
@@ -807,10 +809,35 @@ __global__ void __launch_bounds__(km_tc_threads(W), 1)
   }
   tc_fence_before();
   __syncthreads();
+  // the settle kernel may now be scheduled (it waits for this grid itself);
+  // earlier, its waiting CTAs would sit beside this kernel's on every SM
+  allow_dependent_launch();
   if (warp == 2) {
     tc_fence_after();
     tmem_dealloc(tmem, 512);
   }
+}
+
+// Prep for the tensor-core form: the TF32 planes of the centroids and their
+// norms (one warp per centroid row, the norm summed lane-wise -- it only
+// enters the bound), and an empty close-call list.
+__global__ void kmeans_tc_prep_kernel(const float *cent, int k, int d, int kp, int dp,
+                                      uint32_t *planes, float *cnorm, unsigned *ccount) {
+  allow_dependent_launch();
+  if (blockIdx.x == 0 && threadIdx.x == 0) *ccount = 0u;
+  const int lane = threadIdx.x & 31;
+  const int c = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (c >= kp) return;
+  float sq = 0.0f;
+  for (int j = lane; j < dp; j += 32) {
+    const float v = (c < k && j < d) ? cent[static_cast<int64_t>(c) * d + j] : 0.0f;
+    const uint32_t hi = tf32_rna(v);
+    planes[c * dp + j] = hi;
+    planes[kp * dp + c * dp + j] = tf32_rna(__fsub_rn(v, __uint_as_float(hi)));
+    sq = fmaf(v, v, sq);
+  }
+  sq = warp_sum(sq);
+  if (lane == 0 && c < k) cnorm[c] = sq;
 }
 
 // The call's workspace (the stream's second slot): `extra` bytes for the
@@ -849,13 +876,14 @@ hml_status launch_norms(const float *cent, int k, int d, const KmWs &w, cudaStre
   return cuda_status(e);
 }
 
-// The close calls the screening kernel listed; last in every form.
+// The close calls the screening kernel listed; last in every form
+// (`early`: as a programmatic dependent of a screening kernel that allows it).
 hml_status launch_settle(const float *points, int d, const float *cent, int k, const KmWs &w,
-                         uint32_t *out, unsigned *exact, cudaStream_t s) {
-  count_launch();
-  kmeans_settle_kernel<<<2 * sm_count(), 256, 0, s>>>(points, d, cent, k, w.cnorm, w.ccount,
-                                                      w.citems, out, exact);
-  cudaError_t e = cudaGetLastError();
+                         uint32_t *out, unsigned *exact, cudaStream_t s, bool early = false) {
+  cudaError_t e = launch_k_ex(kmeans_settle_kernel, dim3(2 * sm_count()), dim3(256), 0, s, 1,
+                              early, points, d, cent, k, static_cast<const float *>(w.cnorm),
+                              static_cast<const unsigned *>(w.ccount),
+                              static_cast<const uint2 *>(w.citems), out, exact);
   note_cuda_error(e, "kmeans settle");
   return cuda_status(e);
 }
@@ -963,32 +991,44 @@ hml_status launch_km_tc(const CUtensorMap &tx, const CUtensorMap &tb, const KmTc
   auto kern = kmeans_tc_kernel<W>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        static_cast<int>(smem));
-  if (e == cudaSuccess) {
-    kern<<<grid, km_tc_threads(W), smem, s>>>(tx, tb, a);
-    e = cudaGetLastError();
-  }
+  if (e == cudaSuccess)
+    e = launch_k_ex(kern, dim3(grid), dim3(km_tc_threads(W)), smem, s, 1, true, tx, tb, a);
   note_cuda_error(e, "kmeans tensor-core");
   return cuda_status(e);
 }
 
-// The tensor-core form (method 3): centroid norms and TF32 planes, then one
-// persistent launch.
+// The tensor-core form (method 3): centroid planes and norms in one prep
+// kernel, then the persistent screening kernel and the settle kernel, each a
+// programmatic dependent of the kernel before it.
 hml_status assign_tc(const float *points, int np, int d, const float *cent, int k,
                      uint32_t *out, unsigned *exact, cudaStream_t s) {
   const int dp = (d + 31) & ~31, kp = (k + 31) & ~31, nkb = dp / 32;
-  const int W = kp + 2 * dp <= 128 ? 4 : kp + 2 * dp <= 256 ? 2 : 1;
+  // W groups, each with nc + 2 dp TMEM columns (a pass's accumulator, the A
+  // planes): the fewest passes P (nc = kp / P, a multiple of 32) that give
+  // the most groups, up to 4
+  int W = 0, P = 1;
+  for (int p = 1; p <= kp / 32; ++p) {
+    if ((kp / 32) % p) continue;
+    const int per = kp / p + 2 * dp;
+    const int w = per <= 128 ? 4 : per <= 256 ? 2 : per <= 512 ? 1 : 0;
+    if (w > W) {
+      W = w;
+      P = p;
+    }
+    if (W == 4) break;
+  }
+  if (W == 0) return HML_STATUS_NOT_SUPPORTED;
   const size_t pbytes = static_cast<size_t>(2) * kp * dp * sizeof(uint32_t);
   KmWs w;
   hml_status st = km_workspace(pbytes, np, k, s, &w);
-  if (st == HML_STATUS_SUCCESS) st = launch_norms(cent, k, d, w, s);
   if (st != HML_STATUS_SUCCESS) return st;
   uint32_t *planes = reinterpret_cast<uint32_t *>(w.extra);
   count_launch();
-  const int pblocks = std::min((kp * dp + 255) / 256, 4 * sm_count());
-  kmeans_tf32_planes_kernel<<<pblocks, 256, 0, s>>>(cent, k, d, kp, dp, planes);
+  kmeans_tc_prep_kernel<<<(kp + 7) / 8, 256, 0, s>>>(cent, k, d, kp, dp, planes, w.cnorm,
+                                                     w.ccount);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) {
-    note_cuda_error(e, "kmeans planes");
+    note_cuda_error(e, "kmeans prep");
     return HML_STATUS_CUDA_ERROR;
   }
   CUtensorMap tx, tb;
@@ -1001,7 +1041,10 @@ hml_status assign_tc(const float *points, int np, int d, const float *cent, int 
     return HML_STATUS_CUDA_ERROR;
   const size_t slot = static_cast<size_t>(nkb) * kTcBox;
   const size_t bbytes = static_cast<size_t>(2) * nkb * kp * 128;
-  const int sa = static_cast<int>(std::min<size_t>(6, (200 * 1024 - bbytes) / slot));
+  // a multiple of W (tiles go to group j % W and slot j % sa: each group
+  // then waits for every phase of its slots in order)
+  int sa = static_cast<int>(std::min<size_t>(6, (200 * 1024 - bbytes) / slot));
+  sa -= sa % W;
   if (sa < 2) return HML_STATUS_NOT_SUPPORTED;
   size_t smem = 1024 + sa * slot + bbytes + static_cast<size_t>(kp) * 4 +
                 static_cast<size_t>(2 * sa + W + 1) * 8 + 16;
@@ -1014,6 +1057,8 @@ hml_status assign_tc(const float *points, int np, int d, const float *cent, int 
   a.dp = dp;
   a.kp = kp;
   a.sa = sa;
+  a.nc = kp / P;
+  a.passes = P;
   a.cnorm = w.cnorm;
   a.out = out;
   a.ccount = w.ccount;
@@ -1021,14 +1066,13 @@ hml_status assign_tc(const float *points, int np, int d, const float *cent, int 
   a.err = device_error_word();
   const int64_t tiles = (static_cast<int64_t>(np) + kTP - 1) / kTP;
   const int grid = static_cast<int>(std::min<int64_t>(tiles, sm_count()));
-  count_launch();
   switch (W) {
     case 4: st = launch_km_tc<4>(tx, tb, a, grid, smem, s); break;
     case 2: st = launch_km_tc<2>(tx, tb, a, grid, smem, s); break;
     default: st = launch_km_tc<1>(tx, tb, a, grid, smem, s); break;
   }
   if (st != HML_STATUS_SUCCESS) return st;
-  return launch_settle(points, d, cent, k, w, out, exact, s);
+  return launch_settle(points, d, cent, k, w, out, exact, s, true);
 }
 
 }  // namespace

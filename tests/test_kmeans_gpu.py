@@ -103,6 +103,17 @@ def test_automatic_choice_and_edge_cases(cuda):
                           method=hml.KMEANS_TENSOR)
 
 
+@pytest.mark.parametrize("d,k", [(64, 250), (40, 256), (64, 160), (12, 256), (4, 1)])
+def test_tensor_core_form_shapes(cuda, d, k):
+    """The tensor-core form's kernels: the pipelined one (planes in shared
+    memory) where two tile slots fit beside the centroids, the first one
+    (planes in TMEM) beyond (64 dimensions with more than 160 centroids)."""
+    rng = np.random.default_rng(d * 7 + k)
+    P, C = clustered(rng, 5000, d, k)
+    got, _ = ours(P, C, hml.KMEANS_TENSOR)
+    np.testing.assert_array_equal(got, oracle.kmeans_assign(P, C))
+
+
 @pytest.mark.parametrize("method", METHODS)
 def test_non_finite_values(cuda, method):
     """NaN and infinite coordinates: the reference skips a NaN distance
