@@ -70,39 +70,48 @@ __device__ __forceinline__ float ref_dist(const float *x, const float *c, int d)
 }
 
 // The reference's pick for point x among the candidates -- the centroids
-// whose g_k, recomputed, is at most lim -- by the G lanes of a group (lanes
-// `gmask`, this one lane r of G): lane r takes centroids r, r + G, ...,
-// keeping the first smallest dist below FLT_MAX (strict <, increasing k),
-// and the group keeps the smallest dist, the lowest k among equal ones: the
-// first minimum in k order, which is the reference's pick.  0 when no
-// candidate's dist is below FLT_MAX (the reference leaves that case unset).
-template <int G>
+// whose g_k, recomputed, is at most lim -- by one warp (every lane calls
+// this with the same arguments).  For 8 centroids at a time, in increasing
+// k, the lanes form x . c_k together (lane r takes dimensions r, r + 32,
+// ...: coalesced loads of the rows; the partial sums added by xor shuffles,
+// so every lane holds the same dot product: any FP32 evaluation of g stays
+// within the bound the screen allowed for); for a candidate every lane forms
+// the reference's own distance (sequential, subtract then FMA) and keeps the
+// first smallest below FLT_MAX (strict <), which is the reference's pick.
+// 0 when no candidate's distance is below FLT_MAX (the reference leaves that
+// case unset).
 __device__ __noinline__ uint32_t exact_pick(const float *x, int d, const float *cent, int k,
-                                            const float *cnorm, float lim, unsigned gmask,
-                                            int r) {
+                                            const float *cnorm, float lim) {
+  constexpr int U = 8;  // centroids in flight: their loads and shuffle trees interleave
+  const int lane = threadIdx.x & 31;
   float bd = FLT_MAX;
-  int bk = -1;
-  for (int c = r; c < k; c += G) {
-    const float *cp = cent + static_cast<int64_t>(c) * d;
-    float dot = 0.0f;
-    for (int j = 0; j < d; ++j) dot = fmaf(x[j], cp[j], dot);
-    if (!(fmaf(-2.0f, dot, cnorm[c]) <= lim)) continue;
-    const float dist = ref_dist(x, cp, d);
-    if (dist < bd) {
-      bd = dist;
-      bk = c;
-    }
-  }
+  uint32_t bk = 0;
+  for (int c0 = 0; c0 < k; c0 += U) {
+    float part[U];
 #pragma unroll
-  for (int o = 1; o < G; o <<= 1) {
-    const float od = __shfl_xor_sync(gmask, bd, o);
-    const int ok = __shfl_xor_sync(gmask, bk, o);
-    if (ok >= 0 && (bk < 0 || od < bd || (od == bd && ok < bk))) {
-      bd = od;
-      bk = ok;
+    for (int u = 0; u < U; ++u) part[u] = 0.0f;
+    for (int j = lane; j < d; j += 32) {
+      const float xj = x[j];
+#pragma unroll
+      for (int u = 0; u < U; ++u)
+        if (c0 + u < k) part[u] = fmaf(xj, cent[static_cast<int64_t>(c0 + u) * d + j], part[u]);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1)
+#pragma unroll
+      for (int u = 0; u < U; ++u) part[u] += __shfl_xor_sync(0xffffffffu, part[u], o);
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int c = c0 + u;
+      if (c >= k || !(fmaf(-2.0f, part[u], cnorm[c]) <= lim)) continue;
+      const float dist = ref_dist(x, cent + static_cast<int64_t>(c) * d, d);
+      if (dist < bd) {
+        bd = dist;
+        bk = static_cast<uint32_t>(c);
+      }
     }
   }
-  return bk < 0 ? 0u : static_cast<uint32_t>(bk);
+  return bk;
 }
 
 // Close calls (a second smallest g within the bound of the smallest, or
@@ -134,8 +143,8 @@ __global__ void kmeans_settle_kernel(const float *points, int d, const float *ce
   const unsigned warps = (gridDim.x * blockDim.x) >> 5;
   for (unsigned w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; w < n; w += warps) {
     const uint2 it = citems[w];
-    const uint32_t pick = exact_pick<32>(points + static_cast<int64_t>(it.x) * d, d, cent, k,
-                                         cnorm, __uint_as_float(it.y), 0xffffffffu, lane);
+    const uint32_t pick = exact_pick(points + static_cast<int64_t>(it.x) * d, d, cent, k, cnorm,
+                                     __uint_as_float(it.y));
     if (lane == 0) out[it.x] = pick;
   }
 }
