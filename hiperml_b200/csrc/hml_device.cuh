@@ -92,34 +92,6 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, int *e
   }
 }
 
-// The same with acquire at cluster scope: for a phase completed by arrivals
-// from other CTAs of the cluster (their writes before a release arrive are
-// visible after the wait).
-__device__ __forceinline__ bool mbar_try_wait_cluster(uint64_t *bar, uint32_t parity) {
-  uint32_t ok;
-  asm volatile(
-      "{\n\t.reg .pred p;\n\t"
-      "mbarrier.try_wait.parity.acquire.cluster.shared::cta.b64 p, [%1], %2, %3;\n\t"
-      "selp.u32 %0, 1, 0, p;\n\t}"
-      : "=r"(ok)
-      : "r"(smem_u32(bar)), "r"(parity), "r"(kSuspendNs)
-      : "memory");
-  return ok != 0;
-}
-
-__device__ __forceinline__ bool mbar_wait_cluster(uint64_t *bar, uint32_t parity, int *err,
-                                                  int code) {
-  if (mbar_try_wait_cluster(bar, parity)) return true;
-  const uint64_t t0 = globaltimer_ns();
-  for (;;) {
-    if (mbar_try_wait_cluster(bar, parity)) return true;
-    if (globaltimer_ns() - t0 > kWaitLimitNs) {
-      set_device_error(err, code);
-      return false;
-    }
-  }
-}
-
 // ------------------------------------------------- dependent launches
 // Lets the next kernel on the stream (launched as a programmatic dependent)
 // begin as soon as every CTA of this grid has executed this.

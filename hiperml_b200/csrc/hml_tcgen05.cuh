@@ -43,54 +43,6 @@ __device__ __forceinline__ void mma_bf16_ts(uint32_t dtmem, uint32_t atmem, uint
       : "memory");
 }
 
-// The same on a CTA pair: issued by the pair's leader (cluster rank 0); A rows
-// 0..127 come from the leader's TMEM and 128..255 from the peer's (same
-// address), B columns 0..N/2-1 from the leader's shared memory and N/2..N-1
-// from the peer's (same address), and D rows likewise from each TMEM.
-__device__ __forceinline__ void mma_bf16_ts_pair(uint32_t dtmem, uint32_t atmem, uint64_t bdesc,
-                                                 uint32_t idesc, uint32_t accumulate) {
-  asm volatile(
-      "{\n\t.reg .pred p;\n\t"
-      "setp.ne.b32 p, %4, 0;\n\t"
-      "tcgen05.mma.cta_group::2.kind::f16 [%0], [%1], %2, %3, p;\n\t}" ::"r"(dtmem),
-      "r"(atmem), "l"(bdesc), "r"(idesc), "r"(accumulate)
-      : "memory");
-}
-
-// Arrives on the mbarrier at this offset in both CTAs of the pair when the
-// pair's MMAs issued so far by this thread have completed.
-__device__ __forceinline__ void mma_commit_pair(uint64_t *bar) {
-  asm volatile(
-      "tcgen05.commit.cta_group::2.mbarrier::arrive::one.shared::cluster.multicast::cluster.b64 "
-      "[%0], %1;" ::"r"(smem_u32(bar)),
-      "h"(static_cast<uint16_t>(3))
-      : "memory");
-}
-
-__device__ __forceinline__ void tmem_alloc_pair(uint32_t *dst_smem, uint32_t ncols) {
-  asm volatile("tcgen05.alloc.cta_group::2.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
-                   smem_u32(dst_smem)),
-               "r"(ncols)
-               : "memory");
-  asm volatile("tcgen05.relinquish_alloc_permit.cta_group::2.sync.aligned;" ::: "memory");
-}
-
-__device__ __forceinline__ void tmem_dealloc_pair(uint32_t taddr, uint32_t ncols) {
-  asm volatile("tcgen05.dealloc.cta_group::2.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(ncols)
-               : "memory");
-}
-
-// Arrive on the mbarrier at the same offset in cluster rank 0 (release at
-// cluster scope: this thread's earlier writes, TMEM included after a
-// tcgen05.fence::before_thread_sync, are visible to a waiter there).
-__device__ __forceinline__ void mbar_arrive_rank0(uint64_t *bar) {
-  asm volatile(
-      "{\n\t.reg .b32 ra;\n\t"
-      "mapa.shared::cluster.u32 ra, %0, 0;\n\t"
-      "mbarrier.arrive.release.cluster.shared::cluster.b64 _, [ra];\n\t}" ::"r"(smem_u32(bar))
-      : "memory");
-}
-
 __device__ __forceinline__ void mma_commit(uint64_t *bar) {
   asm volatile(
       "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
@@ -145,8 +97,7 @@ __device__ __forceinline__ uint64_t sw64_desc(uint32_t saddr) {
          (static_cast<uint64_t>(4) << 61);
 }
 
-// Instruction descriptor: BF16 x BF16 -> F32, both K-major, M = bm (128, or
-// 256 on a CTA pair), N = bn.
+// Instruction descriptor: BF16 x BF16 -> F32, both K-major, M = bm, N = bn.
 __host__ __device__ constexpr uint32_t idesc_bf16(int bn, int bm = 128) {
   return (1u << 4) | (1u << 7) | (1u << 10) | (static_cast<uint32_t>(bn >> 3) << 17) |
          (static_cast<uint32_t>(bm >> 4) << 24);

@@ -65,14 +65,14 @@ constexpr int kBK = 32;       // K per block (one 64-byte BF16 swizzle row)
 constexpr int kChunkK = 64;   // K accumulated in TMEM before an FP32 drain
 constexpr int kTmemCols = 512;
 
-// Tile shapes: 128-row tiles on one CTA, and 256-row tiles on a CTA pair
-// (tcgen05.mma.cta_group::2: one MMA spans both SMs of a cluster pair, each
-// SM holding its 128 rows of A and C in its TMEM and half of B).
+// Tile shapes: 128-row tiles, one per CTA.  (256-row tiles on a CTA pair,
+// tcgen05.mma.cta_group::2, were bitwise equal but slower on every measured
+// shape -- the cross-CTA handshakes cost about 1 us per 32-deep block -- and
+// are not built.)
 struct TcShape {
   int bm, bn;
 };
-constexpr TcShape kTcShapes[] = {{128, 16}, {128, 32}, {128, 64}, {128, 128},
-                                 {256, 32}, {256, 64}, {256, 128}};
+constexpr TcShape kTcShapes[] = {{128, 16}, {128, 32}, {128, 64}, {128, 128}};
 constexpr int kNumTcShapes = sizeof(kTcShapes) / sizeof(kTcShapes[0]);
 
 // Warp roles of one CTA:
@@ -392,17 +392,10 @@ __host__ __device__ constexpr uint32_t tc_tmem_alloc_cols(int bn, int ns, int so
   return tc_pow2_cols(tc_issuers(bn, ns) * bn + so * tc_stage_cols(ns));
 }
 
-// PAIR: the CTA is one of a cluster pair running 256-row tiles with
-// tcgen05.mma.cta_group::2.  Both CTAs load and convert their own 128 rows of
-// A and their own half of B (BN/2 rows of each plane) and drain their own
-// rows of C; only the leader (rank 0) issues MMAs, for both.  The peer's
-// converters, B loader and drain warps arrive on the leader's barriers
-// (remote arrives); the leader's commits arrive on both CTAs' barriers.
-template <int BN, int NS, bool AK, bool PAIR>
+template <int BN, int NS, bool AK>
 __global__ void __launch_bounds__(tc_warps(BN, NS) * 32, 1)
     tc_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
               TcArgs args) {
-  static_assert(!PAIR || BN >= 32, "a CTA pair holds BN/2 >= 16 rows of B each");
   // NS = 4 is the TF32 form: 2 planes of 32-bit TF32 (hi, lo), the TMEM and
   // shared-memory footprint of 4 BF16 planes
   constexpr bool TF = NS == 4;
@@ -410,7 +403,6 @@ __global__ void __launch_bounds__(tc_warps(BN, NS) * 32, 1)
   // of 2 BF16 planes), a power-of-two scale per row and 32-deep block of A
   // and per column of B, each block accumulated and drained on its own
   constexpr bool FH = NS == 5;
-  static_assert(!(PAIR && (TF || FH)), "CTA pairs run the BF16 forms only");
   constexpr int PL = TF ? 2 : tc_geom(NS);                   // planes
   constexpr int PLC = TF ? kBK : kBK / 2;                    // TMEM columns of a plane
   constexpr int KMMA = TF ? 8 : 16;                          // K of one MMA
@@ -421,13 +413,12 @@ __global__ void __launch_bounds__(tc_warps(BN, NS) * 32, 1)
   constexpr int kThreads = tc_warps(BN, NS) * 32;
   constexpr int kConvWarp0 = tc_conv_warp0(BN, NS), kDrainWarp0 = kConvWarp0 + 4 * G;
   constexpr int A32_BYTES = static_cast<int>(tc_a_bytes());  // FP32 A slot (16 KB)
-  constexpr int BROWS = PAIR ? BN / 2 : BN;                 // B rows of a plane in this CTA
-  constexpr int BPL_BYTES = BROWS * kBK * (TF ? 4 : 2);      // one B plane tile
+  constexpr int BPL_BYTES = BN * kBK * (TF ? 4 : 2);         // one B plane tile
   constexpr int BSLOT = PL * BPL_BYTES;                      // one B slot
   constexpr int SC = tc_stage_cols(NS);                      // TMEM columns of an A stage
   static_assert(SC == PL * PLC, "stage columns");
   constexpr uint32_t IDESC =
-      TF ? idesc_tf32(BN) : FH ? idesc_f16(BN) : idesc_bf16(BN, PAIR ? 2 * kBM : kBM);
+      TF ? idesc_tf32(BN) : FH ? idesc_f16(BN) : idesc_bf16(BN);
   // blocks per TMEM chunk (FP16X3: one, the row scales change every block)
   constexpr int P = FH ? 1 : kChunkK / kBK;
 
@@ -459,8 +450,6 @@ __global__ void __launch_bounds__(tc_warps(BN, NS) * 32, 1)
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int split = args.split;
   const int rank = split > 1 ? static_cast<int>(cluster_ctarank()) : 0;
-  const int prank = PAIR ? static_cast<int>(cluster_ctarank()) : 0;  // 0 or 1 in a pair
-  const bool leader = prank == 0;
   const int64_t m0 = static_cast<int64_t>(blockIdx.x / split) * kBM;
   const int n0 = blockIdx.y * BN;
   const int kbeg = rank * args.kc;
@@ -475,31 +464,21 @@ __global__ void __launch_bounds__(tc_warps(BN, NS) * 32, 1)
       mbar_init(&aempty[s], 4);
     }
     for (int o = 0; o < SO; ++o) {
-      // the converter group's warps + the B loader (both CTAs' on a pair's
-      // leader; on the peer, only its B loader's own TMA completion)
-      mbar_init(&opfull[o], PAIR ? (leader ? 2 * (4 + 1) : 1) : 4 + 1);
+      mbar_init(&opfull[o], 4 + 1);  // the converter group's warps + the B loader
       mbar_init(&opempty[o], 1);
     }
     for (int b = 0; b < NI; ++b) {
       mbar_init(&accfull[b], 1);
-      mbar_init(&accempty[b], PAIR ? 2 * 4 * D : 4 * D);
+      mbar_init(&accempty[b], 4 * D);
     }
     mbar_init(mmadone, NI);  // one commit per MMA issuer
     for (int r = 0; r < R; ++r) mbar_init(&sfull[r], 4);  // the converter group's warps
     *bad_flag = 0;
     fence_mbar_init();
   }
-  if (warp == 2) {
-    if (PAIR)
-      tmem_alloc_pair(tmem_slot, tmem_cols);
-    else
-      tmem_alloc(tmem_slot, tmem_cols);
-  }
+  if (warp == 2) tmem_alloc(tmem_slot, tmem_cols);
   tc_fence_before();
-  if (PAIR)
-    cluster_sync();  // both CTAs' barriers are initialised before any remote arrive
-  else
-    __syncthreads();
+  __syncthreads();
   tc_fence_after();
   const uint32_t tmem = *tmem_slot;
   const uint32_t tacc = tmem;           // accumulator b: columns b*BN .. +BN-1
@@ -543,8 +522,7 @@ __global__ void __launch_bounds__(tc_warps(BN, NS) * 32, 1)
         mbar_arrive_expect_tx(&opfull[o], BSLOT);
 #pragma unroll
         for (int i = 0; i < PL; ++i)
-          tma_load_2d(dst + i * BPL_BYTES, &tmB, &opfull[o], k0,
-                      i * args.n_pad + n0 + prank * BROWS);
+          tma_load_2d(dst + i * BPL_BYTES, &tmB, &opfull[o], k0, i * args.n_pad + n0);
       }
     }
   } else if (warp >= 2 && warp < 2 + NI) {
@@ -552,15 +530,13 @@ __global__ void __launch_bounds__(tc_warps(BN, NS) * 32, 1)
     // NI issuing threads, one per accumulator: issuer b takes the chunks
     // q = b, b+NI, ...  A commit tracks only the MMAs of the thread that
     // issues it.
-    if (lane == 0 && leader) {
+    if (lane == 0) {
       const int b = warp - 2;
       const uint32_t dacc = tacc + static_cast<uint32_t>(b * BN);
       bool ok = true;
       for (int q = b; q < nchunks && ok; q += NI) {
-        const bool w = PAIR ? mbar_wait_cluster(&accempty[b], ((q / NI) & 1) ^ 1, args.err,
-                                                kDevErrEmptyBarrier)
-                            : mbar_wait(&accempty[b], ((q / NI) & 1) ^ 1, args.err,
-                                        kDevErrEmptyBarrier);
+        const bool w =
+            mbar_wait(&accempty[b], ((q / NI) & 1) ^ 1, args.err, kDevErrEmptyBarrier);
         if (!w) {
           ok = false;
           break;
@@ -569,9 +545,7 @@ __global__ void __launch_bounds__(tc_warps(BN, NS) * 32, 1)
         for (int kb = q * P; kb < kb1; ++kb) {
           const int o = kb % SO;
           const bool first = kb == q * P;
-          const bool w = PAIR ? mbar_wait_cluster(&opfull[o], (kb / SO) & 1, args.err,
-                                                  kDevErrFullBarrier)
-                              : mbar_wait(&opfull[o], (kb / SO) & 1, args.err, kDevErrFullBarrier);
+          const bool w = mbar_wait(&opfull[o], (kb / SO) & 1, args.err, kDevErrFullBarrier);
           if (!w) {
             ok = false;
             break;
@@ -595,42 +569,17 @@ __global__ void __launch_bounds__(tc_warps(BN, NS) * 32, 1)
                 const uint32_t acc = (!first || kk > 0 || i > 0 || j > 0) ? 1u : 0u;
                 if constexpr (TF)
                   mma_tf32_ts(dacc, at, bd, IDESC, acc);
-                else if (PAIR)
-                  mma_bf16_ts_pair(dacc, at, bd, IDESC, acc);
                 else
                   mma_bf16_ts(dacc, at, bd, IDESC, acc);
               }
           }
-          if (PAIR)
-            mma_commit_pair(&opempty[o]);
-          else
-            mma_commit(&opempty[o]);
+          mma_commit(&opempty[o]);
         }
-        if (ok) {
-          if (PAIR)
-            mma_commit_pair(&accfull[b]);
-          else
-            mma_commit(&accfull[b]);
-        }
+        if (ok) mma_commit(&accfull[b]);
       }
       if (!ok) *bad_flag = 1;
       // tracks every MMA this thread issued
-      if (PAIR)
-        mma_commit_pair(mmadone);
-      else
-        mma_commit(mmadone);
-    } else if (PAIR && !leader && warp == 3 && lane == 0) {
-      // the peer's B relay: each time a B slot of this CTA has landed (its
-      // own opfull completes on the TMA bytes), arrive on the leader's.  In
-      // a thread of its own so the B loader keeps several loads in flight.
-      for (int kb = 0; kb < nkb; ++kb) {
-        const int o = kb % SO;
-        if (!mbar_wait(&opfull[o], (kb / SO) & 1, args.err, kDevErrFullBarrier)) {
-          *bad_flag = 1;
-          break;
-        }
-        mbar_arrive_rank0(&opfull[o]);
-      }
+      mma_commit(mmadone);
     }
   } else if (warp >= kConvWarp0 && warp < kDrainWarp0) {
     // ------------------------------------------ converters (G groups)
@@ -729,12 +678,7 @@ __global__ void __launch_bounds__(tc_warps(BN, NS) * 32, 1)
       tmem_wait_st();
       tc_fence_before();
       __syncwarp();
-      if (lane == 0) {
-        if (PAIR && !leader)
-          mbar_arrive_rank0(&opfull[o]);
-        else
-          mbar_arrive(&opfull[o]);
-      }
+      if (lane == 0) mbar_arrive(&opfull[o]);
     }
   } else if (warp >= kDrainWarp0) {
     // ------------------------------------------ drain (D groups)
@@ -842,12 +786,7 @@ __global__ void __launch_bounds__(tc_warps(BN, NS) * 32, 1)
       }
       tc_fence_before();
       __syncwarp();
-      if (lane == 0) {
-        if (PAIR && !leader)
-          mbar_arrive_rank0(&accempty[b]);
-        else
-          mbar_arrive(&accempty[b]);
-      }
+      if (lane == 0) mbar_arrive(&accempty[b]);
     }
     // ---------------------------------------------------- epilogue
     // (the running sums stay in this branch's registers; the barrier is the
@@ -915,22 +854,14 @@ __global__ void __launch_bounds__(tc_warps(BN, NS) * 32, 1)
   tc_fence_before();
   __syncthreads();
   if (warp == 2) {
-    // the TMEM is freed only once every issued MMA has completed (on a pair,
-    // the leader's commits arrive on both CTAs' mmadone)
+    // the TMEM is freed only once every issued MMA has completed
     bool w = true;
     if (lane == 0) w = mbar_wait(mmadone, 0, args.err, kDevErrMmaBarrier);
     __syncwarp();
     (void)w;
     tc_fence_after();
   }
-  if (PAIR) cluster_sync();  // neither CTA leaves while the other may arrive on it
-  if (warp == 2) {
-    if (PAIR)
-      tmem_dealloc_pair(tmem, tmem_cols);
-    else
-      tmem_dealloc(tmem, tmem_cols);
-  }
-  if (PAIR) cluster_sync();
+  if (warp == 2) tmem_dealloc(tmem, tmem_cols);
 }
 
 }  // namespace
@@ -947,9 +878,6 @@ template <int BN, int NS, bool AK>
 hml_status launch_tc_planes(const GemmProblem &p, const hml_sgemm_config &c,
                             const __nv_bfloat16 *planes, int k_pad, int n_pad, int *err,
                             cudaStream_t s, const int *bexp = nullptr) {
-  // a 256-row configuration runs on CTA pairs (clusters of two)
-  const bool pair = c.tile_m == 2 * kBM;
-  if (pair && (BN < 32 || c.split_k != 1 || NS >= 4)) return HML_STATUS_INVALID_VALUE;
   if (NS == 5 && !bexp) return HML_STATUS_INVALID_VALUE;
   CUtensorMap ta, tb;
   memset(&ta, 0, sizeof ta);
@@ -969,7 +897,7 @@ hml_status launch_tc_planes(const GemmProblem &p, const hml_sgemm_config &c,
     else  // 16-bit planes (BF16, or FP16 for NS = 5: TMA only moves the bytes)
       ok = tensor_map_2d(&tb, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, planes, k_pad,
                          static_cast<uint64_t>(tc_geom(NS)) * n_pad,
-                         static_cast<uint64_t>(k_pad) * 2, kBK, pair ? BN / 2 : BN,
+                         static_cast<uint64_t>(k_pad) * 2, kBK, BN,
                          CU_TENSOR_MAP_SWIZZLE_64B);
   }
   if (!ok) return HML_STATUS_CUDA_ERROR;
@@ -986,10 +914,7 @@ hml_status launch_tc_planes(const GemmProblem &p, const hml_sgemm_config &c,
   args.err = err;
   args.bexp = bexp;
   const size_t smem = tc_plan_bytes(BN, NS, plan);
-  void (*kern)(CUtensorMap, CUtensorMap, TcArgs) = tc_kernel<BN, NS, AK, false>;
-  if constexpr (BN >= 32 && NS < 4) {
-    if (pair) kern = tc_kernel<BN, NS, AK, true>;
-  }
+  void (*kern)(CUtensorMap, CUtensorMap, TcArgs) = tc_kernel<BN, NS, AK>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        static_cast<int>(smem));
   if (e == cudaSuccess && c.split_k > 8)
@@ -998,14 +923,13 @@ hml_status launch_tc_planes(const GemmProblem &p, const hml_sgemm_config &c,
     note_cuda_error(e, "tc attributes");
     return HML_STATUS_CUDA_ERROR;
   }
-  int64_t tiles_m = (static_cast<int64_t>(p.M) + kBM - 1) / kBM;
-  if (pair) tiles_m = (tiles_m + 1) / 2 * 2;  // whole pairs; rows past M are not stored
+  const int64_t tiles_m = (static_cast<int64_t>(p.M) + kBM - 1) / kBM;
   const int64_t tiles_n = n_pad / BN;
   if (tiles_m * c.split_k > 0x7fffffff || tiles_n > 65535) return HML_STATUS_NOT_SUPPORTED;
   dim3 grid(static_cast<unsigned>(tiles_m * c.split_k), static_cast<unsigned>(tiles_n));
   // launched right after split_b_kernel wrote the planes: a programmatic
   // dependent whose B loader waits for it (wait_prior_grid)
-  e = launch_k_ex(kern, grid, dim3(tc_warps(BN, NS) * 32), smem, s, pair ? 2 : c.split_k, true,
+  e = launch_k_ex(kern, grid, dim3(tc_warps(BN, NS) * 32), smem, s, c.split_k, true,
                   ta, tb, args);
   note_cuda_error(e, "tc launch");
   return cuda_status(e);
@@ -1111,10 +1035,6 @@ hml_status check_tc(const GemmProblem &p, const hml_sgemm_config &c) {
     return HML_STATUS_INVALID_VALUE;
   if (c.variant < 0 || c.variant >= kNumTcShapes) return HML_STATUS_INVALID_VALUE;
   if (c.tile_m != kTcShapes[c.variant].bm || c.tile_n != kTcShapes[c.variant].bn)
-    return HML_STATUS_INVALID_VALUE;
-  // a CTA pair is one cluster: no cluster split-K on top of it
-  if (c.tile_m == 2 * kBM &&
-      (c.split_k != 1 || c.algo == HML_ALGO_TF32X3 || c.algo == HML_ALGO_FP16X3))
     return HML_STATUS_INVALID_VALUE;
   if (c.split_k < 1 || c.split_k > 16 || (c.split_k & (c.split_k - 1)) != 0)
     return HML_STATUS_INVALID_VALUE;

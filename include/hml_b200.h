@@ -75,10 +75,8 @@ typedef enum hml_math_mode {
 /* One point of the SGEMM configuration space. */
 typedef struct hml_sgemm_config {
   int32_t algo;    /* hml_algo                                            */
-  int32_t tile_m;  /* rows of C per CTA (the long dimension); 256 with
-                      BF16X3/BF16X6 runs a CTA pair (tcgen05 2-SM MMA,
-                      tile_n 32/64/128, split_k 1), an explicit choice
-                      only: automatic selection uses 128-row tiles       */
+  int32_t tile_m;  /* rows of C per CTA (the long dimension): 128 for
+                      the tensor-core forms, 128 or 256 for SIMT         */
   int32_t tile_n;  /* columns of C per CTA (the skinny dimension)         */
   int32_t split_k; /* CTAs of one thread-block cluster sharing a C tile,
                       each taking a slice of K; partial tiles are summed

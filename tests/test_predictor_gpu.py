@@ -145,11 +145,15 @@ def test_selection_consults_predictor(cuda):
 
 def test_live_regret_on_unseen_shapes(cuda):
     """Fresh shapes, measured now by exhaustive autotuning over the FP32
-    families; the predictor's pick is looked up in that measurement."""
+    families; the predictor's pick is looked up in that measurement.  The
+    10 % target is asserted on the 1000 held-out shapes above; on 16 live
+    shapes (a sample whose mean moves with the one or two shapes in the
+    held-out set's 10 % tail above 14 %, and with timing noise on kernels of
+    a few microseconds) the mean must stay within 15 %."""
     d = _dataset()
     pr.train(d["shapes"], d["times_us"], d["configs"])
     try:
-        shapes = td.sample_shapes(8, 99)
+        shapes = td.sample_shapes(16, 99)
         pred = pr.predict_batch(shapes)
         cfgs = [tuple(int(x) for x in c) for c in d["configs"]]
         rs = []
@@ -160,7 +164,7 @@ def test_live_regret_on_unseen_shapes(cuda):
             rs.append(t[cfgs[j]] / min(t.values()) - 1.0)
         hml.tune_clear()
         print("live regret", rs)
-        assert np.mean(rs) <= 0.25, rs
+        assert np.mean(rs) <= 0.15, rs
     finally:
         pr.clear()
 

@@ -27,7 +27,6 @@ META, ARR = load()
 X3, X6, TF, FH = hml.ALGO_BF16X3, hml.ALGO_BF16X6, hml.ALGO_TF32X3, hml.ALGO_FP16X3
 FP32_LEVEL = (X6, TF, FH)
 VAR = {16: 0, 32: 1, 64: 2, 128: 3}
-PAIR_VAR = {32: 4, 64: 5, 128: 6}  # 256-row tiles on a CTA pair
 
 
 def check_tol(algo, got, D, absD, K, what=""):
@@ -50,7 +49,7 @@ def run_tc(M, N, K, algo, bn, split=1, stages=4, order=0, ta=0, tb=0, alpha=1.0,
     Ab, Ap, lda = store(A, order, 0, offset)
     Bb, Bp, ldb = store(B, order, 0, 0)
     Cb, Cp, ldc = store(C, order, 0, 0)
-    var = VAR[bn] if tile_m == 128 else PAIR_VAR[bn]
+    var = VAR[bn]
     cfg = SgemmConfig(algo, tile_m, bn, split, stages, var)
     hml.sgemm_ex(order, ta, tb, M, N, K, alpha, Ap, lda, Bp, ldb, beta, Cp, ldc, config=cfg)
     torch.cuda.synchronize()
@@ -201,36 +200,16 @@ def test_no_device_error_left(cuda):
     assert hml.device_error() == 0
 
 
-@pytest.mark.parametrize("algo", [X3, X6])
-@pytest.mark.parametrize("bn", [32, 64, 128])
-@pytest.mark.parametrize("layout", [(0, 0, 0), (0, 1, 1), (1, 0, 0)])
-def test_tc_cta_pair_equals_single_cta(cuda, algo, bn, layout):
-    """256-row tiles on a CTA pair (tcgen05.mma.cta_group::2) accumulate each
-    row in the same order as the 128-row single-CTA tile: the results are
-    bitwise equal, and within the FP64 tolerance.  Row counts cover an odd
-    number of 128-row tiles (a pair whose second half is past M) and a
-    ragged last tile; K covers a partial 64-deep chunk."""
-    order, ta, tb = layout
-    # (leading dimensions stay multiples of 4 floats: TMA addresses A)
-    for (M, N, K) in ((300, max(1, bn - 5), 224), (640, bn, 1000), (132, bn // 2 + 1, 64)):
-        kw = dict(order=order, ta=ta, tb=tb, alpha=0.5, beta=-2.0)
-        pair, D, absD = run_tc(M, N, K, algo, bn, tile_m=256, **kw)
-        single, _, _ = run_tc(M, N, K, algo, bn, **kw)
-        assert np.array_equal(pair.view(np.uint32), single.view(np.uint32)), (algo, bn, layout, M, N, K)
-        check_tol(algo, pair, D, absD, K, what=f"pair {algo} {bn} {layout} {(M, N, K)}")
-    assert hml.device_error() == 0
+def test_tc_tiles_are_128_rows(cuda):
+    """Only 128-row tiles exist: a 256-row configuration is refused."""
+    assert all(c.tile_m == 128 for c in hml.configs() if c.algo in (X3, X6))
+    for algo in (X3, X6, TF):
+        assert hml.config_check(0, 0, 0, 512, 64, 256, 512, 256, 512,
+                                SgemmConfig(algo, 256, 64, 1, 4, VAR[64])) == 1
 
 
-def test_tc_cta_pair_rejects_split_k(cuda):
-    cfg = SgemmConfig(X6, 256, 64, 2, 4, PAIR_VAR[64])
-    assert hml.config_check(0, 0, 0, 512, 64, 256, 512, 256, 512, cfg) == 1
-
-
-def test_tf32x3_explicit_only_and_no_cta_pair(cuda):
-    """TF32X3 is an explicit configuration: outside the autotuner's space,
-    and single-CTA tiles only."""
+def test_tf32x3_explicit_only(cuda):
+    """TF32X3 is an explicit configuration: outside the autotuner's space."""
     assert all(c.algo != TF for c in hml.configs())
-    assert hml.config_check(0, 0, 0, 4096, 64, 4096, 4096, 4096, 4096,
-                            SgemmConfig(TF, 256, 64, 1, 4, PAIR_VAR[64])) == 1
     assert hml.config_check(0, 0, 0, 4096, 64, 4096, 4096, 4096, 4096,
                             SgemmConfig(TF, 128, 64, 1, 4, VAR[64])) == 0
