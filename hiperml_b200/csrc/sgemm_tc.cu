@@ -165,8 +165,13 @@ __device__ __forceinline__ void split_plane32(float (&x)[32], uint32_t (&w)[16])
     const uint32_t t = bf16x2_rn(x[2 * j], x[2 * j + 1]);
     w[j] = t;
     if (!LAST) {
-      x[2 * j] -= __uint_as_float(t << 16);
-      x[2 * j + 1] -= __uint_as_float(t & 0xFFFF0000u);
+      // both residuals with one packed FMA: fma(hi, -1, x) rounds the exact
+      // x - hi, so the bits are those of the two subtractions
+      const float2 h = make_float2(__uint_as_float(t << 16), __uint_as_float(t & 0xFFFF0000u));
+      const float2 r =
+          __ffma2_rn(h, make_float2(-1.0f, -1.0f), make_float2(x[2 * j], x[2 * j + 1]));
+      x[2 * j] = r.x;
+      x[2 * j + 1] = r.y;
     }
   }
 }
