@@ -71,7 +71,7 @@ __device__ __forceinline__ float ref_dist(const float *x, const float *c, int d)
 
 // The reference's pick for point x among the candidates -- the centroids
 // whose g_k, recomputed, is at most lim -- by one warp (every lane calls
-// this with the same arguments).  For 8 centroids at a time, in increasing
+// this with the same arguments).  For 16 centroids at a time, in increasing
 // k, the lanes form x . c_k together (lane r takes dimensions r, r + 32,
 // ...: coalesced loads of the rows; the partial sums added by xor shuffles,
 // so every lane holds the same dot product: any FP32 evaluation of g stays
@@ -82,7 +82,7 @@ __device__ __forceinline__ float ref_dist(const float *x, const float *c, int d)
 // case unset).
 __device__ __noinline__ uint32_t exact_pick(const float *x, int d, const float *cent, int k,
                                             const float *cnorm, float lim) {
-  constexpr int U = 8;  // centroids in flight: their loads and shuffle trees interleave
+  constexpr int U = 16;  // centroids in flight: their loads and shuffle trees interleave
   const int lane = threadIdx.x & 31;
   float bd = FLT_MAX;
   uint32_t bk = 0;
@@ -133,19 +133,29 @@ __device__ __forceinline__ void push_close(unsigned *ccount, uint2 *citems, int6
         make_uint2(static_cast<uint32_t>(p), __float_as_uint(lim));
 }
 
+// `cfloats` > 0: the centroids (k x d floats) fit in the block's dynamic
+// shared memory and are read from there.
 __global__ void kmeans_settle_kernel(const float *points, int d, const float *cent, int k,
                                      const float *cnorm, const unsigned *ccount,
-                                     const uint2 *citems, uint32_t *out, unsigned *exact) {
+                                     const uint2 *citems, uint32_t *out, unsigned *exact,
+                                     int cfloats) {
   wait_prior_grid();  // launched as a programmatic dependent of the screening kernel
+  extern __shared__ float s_cent[];
   const unsigned n = *ccount;
   if (exact && n && blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(exact, n);
-  const int lane = threadIdx.x & 31;
-  const unsigned warps = (gridDim.x * blockDim.x) >> 5;
+  const unsigned wpb = blockDim.x >> 5, warps = gridDim.x * wpb;
+  if (blockIdx.x * wpb >= n) return;  // no entry for this block's warps
+  const float *cb = cent;
+  if (cfloats > 0) {
+    for (int e = threadIdx.x; e < cfloats; e += blockDim.x) s_cent[e] = cent[e];
+    __syncthreads();
+    cb = s_cent;
+  }
   for (unsigned w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; w < n; w += warps) {
     const uint2 it = citems[w];
-    const uint32_t pick = exact_pick(points + static_cast<int64_t>(it.x) * d, d, cent, k, cnorm,
+    const uint32_t pick = exact_pick(points + static_cast<int64_t>(it.x) * d, d, cb, k, cnorm,
                                      __uint_as_float(it.y));
-    if (lane == 0) out[it.x] = pick;
+    if ((threadIdx.x & 31) == 0) out[it.x] = pick;
   }
 }
 
@@ -889,10 +899,19 @@ hml_status launch_norms(const float *cent, int k, int d, const KmWs &w, cudaStre
 // (`early`: as a programmatic dependent of a screening kernel that allows it).
 hml_status launch_settle(const float *points, int d, const float *cent, int k, const KmWs &w,
                          uint32_t *out, unsigned *exact, cudaStream_t s, bool early = false) {
-  cudaError_t e = launch_k_ex(kmeans_settle_kernel, dim3(2 * sm_count()), dim3(256), 0, s, 1,
-                              early, points, d, cent, k, static_cast<const float *>(w.cnorm),
-                              static_cast<const unsigned *>(w.ccount),
-                              static_cast<const uint2 *>(w.citems), out, exact);
+  // the centroids in shared memory when they fit in 96 KB
+  const int64_t cf = static_cast<int64_t>(k) * d;
+  const int cfloats = cf * 4 <= 96 * 1024 ? static_cast<int>(cf) : 0;
+  const size_t smem = static_cast<size_t>(cfloats) * 4;
+  cudaError_t e = cudaSuccess;
+  if (smem > 48 * 1024)
+    e = cudaFuncSetAttribute(kmeans_settle_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             static_cast<int>(smem));
+  if (e == cudaSuccess)
+    e = launch_k_ex(kmeans_settle_kernel, dim3(2 * sm_count()), dim3(256), smem, s, 1, early,
+                    points, d, cent, k, static_cast<const float *>(w.cnorm),
+                    static_cast<const unsigned *>(w.ccount),
+                    static_cast<const uint2 *>(w.citems), out, exact, cfloats);
   note_cuda_error(e, "kmeans settle");
   return cuda_status(e);
 }
