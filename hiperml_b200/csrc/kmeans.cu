@@ -87,9 +87,12 @@ __device__ __noinline__ uint32_t exact_pick(const float *x, int d, const float *
   float bd = FLT_MAX;
   uint32_t bk = 0;
   for (int c0 = 0; c0 < k; c0 += U) {
-    float part[U];
+    float part[U], cnv[U];
 #pragma unroll
-    for (int u = 0; u < U; ++u) part[u] = 0.0f;
+    for (int u = 0; u < U; ++u) {
+      part[u] = 0.0f;
+      cnv[u] = c0 + u < k ? cnorm[c0 + u] : 0.0f;  // loaded ahead of the tests below
+    }
     for (int j = lane; j < d; j += 32) {
       const float xj = x[j];
 #pragma unroll
@@ -103,7 +106,7 @@ __device__ __noinline__ uint32_t exact_pick(const float *x, int d, const float *
 #pragma unroll
     for (int u = 0; u < U; ++u) {
       const int c = c0 + u;
-      if (c >= k || !(fmaf(-2.0f, part[u], cnorm[c]) <= lim)) continue;
+      if (c >= k || !(fmaf(-2.0f, part[u], cnv[u]) <= lim)) continue;
       const float dist = ref_dist(x, cent + static_cast<int64_t>(c) * d, d);
       if (dist < bd) {
         bd = dist;
@@ -133,29 +136,83 @@ __device__ __forceinline__ void push_close(unsigned *ccount, uint2 *citems, int6
         make_uint2(static_cast<uint32_t>(p), __float_as_uint(lim));
 }
 
-// `cfloats` > 0: the centroids (k x d floats) fit in the block's dynamic
-// shared memory and are read from there.
-__global__ void kmeans_settle_kernel(const float *points, int d, const float *cent, int k,
-                                     const float *cnorm, const unsigned *ccount,
-                                     const uint2 *citems, uint32_t *out, unsigned *exact,
-                                     int cfloats) {
+// The same pick with the centroids staged in shared memory (rows padded to
+// cs = d + 1 floats, so that lane r reading element j of centroid r + 32 i
+// hits bank (r + j) % 32: no conflicts), their norms beside them and the
+// point's row in `xs`: lane r takes whole centroids r, r + 32, ... (its dot
+// products in dimension order, any FP32 order being within the bound), forms
+// the reference's distance of its candidates and keeps the first smallest
+// below FLT_MAX; the warp then keeps the smallest distance, the lowest index
+// among equal ones -- the first minimum in k order, the reference's pick.
+__device__ __forceinline__ uint32_t exact_pick_smem(const float *xs, int d, const float *cs,
+                                                    int k, const float *cn, float lim) {
+  const int lane = threadIdx.x & 31, st = d + 1;
+  float bd = FLT_MAX;
+  int bk = -1;
+  for (int c = lane; c < k; c += 32) {
+    const float *cp = cs + c * st;
+    float dot = 0.0f;
+    for (int j = 0; j < d; ++j) dot = fmaf(xs[j], cp[j], dot);
+    if (!(fmaf(-2.0f, dot, cn[c]) <= lim)) continue;
+    const float dist = ref_dist(xs, cp, d);
+    if (dist < bd) {
+      bd = dist;
+      bk = c;
+    }
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    const float od = __shfl_xor_sync(0xffffffffu, bd, o);
+    const int ok = __shfl_xor_sync(0xffffffffu, bk, o);
+    if (ok >= 0 && (bk < 0 || od < bd || (od == bd && ok < bk))) {
+      bd = od;
+      bk = ok;
+    }
+  }
+  return bk < 0 ? 0u : static_cast<uint32_t>(bk);
+}
+
+// Shared-memory floats the settle kernel stages (0: the centroids do not fit
+// in 96 KB and are read from global memory): centroids with rows of d + 1,
+// their norms, one point row per warp (8 warps).
+__host__ __device__ constexpr int64_t settle_smem_floats(int k, int d) {
+  return static_cast<int64_t>(k) * (d + 1) + k + 8 * static_cast<int64_t>(d);
+}
+constexpr int64_t kSettleSmemFloats = 96 * 1024 / 4;
+
+__global__ void __launch_bounds__(256) kmeans_settle_kernel(
+    const float *points, int d, const float *cent, int k, const float *cnorm,
+    const unsigned *ccount, const uint2 *citems, uint32_t *out, unsigned *exact, int staged) {
   wait_prior_grid();  // launched as a programmatic dependent of the screening kernel
-  extern __shared__ float s_cent[];
+  extern __shared__ float s_set[];
   const unsigned n = *ccount;
   if (exact && n && blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(exact, n);
   const unsigned wpb = blockDim.x >> 5, warps = gridDim.x * wpb;
   if (blockIdx.x * wpb >= n) return;  // no entry for this block's warps
-  const float *cb = cent;
-  if (cfloats > 0) {
-    for (int e = threadIdx.x; e < cfloats; e += blockDim.x) s_cent[e] = cent[e];
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  float *cs = s_set, *cn = s_set + static_cast<int64_t>(k) * (d + 1);
+  float *xs = cn + k + wib * d;
+  if (staged) {
+    for (int e = threadIdx.x; e < k * d; e += blockDim.x) {
+      const int c = e / d, j = e - c * d;
+      cs[c * (d + 1) + j] = cent[e];
+    }
+    for (int c = threadIdx.x; c < k; c += blockDim.x) cn[c] = cnorm[c];
     __syncthreads();
-    cb = s_cent;
   }
   for (unsigned w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; w < n; w += warps) {
     const uint2 it = citems[w];
-    const uint32_t pick = exact_pick(points + static_cast<int64_t>(it.x) * d, d, cb, k, cnorm,
-                                     __uint_as_float(it.y));
-    if ((threadIdx.x & 31) == 0) out[it.x] = pick;
+    const float *x = points + static_cast<int64_t>(it.x) * d;
+    uint32_t pick;
+    if (staged) {
+      for (int j = lane; j < d; j += 32) xs[j] = x[j];
+      __syncwarp();
+      pick = exact_pick_smem(xs, d, cs, k, cn, __uint_as_float(it.y));
+      __syncwarp();  // xs is rewritten for the warp's next entry
+    } else {
+      pick = exact_pick(x, d, cent, k, cnorm, __uint_as_float(it.y));
+    }
+    if (lane == 0) out[it.x] = pick;
   }
 }
 
@@ -899,10 +956,9 @@ hml_status launch_norms(const float *cent, int k, int d, const KmWs &w, cudaStre
 // (`early`: as a programmatic dependent of a screening kernel that allows it).
 hml_status launch_settle(const float *points, int d, const float *cent, int k, const KmWs &w,
                          uint32_t *out, unsigned *exact, cudaStream_t s, bool early = false) {
-  // the centroids in shared memory when they fit in 96 KB
-  const int64_t cf = static_cast<int64_t>(k) * d;
-  const int cfloats = cf * 4 <= 96 * 1024 ? static_cast<int>(cf) : 0;
-  const size_t smem = static_cast<size_t>(cfloats) * 4;
+  // the centroids, norms and point rows in shared memory when they fit
+  const int staged = settle_smem_floats(k, d) <= kSettleSmemFloats ? 1 : 0;
+  const size_t smem = staged ? static_cast<size_t>(settle_smem_floats(k, d)) * 4 : 0;
   cudaError_t e = cudaSuccess;
   if (smem > 48 * 1024)
     e = cudaFuncSetAttribute(kmeans_settle_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -911,7 +967,7 @@ hml_status launch_settle(const float *points, int d, const float *cent, int k, c
     e = launch_k_ex(kmeans_settle_kernel, dim3(2 * sm_count()), dim3(256), smem, s, 1, early,
                     points, d, cent, k, static_cast<const float *>(w.cnorm),
                     static_cast<const unsigned *>(w.ccount),
-                    static_cast<const uint2 *>(w.citems), out, exact, cfloats);
+                    static_cast<const uint2 *>(w.citems), out, exact, staged);
   note_cuda_error(e, "kmeans settle");
   return cuda_status(e);
 }
