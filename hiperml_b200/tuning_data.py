@@ -95,9 +95,14 @@ def measure(shapes: np.ndarray, reps: int = 3, deadline: float | None = None,
 
 # The reference workloads' SGEMM shapes (M, N, K, transA, transB), column-major:
 # the skinny 4096 x 16 x 4096 case, the M=65536, K=4096 precision sweep and the
-# square 8192^3 case.
+# square 8192^3 case, and the skinny ones again in the reference's own
+# row-major storage.
 TABLE_SHAPES = ((4096, 16, 4096, 0, 0), (65536, 8, 4096, 0, 0), (65536, 32, 4096, 0, 0),
-                (65536, 64, 4096, 0, 0), (65536, 128, 4096, 0, 0), (8192, 8192, 8192, 0, 0))
+                (65536, 64, 4096, 0, 0), (65536, 128, 4096, 0, 0), (8192, 8192, 8192, 0, 0),
+                # the same problems as the reference's row-major hmlSgemm stores
+                # them (column-major op(A) = A^T, op(B) = B^T: A K-contiguous)
+                (4096, 16, 4096, 1, 1), (65536, 8, 4096, 1, 1), (65536, 32, 4096, 1, 1),
+                (65536, 64, 4096, 1, 1), (65536, 128, 4096, 1, 1))
 
 
 # The reference workloads' SGEMV shapes (order, trans, M, N): the column-major

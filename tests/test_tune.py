@@ -104,8 +104,10 @@ def test_shipped_table_parses_and_covers_the_reference_workloads():
             if line.startswith("#") or line.startswith("v "):
                 continue
             akc, bkc, M, N, K = (int(x) for x in line.split(":")[0].split())
-            keys.add((M, N, K))
-        assert {(M, N, K) for (M, N, K, _ta, _tb) in td.TABLE_SHAPES} <= keys
+            keys.add((akc, bkc, M, N, K))
+        # column-major NN: A M-contiguous, B K-contiguous; transposed (the
+        # reference's row-major storage): A K-contiguous, B N-contiguous
+        assert {(ta, 1 - tb, M, N, K) for (M, N, K, ta, tb) in td.TABLE_SHAPES} <= keys
         # every SGEMV shape of the reference workloads has a measured variant
         for (order, trans, M, N) in td.GEMV_TABLE_SHAPES:
             assert hml.sgemv_select(order, trans, M, N) > 0

@@ -110,9 +110,9 @@ def test_shipped_table_is_the_default_selection(cuda):
         elif not line.startswith("#"):
             key, cfg = line.split(":")
             akc, bkc, M, N, K = (int(x) for x in key.split())
-            want[(M, N, K)] = tuple(int(x) for x in cfg.split()[:6])
+            want[(akc, bkc, M, N, K)] = tuple(int(x) for x in cfg.split()[:6])
     shape = (65536, 32, 4096)
-    got, size = _select_child(None, shape)
-    assert size == len(want) + n_gemv and got == want[shape]
+    got, size = _select_child(None, shape)  # column-major NN: A M-, B K-contiguous
+    assert size == len(want) + n_gemv and got == want[(0, 1) + shape]
     _, size = _select_child("none", shape)
     assert size == 0
