@@ -612,6 +612,10 @@ def predictor_entry(ctx, live_shapes=4, live_reps=3):
     pr.clear()
     heur = pr.heuristic_choices(shapes[te], cfgs)
     r_heur = pr.summarize(pr.regret(times[te], heur, cfgs))
+    # the library's defaults back (the shipped tuned table and network) for
+    # the entries measured after this one
+    hml.tune_load(os.path.join(os.path.dirname(hml.__file__), "data", "tuned_b200.txt"))
+    pr.load(pr.MODEL)
     return {"workload": "predictor",
             "config": {"dataset": "5000 shapes (M,N,K log-uniform [1,65536]x[1,256]x[16,16384], "
                                   "random transposes), each autotuned over the configuration "
