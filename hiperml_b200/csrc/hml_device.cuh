@@ -106,8 +106,8 @@ __device__ __forceinline__ void wait_prior_grid() {
 }
 
 // ------------------------------------------------------------------ TMA
-// 2-D tiled bulk tensor load, global -> this CTA's shared memory, completing
-// on `bar` with the tile's byte count.  No multicast.
+// 2-D tiled bulk tensor load, global -> this CTA's own shared memory only,
+// completing on `bar` with the tile's byte count.
 __device__ __forceinline__ void tma_load_2d(void *smem_dst, const void *tmap, uint64_t *bar,
                                             int x, int y) {
   asm volatile(

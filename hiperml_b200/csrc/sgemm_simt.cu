@@ -8,7 +8,7 @@
 //   * 32-deep K slabs of A (BM x 32) and B (32 x BN) are staged into a ring
 //     of `stages` shared-memory buffers, stages-1 slabs ahead of the math.
 //     When strides and base addresses allow it one thread issues 2-D TMA
-//     tile loads (cp.async.bulk.tensor, no multicast) that complete on a
+//     tile loads (cp.async.bulk.tensor into this CTA only) that complete on a
 //     per-slot mbarrier; otherwise every thread issues 4-byte cp.async
 //     copies with zero fill (cp.async groups).  A tile of K-contiguous A
 //     uses the 128-byte swizzle so that it is read without bank conflicts.
