@@ -10,21 +10,27 @@
 //
 // Here, with ||x||^2 constant per point, argmin_k dist_k = argmin_k
 // (||c_k||^2 - 2 x . c_k), and the dot products of every point with every
-// centroid are one skinny GEMM S = X C^T (points x clusters), in one of two
-// forms: the tiled form (method 1, up to 256 dimensions by default) runs the
-// GEMM as a register-tiled FP32 SIMT kernel with the argmin in its epilogue,
-// the products never leaving the SM; the GEMM form (method 2, wider points)
-// runs it through the library's SGEMM in an FP32-accurate configuration
-// (BF16X6 or SIMT; never the fast BF16X3 mode), S in HBM, and a second
-// kernel picks the argmin.  Since the products carry rounding errors that the
-// reference's direct sums do not, the pick is made exact: with g_k =
-// ||c_k||^2 - 2 S_k, every centroid whose g_k lies within a bound of the
-// smallest (16 gamma_{dims+4} (||x||^2 + max_k ||c_k||^2), more than twice
-// the sum of the worst-case errors of g and of the reference's dist) is a
-// candidate, the reference's choice is always among them, and when there is
-// more than one the kernel recomputes dist for the candidates with the
-// reference's own arithmetic, in increasing k with strict `<`.  So every
-// point gets the reference kernel's index, exact ties included.
+// centroid are one skinny GEMM S = X C^T (points x clusters), in one of three
+// forms:
+//   * tensor-core (method 3, the default where it applies: dims a multiple of
+//     4 up to 64, at most 256 centroids): TF32X3 products on tcgen05 into
+//     TMEM, the argmin read back from the accumulator by the thread that owns
+//     the point;
+//   * tiled (method 1, the default otherwise up to 256 dimensions): a
+//     register-tiled FP32 SIMT GEMM with the argmin in its epilogue;
+//   * SGEMM (method 2, wider points): the library's SGEMM in an FP32-accurate
+//     configuration (BF16X6 or SIMT; never the fast BF16X3 mode), S in HBM,
+//     and a pick kernel.
+// The products carry rounding errors that the reference's direct sums do
+// not, so the pick is made exact: with g_k = ||c_k||^2 - 2 S_k, every
+// centroid whose g_k lies within a bound of the smallest (16 gamma_{dims+4}
+// (||x||^2 + max_k ||c_k||^2) for the FP32 forms, twice that for TF32X3: more
+// than twice the sum of the worst-case errors of g and of the reference's
+// dist) is a candidate, and the reference's choice is always among them.  A
+// point with more than one candidate (or non-finite values) goes to a
+// close-call list that a settle kernel resolves with the reference's own
+// arithmetic over the candidates, the first smallest in increasing k.  So
+// every point gets the reference kernel's index, exact ties included.
 #include <cfloat>
 #include <cstring>
 
