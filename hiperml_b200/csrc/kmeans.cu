@@ -294,8 +294,8 @@ __global__ void kmeans_pick_kernel(const float *points, int64_t np, int d, int k
 // second smallest for each of its 8 points, in increasing k; at the end the
 // 16 threads that share a point merge theirs (the smaller g, the lower index
 // on equal g) with shuffles.  A point whose second smallest lies within the
-// bound of the smallest is settled as in the GEMM form, by the reference's
-// own distance over the candidates.  The products never leave the SM.
+// bound of the smallest goes to the close-call list.  The products never
+// leave the SM.
 constexpr int kTP = 128;         // points per block
 constexpr int kTC = 64;          // centroids per pass
 constexpr int kTD = 32;          // dimensions per shared-memory stage
@@ -485,13 +485,12 @@ __global__ void __launch_bounds__(kTThreads, 2) kmeans_tile_kernel(
 // memory (k and dims padded to kp = 64-multiple and dp = 4-multiple, dp <= 64
 // and kp * dp <= kResidentFloats, so two blocks fit on an SM): each block
 // stages the transposed centroids and their norms once and then walks
-// 128-point tiles (a persistent grid), the next
-// tile's rows copied by cp.async into the other of two row-major buffers
-// while the current tile is computed, so the loads' latency hides behind the
-// arithmetic.  A thread's 8 points are read as 16-byte row pieces (4
-// dimensions each), the centroids as 16-byte pieces of a dimension row; the
-// products, the running argmin, the merge and the settling of close calls
-// are the tiled kernel's.
+// 128-point tiles (a persistent grid), the next tile's rows copied by
+// cp.async into the other of two row-major buffers while the current tile
+// is computed, so the loads' latency hides behind the arithmetic.  A
+// thread's 8 points are read as 16-byte row pieces (4 dimensions each), the
+// centroids as 16-byte pieces of a dimension row; the products, the running
+// argmin, the merge and the close-call list are the tiled kernel's.
 constexpr int kResidentFloats = 8192;
 
 __global__ void __launch_bounds__(kTThreads, 2) kmeans_resident_kernel(
