@@ -869,10 +869,13 @@ def run_ours(args):
             [(k_, M_, N_, K_) for (k_, M_, N_, K_, *_r) in bufs], seconds=10.0)
         cpu = {"value": v, "unit": UNIT, "cores": cores, "kind": kind, "sample": desc}
 
-    # ---- the other configurations, one short entry each (default run only)
+    # ---- the other configurations, one short entry each (default run on one
+    # GPU only: with several ranks the rank-0 entries would hold the others at
+    # the closing barrier)
     workloads = None
     if (args.workload == "sweep" and not args.no_workloads and args.rows is None
-            and args.only_n is None and algo is None and args.dist == "uniform"):
+            and args.only_n is None and algo is None and args.dist == "uniform"
+            and ctx.world == 1):
         del bufs
         r.pop("bufs")
         torch.cuda.empty_cache()
