@@ -132,6 +132,13 @@ struct SimtTile {
           a4[i] = lds128(sa + m * kBK + (((kb >> 2) ^ (m & 7)) << 2));
         }
       }
+      // B K-contiguous: likewise one 16-byte broadcast per column of the
+      // warp's TN (all lanes read the same column)
+      float4 b4[BK_ ? TN : 1];
+      if (BK_) {
+#pragma unroll
+        for (int j = 0; j < TN; ++j) b4[j] = lds128(sb + (c.ncol + j) * kBK + kb);
+      }
 #pragma unroll
       for (int kk = 0; kk < 4; ++kk) {
         float a[TM];
@@ -149,7 +156,8 @@ struct SimtTile {
         float b[TN];
         if (BK_) {
 #pragma unroll
-          for (int j = 0; j < TN; ++j) b[j] = sb[(c.ncol + j) * kBK + kb + kk];
+          for (int j = 0; j < TN; ++j)
+            b[j] = kk == 0 ? b4[j].x : kk == 1 ? b4[j].y : kk == 2 ? b4[j].z : b4[j].w;
         } else {
 #pragma unroll
           for (int j = 0; j < TN / 4; ++j) {
