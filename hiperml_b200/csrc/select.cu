@@ -16,6 +16,7 @@ namespace hml {
 
 int simt_num_shapes();
 void simt_shape(int v, int *bm, int *bn, int *wk);
+int simt_ctas_per_sm(int v);
 int tc_num_shapes();
 void tc_shape(int v, int *bm, int *bn);
 bool tc_config_fits(int bn, int ns, int stages);
@@ -76,29 +77,39 @@ hml_sgemm_config heuristic_config(const GemmProblem &p, int algo) {
     if (check_stream(p, sc) == HML_STATUS_SUCCESS) return sc;
     break;
   }
-  // SIMT: the narrowest tile that holds N, wider rows when M is large
+  // SIMT, measured on B200 (M = 65536, K = 4096, and squares to 8192): the
+  // 128-row tiles 16, 32 and 64 wide up to those N; wider, 256 x 64 tiles of
+  // 4-row micro-tiles (41.5 TFLOP/s at N = 128) unless 32-wide tiles, at
+  // about 36 TFLOP/s, leave enough fewer columns idle (N = 96: 1.42 ms
+  // against 1.65)
   int var;
   if (p.N <= 8) var = 1;
   else if (p.N <= 16) var = 0;
-  else if (p.N <= 32) var = (p.M >= 256 * 2 * sm_count()) ? 3 : 2;
-  else if (p.N <= 64) var = (p.M >= 256 * sm_count()) ? 4 : 7;
-  else var = (p.M >= 256 * sm_count()) ? 5 : 8;
+  else if (p.N <= 32) var = 2;
+  else if (p.N <= 64) var = 7;
+  else {
+    const int64_t cols32 = (p.N + 31) / 32 * 32, cols64 = (p.N + 63) / 64 * 64;
+    var = cols32 * 415 < cols64 * 360 ? 2 : 6;
+  }
   return simt_config(p, var);
 }
 
-// The tiled SIMT configuration of micro-tile shape `var` for this problem:
-// split_k so the grid covers the machine, the deepest ring that fits.
+// The tiled SIMT configuration of micro-tile shape `var` for this problem.
+// split_k so the grid covers every CTA slot of the machine (at most 8 CTAs
+// to a cluster), and 2 where the grid is under two waves and K is long
+// (65536 x 128 x 4096: 1.65 ms against 1.69); a 3-deep ring where both
+// CTAs of an SM fit with it, else 2 (deeper rings measured no faster and
+// cost the second CTA).
 hml_sgemm_config simt_config(const GemmProblem &p, int var) {
   int bm, bn, wk;
   simt_shape(var, &bm, &bn, &wk);
-  const int per_sm = (bm * bn <= 128 * 16 * 2) ? 2 : 1;
+  const int per_sm = simt_ctas_per_sm(var);
   const int64_t tiles = ((p.M + bm - 1) / bm) * static_cast<int64_t>((p.N + bn - 1) / bn);
-  const int split = choose_split(tiles, p.K, per_sm, 128);
-  // deepest ring that fits the per-CTA share of shared memory
+  int split = std::min(choose_split(tiles, p.K, per_sm, 128), 8);
+  if (split == 1 && tiles < 2LL * sm_count() * per_sm && p.K >= 2048) split = 2;
+  // the per-CTA share of shared memory, less barriers and alignment slack
   const size_t budget = (227 * 1024) / per_sm - 2048;
-  int stages = 2;
-  for (int s : {3, 4, 6})
-    if (static_cast<size_t>(bm + bn) * 128 * s <= budget) stages = s;
+  const int stages = static_cast<size_t>(bm + bn) * 128 * 3 <= budget ? 3 : 2;
   return hml_sgemm_config{HML_ALGO_SIMT, bm, bn, split, stages, var};
 }
 

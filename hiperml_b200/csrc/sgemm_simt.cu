@@ -20,6 +20,9 @@
 //     so B values are shared-memory broadcasts and A values are read once per
 //     warp.  WK > 1 splits every K slab across warps (intra-CTA split-K) for
 //     the skinny shapes, where a C tile is too small to occupy 8 warps.
+//     Micro-tiles of at most 64 accumulators are compiled for 128
+//     registers a thread, so two CTAs share an SM and hide each other's
+//     latencies; the 8 x 16 micro-tiles run one CTA an SM.
 //   * epilogue: the WK partial tiles are summed in shared memory; with
 //     split_k > 1 the CTAs of one thread-block cluster each own a K range
 //     and the cluster sums their tiles through distributed shared memory in
@@ -44,7 +47,7 @@ struct SimtArgs {
 };
 
 template <int TM, int TN, int WM, int WN, int WK, bool AK, bool BK_, bool TMA>
-__global__ void __launch_bounds__(256, 1)
+__global__ void __launch_bounds__(256, TMA && TM * TN <= 64 ? 2 : 1)  // see simt_ctas_per_sm
     simt_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
                 SimtArgs args) {
   using T = SimtTile<TM, TN, WM, WN, WK, AK, BK_>;
@@ -318,5 +321,9 @@ void simt_shape(int v, int *bm, int *bn, int *wk) {
   *bn = kSimtShapes[v].bn();
   *wk = kSimtShapes[v].wk;
 }
+// CTAs of shape v one SM holds: two where the micro-tile has at most 64
+// accumulators (the TMA instances are compiled for 128 registers a thread),
+// given shared memory for both rings.
+int simt_ctas_per_sm(int v) { return kSimtShapes[v].tm * kSimtShapes[v].tn <= 64 ? 2 : 1; }
 
 }  // namespace hml

@@ -117,58 +117,89 @@ struct SimtTile {
       for (int j = 0; j < TN; ++j) acc[i][j] = 0.0f;
   }
 
-  // acc += this warp's K share of one staged slab.
+  // The TM rows of A this lane owns at k values kb..kb+3: a[kk][i].
+  __device__ static __forceinline__ void a_frag(const float *sa, int kb, const Coord &c,
+                                                float (&a)[4][TM]) {
+    if (AK) {
+      // A K-contiguous: one 16-byte read per row gives 4 k values
+#pragma unroll
+      for (int i = 0; i < TM; ++i) {
+        const int m = c.mrow + c.lane + 32 * i;
+        const float4 v = lds128(sa + m * kBK + (((kb >> 2) ^ (m & 7)) << 2));
+        a[0][i] = v.x; a[1][i] = v.y; a[2][i] = v.z; a[3][i] = v.w;
+      }
+    } else {
+#pragma unroll
+      for (int kk = 0; kk < 4; ++kk)
+#pragma unroll
+        for (int j = 0; j < TM / 4; ++j) {
+          const float4 v = lds128(sa + (kb + kk) * BM + c.mrow + 4 * c.lane + 128 * j);
+          a[kk][4 * j + 0] = v.x; a[kk][4 * j + 1] = v.y;
+          a[kk][4 * j + 2] = v.z; a[kk][4 * j + 3] = v.w;
+        }
+    }
+  }
+
+  // acc += this warp's K share of one staged slab.  Every accumulator takes
+  // its products in k order, whatever the operand layouts.
   __device__ static __forceinline__ void slab(const float *sa, const float *sb,
                                               float (&acc)[TM][TN], const Coord &c) {
 #pragma unroll 2
     for (int k4 = 0; k4 < KW / 4; ++k4) {
       const int kb = c.wk * KW + k4 * 4;
-      // A K-contiguous: one 16-byte read per row gives 4 k values
-      float4 a4[AK ? TM : 1];
-      if (AK) {
-#pragma unroll
-        for (int i = 0; i < TM; ++i) {
-          const int m = c.mrow + c.lane + 32 * i;
-          a4[i] = lds128(sa + m * kBK + (((kb >> 2) ^ (m & 7)) << 2));
-        }
-      }
-      // B K-contiguous: likewise one 16-byte broadcast per column of the
-      // warp's TN (all lanes read the same column)
-      float4 b4[BK_ ? TN : 1];
       if (BK_) {
+        float a[4][TM];
+        a_frag(sa, kb, c, a);
+        // B K-contiguous: one 16-byte broadcast per column gives its 4 k
+        // values (all lanes read the same column); each column is used as
+        // soon as it arrives, so only 4 B values are live at a time
 #pragma unroll
-        for (int j = 0; j < TN; ++j) b4[j] = lds128(sb + (c.ncol + j) * kBK + kb);
-      }
+        for (int j = 0; j < TN; ++j) {
+          const float4 v = lds128(sb + (c.ncol + j) * kBK + kb);
 #pragma unroll
-      for (int kk = 0; kk < 4; ++kk) {
-        float a[TM];
-        if (AK) {
-#pragma unroll
-          for (int i = 0; i < TM; ++i)
-            a[i] = kk == 0 ? a4[i].x : kk == 1 ? a4[i].y : kk == 2 ? a4[i].z : a4[i].w;
-        } else {
-#pragma unroll
-          for (int j = 0; j < TM / 4; ++j) {
-            const float4 v = lds128(sa + (kb + kk) * BM + c.mrow + 4 * c.lane + 128 * j);
-            a[4 * j + 0] = v.x; a[4 * j + 1] = v.y; a[4 * j + 2] = v.z; a[4 * j + 3] = v.w;
+          for (int i = 0; i < TM; ++i) {
+            float s = acc[i][j];
+            s = fmaf(a[0][i], v.x, s);
+            s = fmaf(a[1][i], v.y, s);
+            s = fmaf(a[2][i], v.z, s);
+            acc[i][j] = fmaf(a[3][i], v.w, s);
           }
         }
-        float b[TN];
-        if (BK_) {
+      } else {
+        // A K-contiguous: one 16-byte read per row gives 4 k values
+        float4 a4[AK ? TM : 1];
+        if (AK) {
 #pragma unroll
-          for (int j = 0; j < TN; ++j)
-            b[j] = kk == 0 ? b4[j].x : kk == 1 ? b4[j].y : kk == 2 ? b4[j].z : b4[j].w;
-        } else {
+          for (int i = 0; i < TM; ++i) {
+            const int m = c.mrow + c.lane + 32 * i;
+            a4[i] = lds128(sa + m * kBK + (((kb >> 2) ^ (m & 7)) << 2));
+          }
+        }
+#pragma unroll
+        for (int kk = 0; kk < 4; ++kk) {
+          float a[TM];
+          if (AK) {
+#pragma unroll
+            for (int i = 0; i < TM; ++i)
+              a[i] = kk == 0 ? a4[i].x : kk == 1 ? a4[i].y : kk == 2 ? a4[i].z : a4[i].w;
+          } else {
+#pragma unroll
+            for (int j = 0; j < TM / 4; ++j) {
+              const float4 v = lds128(sa + (kb + kk) * BM + c.mrow + 4 * c.lane + 128 * j);
+              a[4 * j + 0] = v.x; a[4 * j + 1] = v.y; a[4 * j + 2] = v.z; a[4 * j + 3] = v.w;
+            }
+          }
+          float b[TN];
 #pragma unroll
           for (int j = 0; j < TN / 4; ++j) {
             const float4 v = lds128(sb + (kb + kk) * BN + c.ncol + 4 * j);
             b[4 * j + 0] = v.x; b[4 * j + 1] = v.y; b[4 * j + 2] = v.z; b[4 * j + 3] = v.w;
           }
+#pragma unroll
+          for (int i = 0; i < TM; ++i)
+#pragma unroll
+            for (int j = 0; j < TN; ++j) acc[i][j] = fmaf(a[i], b[j], acc[i][j]);
         }
-#pragma unroll
-        for (int i = 0; i < TM; ++i)
-#pragma unroll
-          for (int j = 0; j < TN; ++j) acc[i][j] = fmaf(a[i], b[j], acc[i][j]);
       }
     }
   }
