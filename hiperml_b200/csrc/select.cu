@@ -77,36 +77,38 @@ hml_sgemm_config heuristic_config(const GemmProblem &p, int algo) {
     if (check_stream(p, sc) == HML_STATUS_SUCCESS) return sc;
     break;
   }
-  // SIMT, measured on B200 (M = 65536, K = 4096, and squares to 8192): the
-  // 128-row tiles 16, 32 and 64 wide up to those N; wider, 256 x 64 tiles of
-  // 4-row micro-tiles (41.5 TFLOP/s at N = 128) unless 32-wide tiles, at
-  // about 36 TFLOP/s, leave enough fewer columns idle (N = 96: 1.42 ms
-  // against 1.65)
+  // SIMT, measured on B200 (M = 1024 to 65536, K = 4096, and squares to
+  // 8192): 128-row tiles 8, 16, 32 and 64 wide up to those N, except 256 x 64
+  // tiles of 4-row micro-tiles from N = 33 once M gives them 64 row tiles
+  // (16384 x 64: 208 us against 228); above N = 64 those 256 x 64 tiles (52
+  // TFLOP/s at N = 128) unless 32-wide tiles, at about 42 TFLOP/s, leave
+  // enough fewer columns idle (N = 96: 1.27 ms against 1.31)
   int var;
   if (p.N <= 8) var = 1;
   else if (p.N <= 16) var = 0;
   else if (p.N <= 32) var = 2;
-  else if (p.N <= 64) var = 7;
+  else if (p.N <= 64) var = p.M >= 64 * 256 ? 6 : 7;
   else {
     const int64_t cols32 = (p.N + 31) / 32 * 32, cols64 = (p.N + 63) / 64 * 64;
-    var = cols32 * 415 < cols64 * 360 ? 2 : 6;
+    var = cols32 * 52 < cols64 * 42 ? 2 : 6;
   }
   return simt_config(p, var);
 }
 
 // The tiled SIMT configuration of micro-tile shape `var` for this problem.
-// split_k so the grid covers every CTA slot of the machine (at most 8 CTAs
-// to a cluster), and 2 where the grid is under two waves and K is long
-// (65536 x 128 x 4096: 1.65 ms against 1.69); a 3-deep ring where both
-// CTAs of an SM fit with it, else 2 (deeper rings measured no faster and
-// cost the second CTA).
+// split_k so the grid covers every CTA slot of the machine, at most 8 (4096
+// x 32 x 4096: 41 us against 68 at 16), and 2 for tiles
+// of two CTAs an SM where the grid is under two waves and K is long (65536
+// x 128 x 4096 on 256 x 64 tiles: 1.31 ms; one CTA an SM measured slower
+// split); a 3-deep ring where both CTAs of an SM fit with it, else 2
+// (deeper rings measured no faster and cost the second CTA).
 hml_sgemm_config simt_config(const GemmProblem &p, int var) {
   int bm, bn, wk;
   simt_shape(var, &bm, &bn, &wk);
   const int per_sm = simt_ctas_per_sm(var);
   const int64_t tiles = ((p.M + bm - 1) / bm) * static_cast<int64_t>((p.N + bn - 1) / bn);
   int split = std::min(choose_split(tiles, p.K, per_sm, 128), 8);
-  if (split == 1 && tiles < 2LL * sm_count() * per_sm && p.K >= 2048) split = 2;
+  if (split == 1 && per_sm == 2 && tiles < 2LL * sm_count() * per_sm && p.K >= 2048) split = 2;
   // the per-CTA share of shared memory, less barriers and alignment slack
   const size_t budget = (227 * 1024) / per_sm - 2048;
   const int stages = static_cast<size_t>(bm + bn) * 128 * 3 <= budget ? 3 : 2;
