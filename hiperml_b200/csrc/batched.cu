@@ -197,8 +197,7 @@ __device__ __forceinline__ void batch_slot(const BatchProblem &p, int lay, int64
 
 __global__ void __launch_bounds__(kBatchThreads, 2) batched_kernel(BatchArgs a) {
   extern __shared__ uint8_t smem_raw[];
-  uint8_t *smem = reinterpret_cast<uint8_t *>(
-      (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~static_cast<uintptr_t>(1023));
+  uint8_t *smem = align_shared(smem_raw, 1024);
   __shared__ int s_item;
   const int tid = threadIdx.x;
   for (;;) {

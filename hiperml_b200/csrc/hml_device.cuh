@@ -25,6 +25,17 @@ __device__ __forceinline__ uint32_t smem_u32(const void *p) {
   return static_cast<uint32_t>(__cvta_generic_to_shared(p));
 }
 
+// `p` advanced to the next multiple of `align` (a power of two) bytes in the
+// shared window.  Pointer arithmetic on a shared pointer, not a round trip
+// through an integer, so that the compiler keeps the shared state space for
+// everything derived from it (32-bit addresses and shared loads instead of
+// generic 64-bit ones).
+template <typename T>
+__device__ __forceinline__ T *align_shared(T *p, uint32_t align) {
+  const uint32_t pad = (align - (smem_u32(p) & (align - 1))) & (align - 1);
+  return reinterpret_cast<T *>(reinterpret_cast<uint8_t *>(p) + pad);
+}
+
 __device__ __forceinline__ uint64_t globaltimer_ns() {
   uint64_t t;
   asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));

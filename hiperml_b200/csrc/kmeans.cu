@@ -687,8 +687,7 @@ __global__ void __launch_bounds__(km_tc_threads(W), 1)
     kmeans_tc_kernel(const __grid_constant__ CUtensorMap tmX,
                      const __grid_constant__ CUtensorMap tmB, const __grid_constant__ KmTcArgs a) {
   extern __shared__ uint8_t smem_raw[];
-  uint8_t *smem = reinterpret_cast<uint8_t *>(
-      (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~static_cast<uintptr_t>(1023));
+  uint8_t *smem = align_shared(smem_raw, 1024);
   const int dp = a.dp, kp = a.kp, nkb = dp / 32, SA = a.sa;
   const int slot = nkb * kTcBox;   // bytes of one point tile
   const int btile = kp * 128;      // bytes of one (plane, 32-dim block) of the centroids

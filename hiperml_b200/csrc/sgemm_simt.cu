@@ -55,8 +55,7 @@ __global__ void __launch_bounds__(256, TMA && TM * TN <= 64 ? 2 : 1)  // see sim
   constexpr int A_BYTES = T::A_BYTES, STAGE_BYTES = T::STAGE_BYTES;
 
   extern __shared__ uint8_t smem_raw[];
-  uint8_t *smem = reinterpret_cast<uint8_t *>(
-      (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~static_cast<uintptr_t>(1023));
+  uint8_t *smem = align_shared(smem_raw, 1024);
   const GemmProblem &p = args.p;
   const int stages = args.stages;
   // barriers sit past both the ring and the epilogue's reduction buffer

@@ -201,8 +201,7 @@ __global__ void __launch_bounds__(kSThreads, kSCtasPerSm)
   constexpr int B_BYTES = kSCols * NB * 4;
   constexpr int STAGE = A_BYTES + B_BYTES;  // a multiple of 128 bytes
   extern __shared__ uint8_t smem_raw[];
-  uint8_t *smem = reinterpret_cast<uint8_t *>(
-      (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~static_cast<uintptr_t>(1023));
+  uint8_t *smem = align_shared(smem_raw, 1024);
   const int stages = args.stages;
   float *red = reinterpret_cast<float *>(smem + stages * STAGE);  // [phase][row][NB]
   uint64_t *full = reinterpret_cast<uint64_t *>(red + kSPhases * kSRows * NB);

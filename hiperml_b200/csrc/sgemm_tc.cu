@@ -428,8 +428,7 @@ __global__ void __launch_bounds__(tc_warps(BN, NS) * 32, 1)
   constexpr int P = FH ? 1 : kChunkK / kBK;
 
   extern __shared__ uint8_t smem_raw[];
-  uint8_t *smem = reinterpret_cast<uint8_t *>(
-      (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~static_cast<uintptr_t>(1023));
+  uint8_t *smem = align_shared(smem_raw, 1024);
   const GemmProblem &p = args.p;
   const int SA = args.sa, SO = args.so;
   uint8_t *aring = smem;
@@ -449,8 +448,7 @@ __global__ void __launch_bounds__(tc_warps(BN, NS) * 32, 1)
   uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(sfull + R);
   int *bad_flag = reinterpret_cast<int *>(tmem_slot + 1);
   int *tmax_sh = bad_flag + 1;        // FP16X3: the largest column scale exponent of the tile
-  int *sexp = reinterpret_cast<int *>((reinterpret_cast<uintptr_t>(tmax_sh + 1) + 15) &
-                                      ~static_cast<uintptr_t>(15));  // [R][kBM]
+  int *sexp = align_shared(tmax_sh + 1, 16);  // [R][kBM]
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int split = args.split;
@@ -1188,8 +1186,7 @@ __global__ void __launch_bounds__(tcb_warps(BN, NS) * 32, 1) tc_batch_kernel(TcB
   static_assert(G == P, "converter group g converts block g of every chunk");
 
   extern __shared__ uint8_t smem_raw[];
-  uint8_t *smem = reinterpret_cast<uint8_t *>(
-      (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~static_cast<uintptr_t>(1023));
+  uint8_t *smem = align_shared(smem_raw, 1024);
   const int SA = args.sa, SO = args.so;
   uint8_t *aring = smem;
   uint8_t *bring = aring + SA * A32_BYTES;
