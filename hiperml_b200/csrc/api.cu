@@ -148,7 +148,7 @@ bool same_config(const hml_sgemm_config &a, const hml_sgemm_config &b) {
          a.split_k == b.split_k && a.stages == b.stages && a.variant == b.variant;
 }
 
-hml_status run(const GemmProblem &p, const hml_sgemm_config &c, cudaStream_t s) {
+hml_status run(const GemmProblem &p, const hml_sgemm_config &c, cudaStream_t s, bool auto_choice) {
   if (p.M == 0 || p.N == 0) return HML_STATUS_SUCCESS;
   if (p.K == 0 || p.alpha == 0.0f) return launch_scale(p.C, p.M, p.N, p.scm, p.scn, p.beta, s);
   switch (c.algo) {
@@ -156,7 +156,7 @@ hml_status run(const GemmProblem &p, const hml_sgemm_config &c, cudaStream_t s) 
     case HML_ALGO_BF16X3:
     case HML_ALGO_BF16X6:
     case HML_ALGO_TF32X3:
-    case HML_ALGO_FP16X3: return launch_tc(p, c, s);
+    case HML_ALGO_FP16X3: return launch_tc(p, c, s, auto_choice);
     default: return HML_STATUS_INVALID_VALUE;
   }
 }
@@ -190,10 +190,11 @@ bool check_config_ok(const GemmProblem &p, const hml_sgemm_config &c) {
   return check_config(p, c) == HML_STATUS_SUCCESS;
 }
 
-hml_status run_config(const GemmProblem &p, const hml_sgemm_config &c, cudaStream_t s) {
+hml_status run_config(const GemmProblem &p, const hml_sgemm_config &c, cudaStream_t s,
+                      bool auto_choice) {
   hml_status st = check_config(p, c);
   if (st != HML_STATUS_SUCCESS) return st;
-  return run(p, c, s);
+  return run(p, c, s, auto_choice);
 }
 
 }  // namespace hml
@@ -235,7 +236,7 @@ hml_status hml_sgemm_ex(hml_order order, hml_op transA, hml_op transB, int M, in
   hml_sgemm_config c;
   st = select_config(p, &c, s);
   if (st != HML_STATUS_SUCCESS) return st;
-  return run_config(p, c, s);
+  return run_config(p, c, s, true);
 }
 
 hml_status hml_sgemm_ex_config(hml_order order, hml_op transA, hml_op transB, int M, int N,

@@ -72,7 +72,11 @@ inline bool gemv_variant_valid(bool rows, int v) {
 hml_status launch_scale(float *C, int M, int N, int64_t scm, int64_t scn, float beta,
                         cudaStream_t s);
 hml_status launch_simt(const GemmProblem &p, const hml_sgemm_config &c, cudaStream_t s);
-hml_status launch_tc(const GemmProblem &p, const hml_sgemm_config &c, cudaStream_t s);
+// waves: a split_k = 1 configuration whose grid would end in a partial wave
+// runs that wave's rows as a second grid split in K (automatic selection
+// only; an explicitly given configuration runs exactly as given).
+hml_status launch_tc(const GemmProblem &p, const hml_sgemm_config &c, cudaStream_t s,
+                     bool waves = false);
 hml_status check_simt(const GemmProblem &p, const hml_sgemm_config &c);
 // The stream-K SIMT kernel for N <= 8 with contiguous columns of A
 // (sgemm_stream.cu); reached through the SIMT family's variants

@@ -13,5 +13,8 @@ hml_sgemm_config simt_config(const GemmProblem &p, int var);
 // the SIMT family (false when none applies).
 bool v1_rule_config(const GemmProblem &p, int K_row, int N_row, hml_sgemm_config *c);
 const std::vector<hml_sgemm_config> &config_space();
-hml_status run_config(const GemmProblem &p, const hml_sgemm_config &c, cudaStream_t s);
+// auto_choice: the configuration came from select_config, so the launch may
+// add the tail-wave split of launch_tc.
+hml_status run_config(const GemmProblem &p, const hml_sgemm_config &c, cudaStream_t s,
+                      bool auto_choice = false);
 }  // namespace hml

@@ -938,6 +938,38 @@ hml_status launch_tc_planes(const GemmProblem &p, const hml_sgemm_config &c,
   return cuda_status(e);
 }
 
+// launch_tc_planes for a split_k = 1 configuration whose grid ends in a
+// partial wave: the whole waves of row tiles run as configured and the rows
+// of the last wave, when it would leave at least half of the SMs idle, run
+// as a second grid with K split across the idle SMs (disjoint rows of C, so
+// the results are those of split_k = 2..8 on those rows).  One CTA per SM:
+// M = 65536, N = 32 is 3 full waves of 148 tiles and 68 more.
+template <int BN, int NS, bool AK>
+hml_status launch_tc_waves(const GemmProblem &p, const hml_sgemm_config &c,
+                           const __nv_bfloat16 *planes, int k_pad, int n_pad, int *err,
+                           cudaStream_t s) {
+  const int64_t tiles = (static_cast<int64_t>(p.M) + kBM - 1) / kBM;
+  const int64_t slots = sm_count();
+  const int64_t full = (tiles / slots) * slots;
+  const int64_t rest = tiles - full;
+  if (c.split_k != 1 || n_pad != BN || full == 0 || rest == 0 || 2 * rest > slots)
+    return launch_tc_planes<BN, NS, AK>(p, c, planes, k_pad, n_pad, err, s);
+  int split = 1;
+  while (split < 8 && 2 * split * rest <= slots && k_pad / (2 * split) >= 4 * kChunkK) split *= 2;
+  if (split == 1) return launch_tc_planes<BN, NS, AK>(p, c, planes, k_pad, n_pad, err, s);
+  const int64_t m1 = full * kBM;
+  GemmProblem head = p, tail = p;
+  head.M = static_cast<int>(m1);
+  tail.M = p.M - static_cast<int>(m1);
+  tail.A = p.A + m1 * p.sam;
+  tail.C = p.C + m1 * p.scm;
+  hml_sgemm_config ct = c;
+  ct.split_k = split;
+  hml_status st = launch_tc_planes<BN, NS, AK>(head, c, planes, k_pad, n_pad, err, s);
+  if (st != HML_STATUS_SUCCESS) return st;
+  return launch_tc_planes<BN, NS, AK>(tail, ct, planes, k_pad, n_pad, err, s);
+}
+
 // B -> BF16 planes in `planes` ([NS][n_pad][k_pad]).
 template <int NS>
 hml_status split_b(const GemmProblem &p, __nv_bfloat16 *planes, int k_pad, int n_pad,
@@ -971,7 +1003,7 @@ hml_status split_b_fh(const GemmProblem &p, void *planes, int *bexp, int k_pad, 
 }
 
 template <int BN, int NS, bool AK>
-hml_status run_tc(const GemmProblem &p, const hml_sgemm_config &c, cudaStream_t s) {
+hml_status run_tc(const GemmProblem &p, const hml_sgemm_config &c, cudaStream_t s, bool waves) {
   const int k_pad = ((p.K + kChunkK - 1) / kChunkK) * kChunkK;
   const int n_pad = ((p.N + BN - 1) / BN) * BN;
   // B planes in the stream's workspace (FP16X3: then the column exponents)
@@ -992,22 +1024,27 @@ hml_status run_tc(const GemmProblem &p, const hml_sgemm_config &c, cudaStream_t 
   } else {
     st = split_b<NS>(p, planes, k_pad, n_pad, s);
     if (st != HML_STATUS_SUCCESS) return st;
+    if (waves)
+      return launch_tc_waves<BN, NS, AK>(p, c, planes, k_pad, n_pad, device_error_word(), s);
     return launch_tc_planes<BN, NS, AK>(p, c, planes, k_pad, n_pad, device_error_word(), s);
   }
 }
 
 template <int BN, int NS>
-hml_status run_tc_layout(const GemmProblem &p, const hml_sgemm_config &c, cudaStream_t s) {
-  return p.a_kcontig() ? run_tc<BN, NS, true>(p, c, s) : run_tc<BN, NS, false>(p, c, s);
+hml_status run_tc_layout(const GemmProblem &p, const hml_sgemm_config &c, cudaStream_t s,
+                         bool waves) {
+  return p.a_kcontig() ? run_tc<BN, NS, true>(p, c, s, waves)
+                       : run_tc<BN, NS, false>(p, c, s, waves);
 }
 
 template <int NS>
-hml_status run_tc_ns(const GemmProblem &p, const hml_sgemm_config &c, cudaStream_t s) {
+hml_status run_tc_ns(const GemmProblem &p, const hml_sgemm_config &c, cudaStream_t s,
+                     bool waves) {
   switch (c.tile_n) {
-    case 16: return run_tc_layout<16, NS>(p, c, s);
-    case 32: return run_tc_layout<32, NS>(p, c, s);
-    case 64: return run_tc_layout<64, NS>(p, c, s);
-    case 128: return run_tc_layout<128, NS>(p, c, s);
+    case 16: return run_tc_layout<16, NS>(p, c, s, waves);
+    case 32: return run_tc_layout<32, NS>(p, c, s, waves);
+    case 64: return run_tc_layout<64, NS>(p, c, s, waves);
+    case 128: return run_tc_layout<128, NS>(p, c, s, waves);
     default: return HML_STATUS_INVALID_VALUE;
   }
 }
@@ -1055,14 +1092,15 @@ hml_status check_tc(const GemmProblem &p, const hml_sgemm_config &c) {
   return HML_STATUS_SUCCESS;
 }
 
-hml_status launch_tc(const GemmProblem &p, const hml_sgemm_config &c, cudaStream_t s) {
+hml_status launch_tc(const GemmProblem &p, const hml_sgemm_config &c, cudaStream_t s,
+                     bool waves) {
   hml_status st = check_tc(p, c);
   if (st != HML_STATUS_SUCCESS) return st;
   switch (c.algo) {
-    case HML_ALGO_BF16X3: return run_tc_ns<2>(p, c, s);
-    case HML_ALGO_BF16X6: return run_tc_ns<3>(p, c, s);
-    case HML_ALGO_FP16X3: return run_tc_ns<5>(p, c, s);
-    default: return run_tc_ns<4>(p, c, s);
+    case HML_ALGO_BF16X3: return run_tc_ns<2>(p, c, s, waves);
+    case HML_ALGO_BF16X6: return run_tc_ns<3>(p, c, s, waves);
+    case HML_ALGO_FP16X3: return run_tc_ns<5>(p, c, s, waves);
+    default: return run_tc_ns<4>(p, c, s, waves);
   }
 }
 

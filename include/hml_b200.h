@@ -104,7 +104,12 @@ const char *hml_version(void);
  * or trained by hml_predictor_train; without either, the first selection
  * loads the network shipped as data/predictor_b200.txt beside the library
  * (environment: HML_PREDICTOR=<file> names another, HML_PREDICTOR=none
- * disables it).  Replaces the launch half of
+ * disables it).  When the chosen tensor-core configuration has split_k = 1
+ * and its grid of row tiles would end in a wave that leaves at least half of
+ * the SMs idle, the rows of that last wave run as a second grid with K split
+ * across the idle SMs (those rows then carry split-K rounding, within the
+ * same error bounds; hml_sgemm_ex_config runs a configuration exactly as
+ * given).  Replaces the launch half of
  * hmlSgemm (src/hml_sgemm.cu:120-211 in the reference), generalised to
  * both storage orders, transposes and leading dimensions. */
 hml_status hml_sgemm_ex(hml_order order, hml_op transA, hml_op transB, int M,
