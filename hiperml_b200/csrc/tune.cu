@@ -366,13 +366,15 @@ hml_status autotune(hml_order order, hml_op ta, hml_op tb, int M, int N, int K,
     ent.time_us = -1.0f;
     ent.status = check_config(p, c);
     if (ent.status == HML_STATUS_SUCCESS) {
-      // warm-up launch (also rejects configurations the driver refuses)
-      ent.status = run_config(p, c, s);
+      // warm-up launch (also rejects configurations the driver refuses);
+      // timed as hml_sgemm_ex runs a selected configuration (the tail-wave
+      // split of the tensor-core forms included), since the table feeds it
+      ent.status = run_config(p, c, s, true);
       std::vector<float> ts;
       for (int r = 0; r < reps && ent.status == HML_STATUS_SUCCESS; ++r) {
         if (need_flush) cudaMemsetAsync(g_bufs.flush, r & 0xff, flush_bytes, s);
         cudaEventRecord(e0, s);
-        ent.status = run_config(p, c, s);
+        ent.status = run_config(p, c, s, true);
         cudaEventRecord(e1, s);
         if (cudaEventSynchronize(e1) != cudaSuccess) {
           ent.status = HML_STATUS_CUDA_ERROR;

@@ -200,7 +200,8 @@ typedef struct hml_tune_entry {
  * problem shape with leading dimensions rounded up to a multiple of 4 floats
  * (16 bytes, addressable by every kernel family) and uniform[-1,1] operands:
  * one warm-up call, then `reps` calls timed with CUDA events on the stream,
- * L2 flushed before each when the operands fit in it, median kept.  A
+ * L2 flushed before each when the operands fit in it, median kept; each
+ * configuration runs as hml_sgemm_ex would run it once selected.  A
  * configuration that cannot run or fails is recorded with its status and
  * skipped.  Writes up to max_entries results (*n_entries = count) and
  * records the fastest configuration the math mode allows in the tuned table
