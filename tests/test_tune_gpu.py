@@ -116,3 +116,54 @@ def test_shipped_table_is_the_default_selection(cuda):
     assert size == len(want) + n_gemv and got == want[(0, 1) + shape]
     _, size = _select_child("none", shape)
     assert size == 0
+
+
+def test_tail_wave_split(cuda, tmp_path):
+    """hml_sgemm_ex with a whole-K tensor-core choice whose grid ends in a
+    wave of at most half the SMs: the rows of the whole waves are exactly
+    the configuration's, the last wave's rows those of the same tile split in
+    K over the idle SMs (here 4 ways), and repeated calls give the same bits."""
+    import os
+
+    import torch
+    sms = torch.cuda.get_device_properties(0).multi_processor_count
+    rest = 20
+    M, N, K = (sms + rest) * 128, 32, 2048
+    split = 1
+    while split < 8 and 2 * split * rest <= sms and K // (2 * split) >= 256:
+        split *= 2
+    assert split > 1
+    cfg = hml.SgemmConfig(hml.ALGO_BF16X6, 128, 32, 1, 6, 1)
+    f = tmp_path / "tuned.txt"
+    f.write_text("#HML-B200 tuning v2\n# device test sms %d\n"
+                 "# akc bkc M N K : algo tile_m tile_n split_k stages variant time_us\n"
+                 "0 1 %d %d %d : 3 128 32 1 6 1 1.0\n" % (sms, M, N, K))
+    try:
+        hml.tune_clear()
+        assert hml.tune_load(str(f)) == 1
+        assert hml.select(0, 0, 0, M, N, K).as_tuple() == cfg.as_tuple()
+        A = torch.empty(M * K, device="cuda")
+        B = torch.empty(K * N, device="cuda")
+        hml.fill_random(A, 5, 0, 1)
+        hml.fill_random(B, 5, 1, 1)
+        C = torch.zeros(M * N, device="cuda")
+        hml.sgemm_ex(0, 0, 0, M, N, K, 1.0, A, M, B, K, 0.0, C, M)
+        C2 = torch.zeros(M * N, device="cuda")
+        hml.sgemm_ex(0, 0, 0, M, N, K, 1.0, A, M, B, K, 0.0, C2, M)
+        assert torch.equal(C, C2)
+        whole = torch.zeros(M * N, device="cuda")
+        hml.sgemm_ex(0, 0, 0, M, N, K, 1.0, A, M, B, K, 0.0, whole, M, config=cfg)
+        split_cfg = hml.SgemmConfig(hml.ALGO_BF16X6, 128, 32, split, 6, 1)
+        splitk = torch.zeros(M * N, device="cuda")
+        hml.sgemm_ex(0, 0, 0, M, N, K, 1.0, A, M, B, K, 0.0, splitk, M, config=split_cfg)
+        m1 = sms * 128
+        got, w, sk = (t.view(N, M) for t in (C, whole, splitk))
+        assert torch.equal(got[:, :m1], w[:, :m1])
+        assert torch.equal(got[:, m1:], sk[:, m1:])
+        assert not torch.equal(got, w)  # the tail rows did take the split path
+        err = hml.error_fp64(0, 0, 0, M, N, K, 1.0, A, M, B, K, 0.0, None, C, M)
+        assert err[2] <= 2 * (K + 2) * 2.0 ** -24, err
+        assert hml.device_error() == 0
+    finally:
+        hml.tune_clear()
+        hml.tune_load(os.path.join(os.path.dirname(hml.__file__), "data", "tuned_b200.txt"))
